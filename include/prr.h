@@ -1,0 +1,237 @@
+/*
+ * prr.h - C ABI of prr-b200, the B200-native ParRelRay ray tracer.
+ *
+ * Plain C, plain pointers and sizes.  Every entry point returns a prr_status
+ * (0 = PRR_OK); the message of the last failure on a context is available
+ * from prr_last_error().  No exceptions cross this boundary.  The caller owns
+ * every host buffer; a context owns its device buffers.  Calls on one
+ * context are synchronous unless named *_device (those are asynchronous on
+ * the given CUDA stream).  One context per host thread.
+ *
+ * The reference (GKylian/ParRelRay) has no runtime API: its "plugin" surface
+ * is the compile-time metric header (main/metric.h:12) plus the .params
+ * deck (main/io.h:21-58).  Each entry point below names the reference code it
+ * replaces.
+ */
+#ifndef PRR_H
+#define PRR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PRR_ABI_VERSION 1
+#define PRR_MAX_SPHERES 8
+#define PRR_MAX_TEXTURES 32
+
+typedef struct prr_ctx prr_ctx;
+
+typedef enum prr_status {
+    PRR_OK = 0,
+    PRR_ERR_INVALID = 1,     /* bad argument / descriptor */
+    PRR_ERR_CUDA = 2,        /* CUDA runtime error (message in prr_last_error) */
+    PRR_ERR_NOMEM = 3,       /* allocation failed */
+    PRR_ERR_TIMEOUT = 4,     /* device watchdog expired; rays left unfinished */
+    PRR_ERR_IO = 5,          /* file could not be read or written */
+    PRR_ERR_UNSUPPORTED = 6, /* option not implemented */
+    PRR_ERR_NO_DEVICE = 7    /* no CUDA device / extension unusable */
+} prr_status;
+
+/* Integration result per ray; same values as the reference enum RESULT
+ * (main/base.h:37-43). */
+typedef enum prr_result {
+    PRR_RESULT_SUCCESS = 0,
+    PRR_RESULT_MATH_ERROR = 1,
+    PRR_RESULT_IO_ERROR = 2,
+    PRR_RESULT_INFINITE_GEO = 3,
+    PRR_RESULT_INTERSECTION = 4
+} prr_result;
+
+/* Solver ids; same values as the reference enum SOLVER (main/base.h:26-34).
+ * Only EULER and RKF45 are integrators in the reference (prr.cpp:295-305). */
+typedef enum prr_solver { PRR_SOLVER_EULER = 0, PRR_SOLVER_RKF45 = 2 } prr_solver;
+
+/* SSAA sample placement; same values as SSAA_DISTR (main/base.h:46-53). */
+typedef enum prr_ssaa { PRR_SSAA_NONE = 0, PRR_SSAA_REGULAR = 1 } prr_ssaa;
+
+typedef enum prr_metric {
+    PRR_METRIC_FLAT = 0,          /* metrics/flat.cuh */
+    PRR_METRIC_SCHWARZSCHILD = 1, /* metrics/schwarzschild.cuh (Kerr-Schild form) */
+    PRR_METRIC_KERR = 2           /* Kerr-Schild Kerr (new; the reference's is a stub) */
+} prr_metric;
+
+/* Integration semantics.
+ * REFERENCE: reproduces kernels/solver.cuh exactly, quirks included (stage
+ *   inputs of the velocity use h*u, solver.cuh:164-168; the initial 4-velocity
+ *   is (dir,1)*u0, solver.cuh:54; absolute error test against eps,
+ *   solver.cuh:174-188).  FP32 only.  Used for parity with the reference.
+ * PHYSICAL: textbook RKF45 stages, null initial 4-velocity (dir, u^t), and a
+ *   mixed error test |y5-y4| <= atol + rtol*|y| that works in FP32 down to
+ *   1e-7.  Every other rule (hooks, sphere test, colours) is unchanged. */
+typedef enum prr_mode { PRR_MODE_REFERENCE = 0, PRR_MODE_PHYSICAL = 1 } prr_mode;
+
+/* Arithmetic of the integrator (PHYSICAL mode).
+ * FP32: FP32 stages with Kahan-compensated state accumulation.
+ * FP64: everything in FP64.
+ * SPLIT: FP32 pass; rays flagged near the critical impact parameter or near
+ *        the horizon are re-integrated in FP64. */
+typedef enum prr_precision { PRR_PREC_FP32 = 0, PRR_PREC_FP64 = 1, PRR_PREC_SPLIT = 2 } prr_precision;
+
+/* How rays are scheduled on the GPU.
+ * PLAIN: one ray per thread, one kernel per pipeline stage, 64-row layers,
+ *        generic Christoffel-table geodesic (the reference's structure).
+ * PERSISTENT: persistent CTAs, warp-ballot ray compaction, fused ray
+ *        generation/integration/colouring/SSAA combine, Kerr-Schild
+ *        contraction in registers. */
+typedef enum prr_schedule { PRR_SCHED_PLAIN = 0, PRR_SCHED_PERSISTENT = 1 } prr_schedule;
+
+/* Background lookup.  RMS2X2 is the reference's OutSphere::getColorDefault2
+ * (main/base.h:119-162, piecewise constant); BILINEAR is a continuous lookup
+ * used for gradients. */
+typedef enum prr_bg_filter { PRR_BG_RMS2X2 = 0, PRR_BG_BILINEAR = 1 } prr_bg_filter;
+
+/* A textured sphere (scene/sphere.h:19-65). */
+typedef struct prr_sphere {
+    float center[3];
+    float radius;
+    int32_t texture_id; /* id given to prr_upload_texture; -1 = untextured (grey) */
+    int32_t _pad[3];
+} prr_sphere;
+
+/* Everything one frame (one render request) needs.  Field meanings follow
+ * the reference deck (prr.cpp:159-198, 245-253, Spacetime.cpp:17-44). */
+typedef struct prr_frame_desc {
+    /* camera (main/Camera.h:39-42) */
+    int32_t width, height;
+    int32_t ssaa;        /* prr_ssaa */
+    int32_t samples;     /* rays per pixel; a perfect square for REGULAR */
+    float vfov;          /* vertical field of view, radians */
+    float cam_pos[3];    /* camera position (x, y, z) */
+    float cam_alpha;     /* yaw a, radians */
+    float cam_beta;      /* pitch b, radians */
+    /* spacetime */
+    int32_t metric;      /* prr_metric */
+    float mass;          /* M (rs = 2M) */
+    float spin;          /* a (length units; |a| <= M) */
+    /* tracer (main/base.h:166-170) */
+    int32_t solver;      /* prr_solver */
+    int32_t mode;        /* prr_mode */
+    int32_t precision;   /* prr_precision (PHYSICAL mode) */
+    float h, hmin, hmax; /* initial / minimum / maximum step */
+    float eps;           /* REFERENCE mode absolute tolerance */
+    float rtol, atol;    /* PHYSICAL mode tolerances */
+    float rout;          /* outer sphere radius (Tracer::sph1.rout) */
+    float horizon_eps;   /* stop when r <= r_+ + horizon_eps (reference: 0.001) */
+    int32_t max_steps;   /* PHYSICAL mode accepted-step cap */
+    int32_t background_id; /* texture id of the equirectangular sky; -1 = black */
+    int32_t bg_filter;   /* prr_bg_filter */
+    int32_t fxaa;        /* 1 = FXAA after the SSAA combine (kernels/ssaa.cuh:150-181) */
+    float fp64_delta;    /* SPLIT: flag rays with |b - b_c|/b_c < fp64_delta */
+    float fp64_rfac;     /* SPLIT: flag rays reaching r < fp64_rfac * r_+ */
+    int32_t nspheres;
+    int32_t _pad0;
+    prr_sphere spheres[PRR_MAX_SPHERES];
+} prr_frame_desc;
+
+/* Counters of one render call (summed over frames). */
+typedef struct prr_stats {
+    int64_t rays;            /* rays traced (width*height*samples per frame) */
+    int64_t attempts;        /* integrator attempts (accepted + rejected) */
+    int64_t accepted;        /* accepted steps */
+    int64_t n_escaped;       /* SUCCESS with r >= rout */
+    int64_t n_captured;      /* SUCCESS at the horizon */
+    int64_t n_intersection;  /* INTERSECTION */
+    int64_t n_infinite;      /* INFINITE_GEO */
+    int64_t n_math_error;    /* MATH_ERROR */
+    int64_t n_fp64;          /* rays re-integrated in FP64 (SPLIT) */
+    double kernel_ms;        /* device time of the render, CUDA events */
+    int64_t kernel_launches; /* kernels launched by the call */
+} prr_stats;
+
+/* Launch shape of the persistent scheduler. */
+typedef struct prr_launch_config {
+    int32_t block_size;          /* threads per CTA (multiple of 32) */
+    int32_t blocks_per_sm;       /* resident CTAs per SM requested */
+    int32_t compaction_interval; /* attempts between warp refills */
+    int32_t rays_per_thread;     /* 1 or 2 interleaved rays per lane */
+} prr_launch_config;
+
+/* ---- lifetime (replaces prr.cpp:main 345-404, init 203-227) ---- */
+int prr_abi_version(void);
+const char *prr_status_string(prr_status s);
+/* Creates a context on CUDA device `device`; fails with PRR_ERR_NO_DEVICE
+ * when no device is usable. */
+prr_status prr_create(int device, prr_ctx **out);
+void prr_destroy(prr_ctx *ctx);
+const char *prr_last_error(const prr_ctx *ctx);
+
+/* ---- textures (replaces tex2d::load, cudamaths/tex2d.cuh:50-80) ----
+ * rgba8: w*h*4 bytes, row-major, row 0 first.  Texel value = byte/255 (the
+ * reference loads with stbi_ldr_to_hdr_gamma(1), cudamaths/image.cu:15).
+ * Alpha is ignored.  Re-uploading an id replaces it. */
+prr_status prr_upload_texture(prr_ctx *ctx, int id, const uint8_t *rgba8, int w, int h);
+
+/* ---- rendering (replaces prr.cpp:renderframe 237-341 and the frame loop
+ *      382-386) ----
+ * Renders n frames in one batched launch.  Outputs are concatenated per
+ * frame, each width*height pixels, row-major:
+ *   out_rgb8: 3 bytes/pixel, round(255*x) (cudamaths/image.cu:31), may be NULL
+ *   out_rgbf: 3 floats/pixel, the combined (and FXAA'd) colour, may be NULL
+ * Synchronous; host buffers. */
+prr_status prr_render(prr_ctx *ctx, const prr_frame_desc *frames, int n,
+                      uint8_t *out_rgb8, float *out_rgbf, prr_stats *stats);
+
+/* Same, with DEVICE output buffers, asynchronous on `stream` (a
+ * cudaStream_t, NULL = legacy default stream).  `frames` is read before the
+ * call returns.  Stats are not produced. */
+prr_status prr_render_device(prr_ctx *ctx, const prr_frame_desc *frames, int n,
+                             uint8_t *d_rgb8, float *d_rgbf, void *stream);
+
+/* Per-ray final states of one frame, for parity checks (the Ray struct of
+ * main/base.h:172-176 after trace_RKF, solver.cuh:142-219, and after
+ * rayToRGB, metrics/schwarzschild.cuh:151-183).  Host buffers, may be NULL:
+ *   out_state: 12 floats/ray = uv.x uv.y result r.x r.y r.z r.w u.x u.y u.z
+ *              u.w accepted_steps
+ *   out_rgb:   3 floats/ray, the per-sample colour
+ * Ray order is the reference's: ((y*width + x)*samples + sample). */
+prr_status prr_trace_rays(prr_ctx *ctx, const prr_frame_desc *frame,
+                          float *out_state, float *out_rgb, prr_stats *stats);
+
+/* FP64 variant of prr_trace_rays (state in doubles), PHYSICAL mode only. */
+prr_status prr_trace_rays_f64(prr_ctx *ctx, const prr_frame_desc *frame,
+                              double *out_state, double *out_rgb, prr_stats *stats);
+
+/* ---- scheduler tuning (new) ---- */
+prr_status prr_set_schedule(prr_ctx *ctx, int schedule, const prr_launch_config *cfg);
+prr_status prr_get_launch_config(prr_ctx *ctx, prr_launch_config *cfg);
+/* Times candidate launch shapes on `frame` and keeps the fastest. */
+prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, prr_launch_config *best);
+
+/* Context options (values for prr_set_option). */
+#define PRR_OPT_GEOD_TABLE 1      /* 1: persistent kernel uses the Christoffel-table geodesic (A/B runs) */
+#define PRR_OPT_WATCHDOG_CYCLES 2 /* >0: persistent kernels stop after this many SM clock cycles and the
+                                     call returns PRR_ERR_TIMEOUT; 0: off (default) */
+prr_status prr_set_option(prr_ctx *ctx, int option, long long value);
+
+/* Measures FP32 and FP64 FMA throughput (TFLOP/s) of the context's device
+ * with a dependent-chain FMA kernel; either pointer may be NULL. */
+prr_status prr_measure_peak(prr_ctx *ctx, double *fp32_tflops, double *fp64_tflops);
+
+/* ---- host helpers (no GPU needed) ---- */
+/* Seeded procedural RGBA8 textures.  kind 0: sphere texture (checkerboard +
+ * value noise); kind 1: equirectangular starfield (Poisson point stars with
+ * log-normal brightness on a dark gradient). */
+prr_status prr_make_texture(int kind, uint32_t seed, int w, int h, uint8_t *out_rgba8);
+/* Fills `d` with the defaults used where a deck is silent. */
+void prr_frame_desc_defaults(prr_frame_desc *d);
+/* sizeof of the ABI structs, for binding checks: 0 prr_frame_desc,
+ * 1 prr_stats, 2 prr_launch_config, 3 prr_sphere; 0 for other values. */
+size_t prr_sizeof(int which);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PRR_H */

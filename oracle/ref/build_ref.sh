@@ -1,0 +1,91 @@
+#!/usr/bin/env bash
+# Builds the reference ParRelRay solver as a host C++/OpenMP shared library
+# (the CPU oracle, test infrastructure only).  Reads the reference sources
+# from $PRR_REFERENCE (default /root/reference), writes ONLY into
+# oracle/_ref/ (git-ignored).  The reference's own build (compile.bat) is not
+# used: its sources are compiled directly with g++.
+#
+# The shipped reference does not compile as-is.  Three of its defects are
+# supplied by oracle/ref/ref_driver.cpp without touching the sources (the
+# lowercase ray/tracer names, the undefined fx(), the undeclared `frames`).
+# The recipe applies exactly three mechanical edits to its private copy:
+#   1. cudamaths/tex2d.cuh:121-128 - delete the non-const operator[](f2),
+#      which returns a reference to a temporary (a hard error); the const
+#      overload at tex2d.cuh:112-119 with the same body stays and is the one
+#      every caller uses.
+#   2. prr.cpp - rewrite each `k<<<grid, block>>>(args);` launch as
+#      `prr_ref_launch(grid, block, [&]{ k(args); });` (host emulation).
+#   3. main/metric.h - the reference's compile-time metric selection point;
+#      replaced by a switch over PRR_REF_METRIC_{SCHW,FLAT,KERR}.  SCHW and
+#      FLAT select the reference's own headers; KERR selects the Kerr-Schild
+#      plug-in header shipped by this repository in the reference's plug-in
+#      shape (parrelray_b200/compat/metrics/kerr.cuh), since the reference's
+#      metrics/kerr.cuh is a stub whose hooks do not match the solver.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REPO="$(cd "$HERE/../.." && pwd)"
+REF="${PRR_REFERENCE:-/root/reference}"
+OUT="$REPO/oracle/_ref"
+if [ ! -f "$REF/kernels/solver.cuh" ]; then
+    echo "build_ref.sh: reference sources not found at $REF" >&2
+    exit 2
+fi
+rm -rf "$OUT/src"
+mkdir -p "$OUT/src"
+for d in main kernels metrics scene cudamaths stb; do
+    cp -r "$REF/$d" "$OUT/src/$d"
+done
+cp "$REF/prr.cpp" "$OUT/src/prr.cpp"
+
+# 1. drop the non-const bilinear operator[](f2) (reference-to-temporary)
+python3 - "$OUT/src/cudamaths/tex2d.cuh" <<'PY'
+import sys, re
+p = sys.argv[1]
+s = open(p, encoding="utf-8-sig").read()
+pat = re.compile(r"\t__device__ inline f3 &operator\[\]\(f2 uv\) \{.*?\n\t\}\n", re.S)
+s2, n = pat.subn("", s, count=1)
+assert n == 1, "tex2d.cuh: non-const operator[](f2) not found"
+open(p, "w", encoding="utf-8").write(s2)
+PY
+
+# 2. host emulation of kernel launches
+python3 - "$OUT/src/prr.cpp" <<'PY'
+import sys, re
+p = sys.argv[1]
+s = open(p, encoding="utf-8-sig").read()
+pat = re.compile(r"(\w+)<<<\s*([^,>]+?)\s*,\s*([^>]+?)\s*>>>\((.*?)\);")
+s2, n = pat.subn(lambda m: f"prr_ref_launch({m.group(2)}, {m.group(3)}, [&] {{ {m.group(1)}({m.group(4)}); }});", s)
+assert n == 7, f"prr.cpp: expected 7 kernel launches, rewrote {n}"
+open(p, "w", encoding="utf-8").write(s2)
+PY
+
+# 3. metric selection
+mkdir -p "$OUT/src/compat"
+cp "$REPO/parrelray_b200/compat/metrics/kerr.cuh" "$OUT/src/compat/kerr_plugin.cuh"
+cat > "$OUT/src/main/metric.h" <<'EOF'
+#pragma once
+#if defined(PRR_REF_METRIC_FLAT)
+#include "../metrics/flat.cuh"
+#elif defined(PRR_REF_METRIC_KERR)
+#include "../compat/kerr_plugin.cuh"
+#else
+#include "../metrics/schwarzschild.cuh"
+#endif
+EOF
+
+# $CXX may point at a toolchain without libgomp; the system g++ has it.
+CXX="${PRR_ORACLE_CXX:-g++}"
+CXXFLAGS=(-O2 -std=c++17 -fopenmp -fPIC -ffp-contract=off -w -I "$HERE/shim" -I "$OUT/src")
+build_one() {
+    local tag="$1" def="$2"
+    "$CXX" "${CXXFLAGS[@]}" -D"$def" -shared -o "$OUT/libprr_ref_${tag}.so" \
+        -x c++ "$HERE/ref_driver.cpp" \
+        -x c++ "$OUT/src/main/Spacetime.cpp" \
+        -x c++ "$OUT/src/main/Camera.cpp" \
+        -x c++ "$OUT/src/main/Parameters.cpp" \
+        -x c++ "$OUT/src/cudamaths/image.cu"
+}
+build_one schw PRR_REF_METRIC_SCHW
+build_one flat PRR_REF_METRIC_FLAT
+build_one kerr PRR_REF_METRIC_KERR
+echo "built: $(ls "$OUT"/libprr_ref_*.so | tr '\n' ' ')"

@@ -1,0 +1,133 @@
+"""prr-b200: B200-native ParRelRay hot path (geodesic ray tracing through
+flat / Schwarzschild / Kerr spacetimes, textured spheres, SSAA and FXAA).
+
+The product is the C ABI of include/prr.h, implemented by
+_lib/libprr_b200.so (CUDA for sm_100a).  This package is a thin Python view
+of that ABI (numpy in, numpy out) plus the workload builders in scenes.py.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .abi import FrameDesc, LaunchConfig, PrrError, Stats
+
+__all__ = ["Context", "FrameDesc", "LaunchConfig", "PrrError", "Stats", "abi"]
+
+
+def _frames_array(frames) -> tuple[C.Array, list[FrameDesc]]:
+    if isinstance(frames, FrameDesc):
+        frames = [frames]
+    frames = list(frames)
+    arr = (FrameDesc * len(frames))(*frames)
+    return arr, frames
+
+
+class Context:
+    """One device context (prr_create/prr_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = abi.load()
+        h = C.c_void_p()
+        st = self.lib.prr_create(device, C.byref(h))
+        if st != abi.OK:
+            raise PrrError(st, self.lib.prr_status_string(st).decode())
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.prr_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int) -> None:
+        abi.check(st, self.h)
+
+    def upload_texture(self, tex_id: int, rgba8: np.ndarray) -> None:
+        a = np.ascontiguousarray(rgba8, dtype=np.uint8)
+        if a.ndim != 3 or a.shape[2] != 4:
+            raise ValueError("texture must be an (h, w, 4) uint8 array")
+        self._check(self.lib.prr_upload_texture(self.h, tex_id, a.ctypes.data_as(abi._u8p), a.shape[1], a.shape[0]))
+
+    def upload_textures(self, textures: dict[int, np.ndarray]) -> None:
+        for k, v in textures.items():
+            self.upload_texture(k, v)
+
+    def set_schedule(self, schedule: int, cfg: LaunchConfig | None = None) -> None:
+        self._check(self.lib.prr_set_schedule(self.h, schedule, C.byref(cfg) if cfg else None))
+
+    def launch_config(self) -> LaunchConfig:
+        cfg = LaunchConfig()
+        self._check(self.lib.prr_get_launch_config(self.h, C.byref(cfg)))
+        return cfg
+
+    def set_option(self, option: int, value: int) -> None:
+        self._check(self.lib.prr_set_option(self.h, option, value))
+
+    def autotune(self, frame: FrameDesc) -> LaunchConfig:
+        cfg = LaunchConfig()
+        self._check(self.lib.prr_autotune(self.h, C.byref(frame), C.byref(cfg)))
+        return cfg
+
+    def measure_peak(self) -> tuple[float, float]:
+        f32, f64 = C.c_double(), C.c_double()
+        self._check(self.lib.prr_measure_peak(self.h, C.byref(f32), C.byref(f64)))
+        return f32.value, f64.value
+
+    def render(self, frames, want_float: bool = False):
+        """Renders one or more frames; returns (list of uint8 (h, w, 3)
+        images, list of float32 images or None, Stats)."""
+        arr, fl = _frames_array(frames)
+        npx = sum(f.width * f.height for f in fl)
+        out8 = np.empty(npx * 3, dtype=np.uint8)
+        outf = np.empty(npx * 3, dtype=np.float32) if want_float else None
+        stats = Stats()
+        self._check(self.lib.prr_render(self.h, arr, len(fl), out8.ctypes.data_as(abi._u8p),
+                                        outf.ctypes.data_as(abi._fp) if want_float else None, C.byref(stats)))
+        imgs8, imgsf, off = [], [], 0
+        for f in fl:
+            n = f.width * f.height * 3
+            imgs8.append(out8[off:off + n].reshape(f.height, f.width, 3))
+            if want_float:
+                imgsf.append(outf[off:off + n].reshape(f.height, f.width, 3))
+            off += n
+        return imgs8, (imgsf if want_float else None), stats
+
+    def render_device(self, frames, d_rgb8: int, d_rgbf: int | None = None, stream: int | None = None) -> None:
+        """Asynchronous render into device buffers (raw CUDA pointers)."""
+        arr, fl = _frames_array(frames)
+        self._check(self.lib.prr_render_device(self.h, arr, len(fl), C.c_void_p(d_rgb8),
+                                               C.c_void_p(d_rgbf) if d_rgbf else None,
+                                               C.c_void_p(stream) if stream else None))
+
+    def trace_rays(self, frame: FrameDesc):
+        """Per-ray final states (n, 12) float32 and per-sample colours (n, 3)."""
+        n = frame.nrays
+        state = np.empty((n, 12), dtype=np.float32)
+        rgb = np.empty((n, 3), dtype=np.float32)
+        stats = Stats()
+        self._check(self.lib.prr_trace_rays(self.h, C.byref(frame), state.ctypes.data_as(abi._fp),
+                                            rgb.ctypes.data_as(abi._fp), C.byref(stats)))
+        return state, rgb, stats
+
+    def trace_rays_f64(self, frame: FrameDesc):
+        n = frame.nrays
+        state = np.empty((n, 12), dtype=np.float64)
+        rgb = np.empty((n, 3), dtype=np.float64)
+        stats = Stats()
+        self._check(self.lib.prr_trace_rays_f64(self.h, C.byref(frame), state.ctypes.data_as(abi._dp),
+                                                rgb.ctypes.data_as(abi._dp), C.byref(stats)))
+        return state, rgb, stats

@@ -1,0 +1,144 @@
+"""ctypes view of include/prr.h and the loader of libprr_b200.so.
+
+Every struct here mirrors include/prr.h field for field; tests compare
+ctypes.sizeof() with the library's prr_sizeof().  The library is loaded from
+the package's _lib/ directory (built in-tree by parrelray_b200.build); a
+missing library raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "_lib" / "libprr_b200.so"
+HEADER = PKG.parent / "include" / "prr.h"
+
+PRR_MAX_SPHERES = 8
+PRR_MAX_TEXTURES = 32
+
+# prr_status
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_TIMEOUT, ERR_IO, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(8)
+# prr_result (main/base.h:37-43)
+RESULT_SUCCESS, RESULT_MATH_ERROR, RESULT_IO_ERROR, RESULT_INFINITE_GEO, RESULT_INTERSECTION = range(5)
+SOLVER_EULER, SOLVER_RKF45 = 0, 2
+SSAA_NONE, SSAA_REGULAR = 0, 1
+METRIC_FLAT, METRIC_SCHWARZSCHILD, METRIC_KERR = 0, 1, 2
+MODE_REFERENCE, MODE_PHYSICAL = 0, 1
+PREC_FP32, PREC_FP64, PREC_SPLIT = 0, 1, 2
+SCHED_PLAIN, SCHED_PERSISTENT = 0, 1
+BG_RMS2X2, BG_BILINEAR = 0, 1
+OPT_GEOD_TABLE, OPT_WATCHDOG_CYCLES = 1, 2
+
+
+class Sphere(C.Structure):
+    _fields_ = [("center", C.c_float * 3), ("radius", C.c_float), ("texture_id", C.c_int32), ("_pad", C.c_int32 * 3)]
+
+
+class FrameDesc(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32), ("ssaa", C.c_int32), ("samples", C.c_int32),
+        ("vfov", C.c_float), ("cam_pos", C.c_float * 3), ("cam_alpha", C.c_float), ("cam_beta", C.c_float),
+        ("metric", C.c_int32), ("mass", C.c_float), ("spin", C.c_float),
+        ("solver", C.c_int32), ("mode", C.c_int32), ("precision", C.c_int32),
+        ("h", C.c_float), ("hmin", C.c_float), ("hmax", C.c_float), ("eps", C.c_float),
+        ("rtol", C.c_float), ("atol", C.c_float), ("rout", C.c_float), ("horizon_eps", C.c_float),
+        ("max_steps", C.c_int32), ("background_id", C.c_int32), ("bg_filter", C.c_int32), ("fxaa", C.c_int32),
+        ("fp64_delta", C.c_float), ("fp64_rfac", C.c_float),
+        ("nspheres", C.c_int32), ("_pad0", C.c_int32),
+        ("spheres", Sphere * PRR_MAX_SPHERES),
+    ]
+
+    @property
+    def nrays(self) -> int:
+        return self.width * self.height * self.samples
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("rays", C.c_int64), ("attempts", C.c_int64), ("accepted", C.c_int64), ("n_escaped", C.c_int64),
+        ("n_captured", C.c_int64), ("n_intersection", C.c_int64), ("n_infinite", C.c_int64),
+        ("n_math_error", C.c_int64), ("n_fp64", C.c_int64), ("kernel_ms", C.c_double), ("kernel_launches", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LaunchConfig(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("compaction_interval", C.c_int32),
+                ("rays_per_thread", C.c_int32)]
+
+
+_P = C.c_void_p
+_u8p = C.POINTER(C.c_uint8)
+_fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "prr_abi_version": (C.c_int, []),
+    "prr_status_string": (C.c_char_p, [C.c_int]),
+    "prr_create": (C.c_int, [C.c_int, C.POINTER(_P)]),
+    "prr_destroy": (None, [_P]),
+    "prr_last_error": (C.c_char_p, [_P]),
+    "prr_upload_texture": (C.c_int, [_P, C.c_int, _u8p, C.c_int, C.c_int]),
+    "prr_render": (C.c_int, [_P, C.POINTER(FrameDesc), C.c_int, _u8p, _fp, C.POINTER(Stats)]),
+    "prr_render_device": (C.c_int, [_P, C.POINTER(FrameDesc), C.c_int, _P, _P, _P]),
+    "prr_trace_rays": (C.c_int, [_P, C.POINTER(FrameDesc), _fp, _fp, C.POINTER(Stats)]),
+    "prr_trace_rays_f64": (C.c_int, [_P, C.POINTER(FrameDesc), _dp, _dp, C.POINTER(Stats)]),
+    "prr_set_schedule": (C.c_int, [_P, C.c_int, C.POINTER(LaunchConfig)]),
+    "prr_get_launch_config": (C.c_int, [_P, C.POINTER(LaunchConfig)]),
+    "prr_autotune": (C.c_int, [_P, C.POINTER(FrameDesc), C.POINTER(LaunchConfig)]),
+    "prr_set_option": (C.c_int, [_P, C.c_int, C.c_longlong]),
+    "prr_measure_peak": (C.c_int, [_P, _dp, _dp]),
+    "prr_make_texture": (C.c_int, [C.c_int, C.c_uint32, C.c_int, C.c_int, _u8p]),
+    "prr_frame_desc_defaults": (None, [C.POINTER(FrameDesc)]),
+    "prr_sizeof": (C.c_size_t, [C.c_int]),
+}
+
+_lib = None
+
+
+class PrrError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"prr status {status}: {message}")
+        self.status = status
+
+
+def load(path: str | Path | None = None) -> C.CDLL:
+    """Loads the library (once) and declares every signature."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} not built: run `python -m parrelray_b200.build`")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def header_functions(header: Path = HEADER) -> list[str]:
+    """Names of the functions include/prr.h declares."""
+    text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(prr_[a-z0-9_]+)\s*\(", text)) - {"prr_ctx"})
+
+
+def check(status: int, ctx=None) -> None:
+    if status != OK:
+        lib = load()
+        msg = lib.prr_last_error(ctx).decode() if ctx else lib.prr_status_string(status).decode()
+        raise PrrError(status, msg or lib.prr_status_string(status).decode())
+
+
+def defaults() -> FrameDesc:
+    d = FrameDesc()
+    load().prr_frame_desc_defaults(C.byref(d))
+    return d

@@ -1,0 +1,131 @@
+"""Builds libprr_b200.so (CUDA for sm_100a + host C++) in-tree.
+
+    python -m parrelray_b200.build            # library
+    python -m parrelray_b200.build --oracle   # + CPU oracle (tests only)
+
+nvcc cross-compiles for sm_100a without a GPU.  Objects go to
+parrelray_b200/_build/, the library to parrelray_b200/_lib/.  Sources whose
+FP32 operation order must match the reference's (the REFERENCE-mode tracer and
+the SSAA/FXAA pass) are built with -fmad=false.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+REPO = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIBDIR = PKG / "_lib"
+LIB = LIBDIR / "libprr_b200.so"
+INCLUDE = REPO / "include"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NO_FMAD = {"k_reference.cu", "post.cu"}
+CU_SOURCES = ["capi.cu", "render.cu", "k_reference.cu", "post.cu", "k_persistent.cu", "k_plain.cu", "fma_peak.cu"]
+CPP_SOURCES = ["textures.cpp"]
+
+
+def nvcc() -> str:
+    cand = os.environ.get("NVCC") or shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return cand
+
+
+def _newer(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return False
+    t = target.stat().st_mtime
+    return all(d.stat().st_mtime <= t for d in deps if d.exists())
+
+
+def _headers() -> list[Path]:
+    return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _run(cmd: list[str], verbose: bool) -> None:
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_library(verbose: bool = False, ptxas_verbose: bool = False) -> Path:
+    BUILD.mkdir(parents=True, exist_ok=True)
+    LIBDIR.mkdir(parents=True, exist_ok=True)
+    hdrs = _headers()
+    objs: list[Path] = []
+    for src in CU_SOURCES:
+        s = CSRC / src
+        o = BUILD / (src + ".o")
+        objs.append(o)
+        if _newer(o, [s] + hdrs) and not ptxas_verbose:
+            continue
+        cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+               "-I", str(INCLUDE), "-I", str(CSRC), "-c", str(s), "-o", str(o)]
+        if src in NO_FMAD:
+            cmd.insert(1, "-fmad=false")
+        if ptxas_verbose:
+            cmd += ["-Xptxas", "-v"]
+        _run(cmd, verbose)
+    for src in CPP_SOURCES:
+        s = CSRC / src
+        o = BUILD / (src + ".o")
+        objs.append(o)
+        if _newer(o, [s] + hdrs):
+            continue
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-I", str(INCLUDE), "-c", str(s), "-o", str(o)], verbose)
+    if not _newer(LIB, objs):
+        _run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs)], verbose)
+    return LIB
+
+
+ORACLE_DIR = REPO / "oracle"
+ORACLE_BUILD = ORACLE_DIR / "_build"
+ORACLE_LIB = ORACLE_BUILD / "libprr_oracle.so"
+
+
+def build_oracle(verbose: bool = False) -> Path:
+    """CPU restatement (test infrastructure).  System g++ (has libgomp)."""
+    ORACLE_BUILD.mkdir(parents=True, exist_ok=True)
+    src = ORACLE_DIR / "prr_oracle.cpp"
+    if not _newer(ORACLE_LIB, [src, INCLUDE / "prr.h"]):
+        _run(["g++", "-O2", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
+              "-I", str(INCLUDE), str(src), "-o", str(ORACLE_LIB)], verbose)
+    return ORACLE_LIB
+
+
+def build_reference(verbose: bool = False) -> bool:
+    """Reference sources compiled for the host (oracle/_ref); needs the
+    reference tree, so only where it is mounted."""
+    ref = Path(os.environ.get("PRR_REFERENCE", "/root/reference"))
+    if not (ref / "kernels" / "solver.cuh").exists():
+        return False
+    out = ORACLE_DIR / "_ref"
+    libs = [out / f"libprr_ref_{t}.so" for t in ("schw", "flat", "kerr")]
+    deps = [ORACLE_DIR / "ref" / "build_ref.sh", ORACLE_DIR / "ref" / "ref_driver.cpp",
+            PKG / "compat" / "metrics" / "kerr.cuh"] + sorted((ORACLE_DIR / "ref" / "shim").glob("*.h"))
+    if all(_newer(l, deps) for l in libs):
+        return True
+    _run(["bash", str(ORACLE_DIR / "ref" / "build_ref.sh")], verbose)
+    return True
+
+
+def main(argv: list[str] | None = None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--oracle", action="store_true", help="also build the CPU oracle and the reference host build")
+    ap.add_argument("-v", "--verbose", action="store_true")
+    ap.add_argument("--ptxas", action="store_true", help="rebuild with -Xptxas -v (register/spill report)")
+    a = ap.parse_args(argv)
+    build_library(a.verbose, a.ptxas)
+    if a.oracle:
+        build_oracle(a.verbose)
+        build_reference(a.verbose)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

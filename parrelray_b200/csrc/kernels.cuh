@@ -1,0 +1,80 @@
+// kernels.cuh - host-visible launch wrappers of every kernel in the library
+// (each defined in the .cu file named beside it).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "prr_device.cuh"
+
+namespace prr {
+
+// Device counters accumulated by the tracing kernels.
+enum Counter {
+    C_RAYS = 0,
+    C_ATTEMPTS,
+    C_ACCEPTED,
+    C_ESCAPED,
+    C_CAPTURED,
+    C_INTERSECTION,
+    C_INFINITE,
+    C_MATH_ERROR,
+    C_FP64,
+    C_WORK,          // persistent scheduler: next work item
+    C_WORK_FP64,     // split precision: next FP64 work item
+    C_FP64_QUEUED,   // split precision: queue length
+    C_TIMEOUT,       // watchdog fired
+    C_COUNT = 16
+};
+
+// k_reference.cu: REFERENCE-mode tracing, one thread per ray of frame
+// `frame` (rays [0, nrays)).  state: 12 floats/ray, rgb: 3 floats/ray (either
+// may be null).
+cudaError_t launch_ref_trace(const FrameParams *d_fp, int frame, long long nrays, float *state, float *rgb,
+                             unsigned long long *counters, cudaStream_t st);
+
+// post.cu: SSAA combine of per-sample colours into an FP32 image.
+cudaError_t launch_combine(const float *rgb, int w, int h, int samples, float *image, cudaStream_t st);
+// post.cu: FXAA (optional) + quantise.  Writes out_f (FP32, may be null) and
+// out_u8 (3 bytes/pixel, may be null).  in and out_f must differ when fxaa.
+cudaError_t launch_finish(const float *image, int w, int h, int fxaa, float *out_f, uint8_t *out_u8, cudaStream_t st);
+
+// k_persistent.cu: PHYSICAL-mode persistent renderer over a batch of frames.
+struct PersistentArgs {
+    const FrameParams *frames;   // device array
+    const long long *frame_pix_begin;  // device array, nframes+1 prefix of pixel counts
+    int nframes;
+    long long total_pixels;      // work items (pixels over all frames)
+    float *image;                // combined FP32 image, 3 floats/pixel (all frames)
+    uint8_t *rgb8;               // optional direct quantised output (frames without FXAA)
+    float *sample_rgb;           // per-sample colours (split precision; optional otherwise)
+    unsigned long long *fp64_queue;  // split precision: flagged ray ids
+    long long fp64_capacity;
+    unsigned long long *counters;
+    float *ray_state;            // optional per-ray debug state, 12 floats/ray (single frame)
+    double *ray_state64;         // optional per-ray debug state, 12 doubles/ray (FP64, single frame)
+    int geod_table;              // 1 = Christoffel-table geodesic (for comparisons)
+    int compaction_interval;     // attempts between warp refills (>= 1)
+    long long watchdog_cycles;   // 0 = off
+};
+cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st);
+
+// k_persistent.cu: resident CTAs per SM of the persistent kernel variant.
+int persistent_occupancy(int precision, int geod_table, int block);
+
+// k_persistent.cu: FP64 re-integration of the queued rays of a split render.
+cudaError_t launch_fp64_requeue(const PersistentArgs &a, int block, int nsm, cudaStream_t st);
+
+// k_plain.cu: the reference's pipeline structure with PHYSICAL math.
+struct PlainBuffers {
+    void *rays;      // AoS ray records, one per sample
+    float *rgb;      // per-sample colours
+};
+cudaError_t launch_plain_frame(const FrameParams *d_fp, const FrameParams &h_fp, int frame, PlainBuffers &b,
+                               unsigned long long *counters, int geod_table, cudaStream_t st, int *launches);
+size_t plain_ray_record_bytes();
+
+// fma_peak.cu
+cudaError_t launch_fma_peak(float *sink, int blocks, int threads, int iters, cudaStream_t st);
+cudaError_t launch_dfma_peak(double *sink, int blocks, int threads, int iters, cudaStream_t st);
+
+}  // namespace prr

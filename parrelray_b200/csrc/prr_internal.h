@@ -1,0 +1,65 @@
+// prr_internal.h - the context behind the C ABI and the render plan that
+// turns an array of prr_frame_desc into launches.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "prr.h"
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    prr_status ensure(size_t bytes);  // grow-only
+    void release();
+};
+
+struct TexSlot {
+    DevBuf buf;
+    int w = 0, h = 0;
+};
+
+struct prr_ctx {
+    int device = 0;
+    int nsm = 0;
+    int sm_clock_khz = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::string err;
+    TexSlot tex[PRR_MAX_TEXTURES];
+    int schedule = PRR_SCHED_PERSISTENT;
+    prr_launch_config cfg{};
+    int geod_table = 0;
+    long long watchdog_cycles = 0;
+    int last_launches = 0;
+    float last_ms = 0.f;
+    // device scratch, grown on demand and reused across calls
+    DevBuf frames, frame_begin, counters, image, sample_rgb, rays, queue, state, out_u8, out_f, scratch;
+    std::vector<DevBuf *> all_buffers()
+    {
+        return {&frames, &frame_begin, &counters, &image, &sample_rgb, &rays, &queue, &state, &out_u8, &out_f, &scratch};
+    }
+};
+
+// Host-side description of one render call.
+struct RenderPlan {
+    std::vector<prr::FrameParams> fp;
+    std::vector<long long> pix_begin;  // nframes + 1
+    std::vector<long long> ray_begin;  // nframes + 1
+    long long total_pixels = 0;
+    long long total_rays = 0;
+    int mode = PRR_MODE_PHYSICAL;
+    int precision = PRR_PREC_FP32;
+    bool any_fxaa = false;
+};
+
+// render.cu
+prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderPlan &plan);
+// Runs a plan into device outputs (either may be null).  When `timed`, the
+// device time between two events around the launches is kept in ctx->last_ms.
+prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float *d_rgbf, cudaStream_t st, bool timed);
+// Single frame: per-ray states and per-sample colours to host buffers.
+prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, double *h_state64, float *h_rgb);
+prr_status collect_stats(prr_ctx *ctx, const RenderPlan &plan, prr_stats *stats);

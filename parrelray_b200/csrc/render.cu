@@ -1,0 +1,382 @@
+// render.cu - frame validation, the render plan and its execution on the
+// REFERENCE, PLAIN and PERSISTENT paths, ray-state readback, stats and the
+// launch-shape autotuner.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "prr_internal.h"
+
+using namespace prr;
+
+#define PRR_CK(ctx, expr)                                                                                  \
+    do {                                                                                                   \
+        cudaError_t _e = (expr);                                                                           \
+        if (_e != cudaSuccess) {                                                                           \
+            (ctx)->err = std::string(#expr) + ": " + cudaGetErrorString(_e);                               \
+            return PRR_ERR_CUDA;                                                                           \
+        }                                                                                                  \
+    } while (0)
+
+namespace {
+
+prr_status bad(prr_ctx *ctx, int f, const std::string &msg)
+{
+    ctx->err = "frame " + std::to_string(f) + ": " + msg;
+    return PRR_ERR_INVALID;
+}
+
+bool finite_pos(float v) { return std::isfinite(v) && v > 0.0f; }
+
+DevTex dev_tex(prr_ctx *ctx, int id)
+{
+    DevTex t{nullptr, 0, 0};
+    if (id >= 0 && id < PRR_MAX_TEXTURES && ctx->tex[id].buf.p) {
+        t.p = (const uint32_t *)ctx->tex[id].buf.p;
+        t.w = ctx->tex[id].w;
+        t.h = ctx->tex[id].h;
+    }
+    return t;
+}
+
+prr_status alloc(prr_ctx *ctx, DevBuf &b, size_t bytes, const char *what)
+{
+    if (b.ensure(bytes) != PRR_OK) {
+        ctx->err = std::string("out of device memory for ") + what + " (" + std::to_string(bytes) + " bytes)";
+        return PRR_ERR_NOMEM;
+    }
+    return PRR_OK;
+}
+
+int resolve_bpsm(prr_ctx *ctx, int precision)
+{
+    if (ctx->cfg.blocks_per_sm > 0) return ctx->cfg.blocks_per_sm;
+    int b = persistent_occupancy(precision, ctx->geod_table, ctx->cfg.block_size);
+    return b > 0 ? b : 1;
+}
+
+}  // namespace
+
+prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderPlan &plan)
+{
+    if (!frames || n < 1 || n > (1 << 22)) { ctx->err = "need 1 <= n <= 4194304 frames and a non-null array"; return PRR_ERR_INVALID; }
+    plan.fp.resize(n);
+    plan.pix_begin.assign(n + 1, 0);
+    plan.ray_begin.assign(n + 1, 0);
+    plan.mode = frames[0].mode;
+    plan.precision = frames[0].precision;
+    plan.any_fxaa = false;
+    for (int f = 0; f < n; f++) {
+        const prr_frame_desc &d = frames[f];
+        FrameParams &p = plan.fp[f];
+        memset(&p, 0, sizeof(p));
+        if (d.mode != plan.mode || d.precision != plan.precision) return bad(ctx, f, "all frames of one call need the same mode and precision");
+        if (d.width < 1 || d.height < 1 || d.width > 65536 || d.height > 65536) return bad(ctx, f, "width/height must be in [1, 65536]");
+        if (d.samples < 1 || d.samples > 64) return bad(ctx, f, "samples must be in [1, 64]");
+        if (d.ssaa == PRR_SSAA_NONE) {
+            if (d.samples != 1) return bad(ctx, f, "SSAA none needs samples == 1");
+            p.nsub = 1;
+        } else if (d.ssaa == PRR_SSAA_REGULAR) {
+            int q = (int)std::lround(std::sqrt((double)d.samples));
+            if (q * q != d.samples) return bad(ctx, f, "SSAA regular needs a perfect-square sample count (kernels/ssaa.cuh:41)");
+            p.nsub = q;
+        } else return bad(ctx, f, "unknown SSAA distribution (only none and regular are implemented, as in prr.cpp:261-273)");
+        if (!finite_pos(d.vfov) || d.vfov >= 6.3f) return bad(ctx, f, "vfov must be in (0, 2*pi) radians");
+        for (int k = 0; k < 3; k++) if (!std::isfinite(d.cam_pos[k])) return bad(ctx, f, "camera position is not finite");
+        if (!std::isfinite(d.cam_alpha) || !std::isfinite(d.cam_beta)) return bad(ctx, f, "camera angles are not finite");
+        if (d.metric < PRR_METRIC_FLAT || d.metric > PRR_METRIC_KERR) return bad(ctx, f, "unknown metric");
+        if (!std::isfinite(d.mass) || d.mass < 0.0f) return bad(ctx, f, "mass must be >= 0");
+        if (d.metric != PRR_METRIC_FLAT && d.mass <= 0.0f) return bad(ctx, f, "Schwarzschild/Kerr need mass > 0");
+        if (d.metric == PRR_METRIC_KERR && !(std::fabs(d.spin) <= d.mass)) return bad(ctx, f, "Kerr needs |spin| <= mass");
+        if (d.solver != PRR_SOLVER_EULER && d.solver != PRR_SOLVER_RKF45) return bad(ctx, f, "solver must be euler (0) or rkf45 (2)");
+        if (d.mode != PRR_MODE_REFERENCE && d.mode != PRR_MODE_PHYSICAL) return bad(ctx, f, "unknown mode");
+        if (d.precision < PRR_PREC_FP32 || d.precision > PRR_PREC_SPLIT) return bad(ctx, f, "unknown precision");
+        if (d.mode == PRR_MODE_REFERENCE && d.precision != PRR_PREC_FP32) return bad(ctx, f, "REFERENCE mode is FP32 only");
+        if (d.mode == PRR_MODE_PHYSICAL && d.solver == PRR_SOLVER_EULER) return bad(ctx, f, "PHYSICAL mode integrates with rkf45 only");
+        if (!finite_pos(d.h) || !finite_pos(d.hmin) || !finite_pos(d.hmax) || d.hmin > d.hmax) return bad(ctx, f, "need 0 < hmin <= hmax and h > 0");
+        if (d.mode == PRR_MODE_REFERENCE && !finite_pos(d.eps)) return bad(ctx, f, "REFERENCE mode needs eps > 0");
+        if (d.mode == PRR_MODE_PHYSICAL && (!(d.rtol >= 0.0f) || !(d.atol >= 0.0f) || d.rtol + d.atol <= 0.0f)) return bad(ctx, f, "need rtol, atol >= 0, not both 0");
+        if (!finite_pos(d.rout)) return bad(ctx, f, "rout must be > 0");
+        if (!(d.horizon_eps >= 0.0f)) return bad(ctx, f, "horizon_eps must be >= 0");
+        if (d.max_steps < 1) return bad(ctx, f, "max_steps must be >= 1");
+        if (d.background_id >= PRR_MAX_TEXTURES || (d.background_id >= 0 && !ctx->tex[d.background_id].buf.p)) return bad(ctx, f, "background texture id not uploaded");
+        if (d.bg_filter != PRR_BG_RMS2X2 && d.bg_filter != PRR_BG_BILINEAR) return bad(ctx, f, "unknown background filter");
+        if (d.nspheres < 0 || d.nspheres > PRR_MAX_SPHERES) return bad(ctx, f, "nspheres must be in [0, PRR_MAX_SPHERES]");
+        for (int s = 0; s < d.nspheres; s++) {
+            const prr_sphere &S = d.spheres[s];
+            if (!finite_pos(S.radius) || !std::isfinite(S.center[0]) || !std::isfinite(S.center[1]) || !std::isfinite(S.center[2]))
+                return bad(ctx, f, "sphere " + std::to_string(s) + " has a bad centre or radius");
+            if (S.texture_id >= PRR_MAX_TEXTURES || (S.texture_id >= 0 && !ctx->tex[S.texture_id].buf.p))
+                return bad(ctx, f, "sphere " + std::to_string(s) + " texture id not uploaded");
+            p.sph[s] = {S.center[0], S.center[1], S.center[2], S.radius, dev_tex(ctx, S.texture_id)};
+        }
+        p.width = d.width; p.height = d.height; p.samples = d.samples; p.ssaa = d.ssaa;
+        p.vfov = d.vfov; p.cam[0] = d.cam_pos[0]; p.cam[1] = d.cam_pos[1]; p.cam[2] = d.cam_pos[2];
+        p.alpha = d.cam_alpha; p.beta = d.cam_beta;
+        p.metric = d.metric; p.M = d.mass; p.a = d.metric == PRR_METRIC_KERR ? d.spin : 0.0f;
+        p.rs = 2.0f * d.mass;  // Spacetime::setBhMass (main/Spacetime.h:23)
+        float rplus = d.metric == PRR_METRIC_KERR ? kerr_r_plus<float>(d.mass, d.spin) : (d.metric == PRR_METRIC_SCHWARZSCHILD ? p.rs : 0.0f);
+        p.rstop = rplus + d.horizon_eps;
+        p.rblack = rplus * 1.01f;
+        p.solver = d.solver; p.mode = d.mode; p.precision = d.precision;
+        p.h = d.h; p.hmin = d.hmin; p.hmax = d.hmax; p.eps = d.eps; p.rtol = d.rtol; p.atol = d.atol; p.rout = d.rout;
+        p.max_steps = d.max_steps;
+        p.bg_filter = d.bg_filter; p.fxaa = d.fxaa ? 1 : 0;
+        p.bg = dev_tex(ctx, d.background_id);
+        p.fp64_delta = d.precision == PRR_PREC_SPLIT ? d.fp64_delta : 0.0f;
+        p.fp64_rfac = d.precision == PRR_PREC_SPLIT ? d.fp64_rfac : 0.0f;
+        p.nspheres = d.nspheres;
+        long long npx = (long long)d.width * d.height;
+        p.pix_begin = plan.pix_begin[f];
+        p.ray_begin = plan.ray_begin[f];
+        plan.pix_begin[f + 1] = plan.pix_begin[f] + npx;
+        plan.ray_begin[f + 1] = plan.ray_begin[f] + npx * d.samples;
+        if (d.fxaa) plan.any_fxaa = true;
+    }
+    plan.total_pixels = plan.pix_begin[n];
+    plan.total_rays = plan.ray_begin[n];
+    if (plan.total_rays > (1LL << 38)) { ctx->err = "too many rays in one call"; return PRR_ERR_INVALID; }
+    return PRR_OK;
+}
+
+static prr_status upload_plan(prr_ctx *ctx, const RenderPlan &plan, cudaStream_t st)
+{
+    size_t n = plan.fp.size();
+    prr_status s;
+    if ((s = alloc(ctx, ctx->frames, n * sizeof(FrameParams), "frame parameters")) != PRR_OK) return s;
+    if ((s = alloc(ctx, ctx->frame_begin, (n + 1) * sizeof(long long), "frame table")) != PRR_OK) return s;
+    if ((s = alloc(ctx, ctx->counters, C_COUNT * sizeof(unsigned long long), "counters")) != PRR_OK) return s;
+    PRR_CK(ctx, cudaMemcpyAsync(ctx->frames.p, plan.fp.data(), n * sizeof(FrameParams), cudaMemcpyHostToDevice, st));
+    PRR_CK(ctx, cudaMemcpyAsync(ctx->frame_begin.p, plan.pix_begin.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+    PRR_CK(ctx, cudaMemsetAsync(ctx->counters.p, 0, C_COUNT * sizeof(unsigned long long), st));
+    // the host vectors may be freed when the caller returns: make the copies complete first
+    PRR_CK(ctx, cudaStreamSynchronize(st));
+    return PRR_OK;
+}
+
+static PersistentArgs persistent_args(prr_ctx *ctx, const RenderPlan &plan)
+{
+    PersistentArgs a;
+    memset(&a, 0, sizeof(a));
+    a.frames = (const FrameParams *)ctx->frames.p;
+    a.frame_pix_begin = (const long long *)ctx->frame_begin.p;
+    a.nframes = (int)plan.fp.size();
+    a.total_pixels = plan.total_pixels;
+    a.counters = (unsigned long long *)ctx->counters.p;
+    a.geod_table = ctx->geod_table;
+    a.compaction_interval = ctx->cfg.compaction_interval;
+    a.watchdog_cycles = ctx->watchdog_cycles;
+    return a;
+}
+
+prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float *d_rgbf, cudaStream_t st, bool timed)
+{
+    prr_status s = upload_plan(ctx, plan, st);
+    if (s != PRR_OK) return s;
+    const int n = (int)plan.fp.size();
+    unsigned long long *counters = (unsigned long long *)ctx->counters.p;
+    int launches = 0;
+    if ((s = alloc(ctx, ctx->image, (size_t)plan.total_pixels * 3 * sizeof(float), "image")) != PRR_OK) return s;
+    float *image = (float *)ctx->image.p;
+    if (timed) PRR_CK(ctx, cudaEventRecord(ctx->e0, st));
+    const FrameParams *d_fp = (const FrameParams *)ctx->frames.p;
+
+    auto finish = [&](int f, bool direct_done) -> prr_status {
+        const FrameParams &p = plan.fp[f];
+        float *img = image + 3 * p.pix_begin;
+        float *of = d_rgbf ? d_rgbf + 3 * p.pix_begin : nullptr;
+        uint8_t *o8 = d_rgb8 ? d_rgb8 + 3 * p.pix_begin : nullptr;
+        if (p.fxaa || !direct_done) {
+            PRR_CK(ctx, launch_finish(img, p.width, p.height, p.fxaa, of, o8, st));
+            launches++;
+        } else if (of) {
+            PRR_CK(ctx, cudaMemcpyAsync(of, img, (size_t)p.width * p.height * 3 * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        }
+        return PRR_OK;
+    };
+
+    if (plan.mode == PRR_MODE_REFERENCE || ctx->schedule == PRR_SCHED_PLAIN) {
+        long long max_rays = 0;
+        for (const auto &p : plan.fp) max_rays = std::max(max_rays, (long long)p.width * p.height * p.samples);
+        if ((s = alloc(ctx, ctx->sample_rgb, (size_t)max_rays * 3 * sizeof(float), "per-sample colours")) != PRR_OK) return s;
+        if (plan.mode != PRR_MODE_REFERENCE &&
+            (s = alloc(ctx, ctx->rays, (size_t)max_rays * plain_ray_record_bytes(), "ray records")) != PRR_OK) return s;
+        float *rgb = (float *)ctx->sample_rgb.p;
+        for (int f = 0; f < n; f++) {
+            const FrameParams &p = plan.fp[f];
+            long long nr = (long long)p.width * p.height * p.samples;
+            if (plan.mode == PRR_MODE_REFERENCE) {
+                PRR_CK(ctx, launch_ref_trace(d_fp, f, nr, nullptr, rgb, counters, st));
+                launches++;
+            } else {
+                PlainBuffers b{ctx->rays.p, rgb};
+                PRR_CK(ctx, launch_plain_frame(d_fp, p, f, b, counters, ctx->geod_table, st, &launches));
+            }
+            PRR_CK(ctx, launch_combine(rgb, p.width, p.height, p.samples, image + 3 * p.pix_begin, st));
+            launches++;
+            if ((s = finish(f, false)) != PRR_OK) return s;
+        }
+    } else {
+        PersistentArgs a = persistent_args(ctx, plan);
+        a.image = image;
+        const int bpsm = resolve_bpsm(ctx, plan.precision);
+        if (plan.precision == PRR_PREC_SPLIT) {
+            if ((s = alloc(ctx, ctx->sample_rgb, (size_t)plan.total_rays * 3 * sizeof(float), "per-sample colours")) != PRR_OK) return s;
+            if ((s = alloc(ctx, ctx->queue, (size_t)plan.total_rays * sizeof(unsigned long long), "FP64 queue")) != PRR_OK) return s;
+            a.sample_rgb = (float *)ctx->sample_rgb.p;
+            a.fp64_queue = (unsigned long long *)ctx->queue.p;
+            a.fp64_capacity = plan.total_rays;
+            PRR_CK(ctx, launch_persistent(a, PRR_PREC_SPLIT, ctx->cfg.block_size, bpsm, ctx->nsm, st));
+            PRR_CK(ctx, launch_fp64_requeue(a, 128, ctx->nsm, st));
+            launches += 2;
+            for (int f = 0; f < n; f++) {
+                const FrameParams &p = plan.fp[f];
+                PRR_CK(ctx, launch_combine(a.sample_rgb + 3 * p.ray_begin, p.width, p.height, p.samples, image + 3 * p.pix_begin, st));
+                launches++;
+                if ((s = finish(f, false)) != PRR_OK) return s;
+            }
+        } else {
+            a.rgb8 = d_rgb8;
+            PRR_CK(ctx, launch_persistent(a, plan.precision, ctx->cfg.block_size, bpsm, ctx->nsm, st));
+            launches++;
+            for (int f = 0; f < n; f++)
+                if ((s = finish(f, true)) != PRR_OK) return s;
+        }
+    }
+    if (timed) {
+        PRR_CK(ctx, cudaEventRecord(ctx->e1, st));
+        PRR_CK(ctx, cudaEventSynchronize(ctx->e1));
+        PRR_CK(ctx, cudaEventElapsedTime(&ctx->last_ms, ctx->e0, ctx->e1));
+    }
+    ctx->last_launches = launches;
+    if (ctx->watchdog_cycles > 0) {
+        unsigned long long flag = 0;
+        PRR_CK(ctx, cudaMemcpyAsync(&flag, counters + C_TIMEOUT, sizeof(flag), cudaMemcpyDeviceToHost, st));
+        PRR_CK(ctx, cudaStreamSynchronize(st));
+        if (flag) { ctx->err = "device watchdog expired: some rays were not finished"; return PRR_ERR_TIMEOUT; }
+    }
+    return PRR_OK;
+}
+
+prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, double *h_state64, float *h_rgb)
+{
+    cudaStream_t st = ctx->stream;
+    prr_status s = upload_plan(ctx, plan, st);
+    if (s != PRR_OK) return s;
+    const FrameParams &p = plan.fp[0];
+    const long long nr = (long long)p.width * p.height * p.samples;
+    unsigned long long *counters = (unsigned long long *)ctx->counters.p;
+    const FrameParams *d_fp = (const FrameParams *)ctx->frames.p;
+    size_t state_bytes = (size_t)nr * 12 * (h_state64 ? sizeof(double) : sizeof(float));
+    if ((s = alloc(ctx, ctx->state, state_bytes, "ray states")) != PRR_OK) return s;
+    if ((s = alloc(ctx, ctx->sample_rgb, (size_t)nr * 3 * sizeof(float), "per-sample colours")) != PRR_OK) return s;
+    float *rgb = (float *)ctx->sample_rgb.p;
+    PRR_CK(ctx, cudaEventRecord(ctx->e0, st));
+    if (plan.mode == PRR_MODE_REFERENCE) {
+        PRR_CK(ctx, launch_ref_trace(d_fp, 0, nr, (float *)ctx->state.p, rgb, counters, st));
+        ctx->last_launches = 1;
+    } else if (ctx->schedule == PRR_SCHED_PLAIN && !h_state64) {
+        if ((s = alloc(ctx, ctx->rays, (size_t)nr * plain_ray_record_bytes(), "ray records")) != PRR_OK) return s;
+        PlainBuffers b{ctx->rays.p, rgb};
+        int launches = 0;
+        PRR_CK(ctx, launch_plain_frame(d_fp, p, 0, b, counters, ctx->geod_table, st, &launches));
+        ctx->last_launches = launches;
+    } else {
+        if ((s = alloc(ctx, ctx->image, (size_t)plan.total_pixels * 3 * sizeof(float), "image")) != PRR_OK) return s;
+        PersistentArgs a = persistent_args(ctx, plan);
+        a.image = (float *)ctx->image.p;
+        a.sample_rgb = rgb;
+        if (h_state64) a.ray_state64 = (double *)ctx->state.p;
+        else a.ray_state = (float *)ctx->state.p;
+        int prec = plan.precision == PRR_PREC_FP64 ? PRR_PREC_FP64 : PRR_PREC_FP32;
+        PRR_CK(ctx, launch_persistent(a, prec, ctx->cfg.block_size, resolve_bpsm(ctx, prec), ctx->nsm, st));
+        ctx->last_launches = 1;
+    }
+    PRR_CK(ctx, cudaEventRecord(ctx->e1, st));
+    PRR_CK(ctx, cudaEventSynchronize(ctx->e1));
+    PRR_CK(ctx, cudaEventElapsedTime(&ctx->last_ms, ctx->e0, ctx->e1));
+    if (plan.mode != PRR_MODE_REFERENCE && ctx->schedule == PRR_SCHED_PLAIN && !h_state64) {
+        // ray records (48 B, main/base.h:172-176 layout) -> 12-float states
+        std::vector<float> rec((size_t)nr * 12);
+        PRR_CK(ctx, cudaMemcpy(rec.data(), ctx->rays.p, (size_t)nr * 48, cudaMemcpyDeviceToHost));
+        if (h_state)
+            for (long long i = 0; i < nr; i++) {
+                const float *r = rec.data() + 12 * i;
+                float *o = h_state + 12 * i;
+                int res;
+                memcpy(&res, r + 2, sizeof(int));
+                o[0] = r[0]; o[1] = r[1]; o[2] = (float)res;
+                for (int k = 0; k < 8; k++) o[3 + k] = r[3 + k];
+                o[11] = r[11];
+            }
+    } else if (h_state) {
+        PRR_CK(ctx, cudaMemcpy(h_state, ctx->state.p, (size_t)nr * 12 * sizeof(float), cudaMemcpyDeviceToHost));
+    } else if (h_state64) {
+        PRR_CK(ctx, cudaMemcpy(h_state64, ctx->state.p, (size_t)nr * 12 * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    if (h_rgb) PRR_CK(ctx, cudaMemcpy(h_rgb, rgb, (size_t)nr * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+    return PRR_OK;
+}
+
+prr_status collect_stats(prr_ctx *ctx, const RenderPlan &plan, prr_stats *stats)
+{
+    if (!stats) return PRR_OK;
+    unsigned long long c[C_COUNT];
+    PRR_CK(ctx, cudaMemcpy(c, ctx->counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+    memset(stats, 0, sizeof(*stats));
+    stats->rays = plan.total_rays;
+    stats->attempts = (int64_t)c[C_ATTEMPTS];
+    stats->accepted = (int64_t)c[C_ACCEPTED];
+    stats->n_escaped = (int64_t)c[C_ESCAPED];
+    stats->n_captured = (int64_t)c[C_CAPTURED];
+    stats->n_intersection = (int64_t)c[C_INTERSECTION];
+    stats->n_infinite = (int64_t)c[C_INFINITE];
+    stats->n_math_error = (int64_t)c[C_MATH_ERROR];
+    stats->n_fp64 = (int64_t)c[C_FP64];
+    stats->kernel_ms = ctx->last_ms;
+    stats->kernel_launches = ctx->last_launches;
+    return PRR_OK;
+}
+
+extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, prr_launch_config *best)
+{
+    if (!ctx || !frame) return PRR_ERR_INVALID;
+    if (frame->mode != PRR_MODE_PHYSICAL) { ctx->err = "prr_autotune: PHYSICAL mode frames only"; return PRR_ERR_INVALID; }
+    RenderPlan plan;
+    prr_status s = build_plan(ctx, frame, 1, plan);
+    if (s != PRR_OK) return s;
+    PRR_CK(ctx, cudaSetDevice(ctx->device));
+    const prr_launch_config saved = ctx->cfg;
+    const int saved_sched = ctx->schedule;
+    ctx->schedule = PRR_SCHED_PERSISTENT;
+    prr_launch_config winner = saved;
+    float best_ms = 1e30f;
+    const int blocks[3] = {64, 128, 256};
+    const int intervals[3] = {1, 4, 16};
+    for (int bi = 0; bi < 3; bi++) {
+        int occ = persistent_occupancy(plan.precision, ctx->geod_table, blocks[bi]);
+        if (occ < 1) continue;
+        const int bpsms[2] = {occ, std::max(1, occ / 2)};
+        for (int pi = 0; pi < (occ > 1 ? 2 : 1); pi++)
+            for (int ii = 0; ii < 3; ii++) {
+                ctx->cfg.block_size = blocks[bi];
+                ctx->cfg.blocks_per_sm = bpsms[pi];
+                ctx->cfg.compaction_interval = intervals[ii];
+                ctx->cfg.rays_per_thread = 1;
+                float ms = 1e30f;
+                for (int rep = 0; rep < 2; rep++) {
+                    s = run_plan(ctx, plan, nullptr, nullptr, ctx->stream, true);
+                    if (s != PRR_OK) { ctx->cfg = saved; ctx->schedule = saved_sched; return s; }
+                    ms = std::min(ms, ctx->last_ms);
+                }
+                if (ms < best_ms) { best_ms = ms; winner = ctx->cfg; }
+            }
+    }
+    ctx->cfg = winner;
+    ctx->schedule = saved_sched;
+    if (best) *best = winner;
+    return PRR_OK;
+}

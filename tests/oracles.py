@@ -1,0 +1,228 @@
+"""Test-side access to the CPU oracles (test infrastructure only).
+
+* `Oracle`  - the CPU restatement, oracle/_build/libprr_oracle.so
+              (oracle/prr_oracle.cpp), REFERENCE and PHYSICAL modes.
+* `RefHost` - the reference's own sources built for the host,
+              oracle/_ref/libprr_ref_{schw,flat,kerr}.so (oracle/ref/), driven
+              through a reference-format deck written by `write_deck`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import random
+import string
+from pathlib import Path
+
+import numpy as np
+
+from parrelray_b200 import abi
+
+REPO = Path(__file__).resolve().parents[1]
+ORACLE_LIB = REPO / "oracle" / "_build" / "libprr_oracle.so"
+REF_DIR = REPO / "oracle" / "_ref"
+
+_u8pp = C.POINTER(C.POINTER(C.c_uint8))
+_ip = C.POINTER(C.c_int)
+
+
+def ref_available(metric_tag: str = "schw") -> bool:
+    return (REF_DIR / f"libprr_ref_{metric_tag}.so").exists()
+
+
+class TexTable:
+    """PRR_MAX_TEXTURES-long pointer/size arrays for the oracle ABI."""
+
+    def __init__(self, textures: dict[int, np.ndarray]):
+        self.keep = {k: np.ascontiguousarray(v, dtype=np.uint8) for k, v in textures.items()}
+        self.ptrs = (C.POINTER(C.c_uint8) * abi.PRR_MAX_TEXTURES)()
+        self.w = (C.c_int * abi.PRR_MAX_TEXTURES)()
+        self.h = (C.c_int * abi.PRR_MAX_TEXTURES)()
+        for k, v in self.keep.items():
+            self.ptrs[k] = v.ctypes.data_as(C.POINTER(C.c_uint8))
+            self.h[k], self.w[k] = v.shape[0], v.shape[1]
+
+
+class Oracle:
+    def __init__(self, path: Path = ORACLE_LIB):
+        if not path.exists():
+            raise FileNotFoundError(f"{path} missing: run `python -m parrelray_b200.build --oracle`")
+        lib = C.CDLL(str(path))
+        lib.prr_oracle_trace.restype = C.c_int
+        lib.prr_oracle_trace.argtypes = [C.POINTER(abi.FrameDesc), _u8pp, _ip, _ip, C.c_int,
+                                         C.POINTER(C.c_longlong), C.c_longlong, C.c_int,
+                                         C.POINTER(C.c_double), C.POINTER(C.c_float)]
+        lib.prr_oracle_post.restype = C.c_int
+        lib.prr_oracle_post.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]
+        lib.prr_oracle_geod.restype = None
+        lib.prr_oracle_geod.argtypes = [C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]
+        lib.prr_oracle_metric.restype = None
+        lib.prr_oracle_metric.argtypes = [C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        self.lib = lib
+
+    def trace(self, d: abi.FrameDesc, textures: dict[int, np.ndarray], precision: int = 0, ids=None,
+              nthreads: int | None = None):
+        """(state (n, 13) float64, rgb (n, 3) float32) for the rays `ids`
+        (default: every ray of the frame).  state columns: uv.x uv.y result
+        r.x r.y r.z r.w u.x u.y u.z u.w accepted attempts."""
+        tt = TexTable(textures)
+        if ids is None:
+            n = d.nrays
+            idp = None
+        else:
+            ids = np.ascontiguousarray(ids, dtype=np.int64)
+            n = len(ids)
+            idp = ids.ctypes.data_as(C.POINTER(C.c_longlong))
+        state = np.zeros((n, 13), dtype=np.float64)
+        rgb = np.zeros((n, 3), dtype=np.float32)
+        rc = self.lib.prr_oracle_trace(C.byref(d), tt.ptrs, tt.w, tt.h, precision, idp, n, nthreads or os.cpu_count(),
+                                       state.ctypes.data_as(C.POINTER(C.c_double)), rgb.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc:
+            raise ValueError("oracle rejected the frame")
+        return state, rgb
+
+    def post(self, rgb: np.ndarray, w: int, h: int, samples: int, fxaa: bool) -> np.ndarray:
+        rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+        out = np.zeros((h, w, 3), dtype=np.float32)
+        self.lib.prr_oracle_post(rgb.ctypes.data_as(C.POINTER(C.c_float)), w, h, samples, 1 if fxaa else 0,
+                                 out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def render(self, d: abi.FrameDesc, textures, precision: int = 0):
+        state, rgb = self.trace(d, textures, precision)
+        img = self.post(rgb, d.width, d.height, d.samples, bool(d.fxaa))
+        return state, rgb, img
+
+    def geod(self, metric: int, M: float, a: float, p, u, refmode: bool = False) -> np.ndarray:
+        pa = (C.c_double * 4)(*p)
+        ua = (C.c_double * 4)(*u)
+        out = (C.c_double * 4)()
+        self.lib.prr_oracle_geod(metric, M, a, pa, ua, 1 if refmode else 0, out)
+        return np.array(out[:])
+
+    def metric(self, metric: int, M: float, a: float, p) -> np.ndarray:
+        pa = (C.c_double * 4)(*p)
+        g = (C.c_double * 16)()
+        self.lib.prr_oracle_metric(metric, M, a, pa, g)
+        return np.array(g[:]).reshape(4, 4)
+
+
+def _safe_dir(base: Path) -> Path:
+    """The reference's deck parser treats any line with '_' as a block header
+    (main/io.h:33), so paths written into a deck must not contain '_'."""
+    base.mkdir(parents=True, exist_ok=True)
+    name = "prr" + "".join(random.choice(string.ascii_lowercase + string.digits) for _ in range(10))
+    d = base / name
+    d.mkdir()
+    assert "_" not in str(d) and "<" not in str(d) and ">" not in str(d), d
+    return d
+
+
+def write_ppm(path: Path, rgba: np.ndarray) -> None:
+    h, w = rgba.shape[:2]
+    with open(path, "wb") as f:
+        f.write(b"P6\n%d %d\n255\n" % (w, h))
+        f.write(np.ascontiguousarray(rgba[:, :, :3]).tobytes())
+
+
+def g9(x: float) -> str:
+    return "%.9g" % float(np.float32(x))
+
+
+def write_deck(base: Path, d: abi.FrameDesc, textures: dict[int, np.ndarray], *, fov_deg: float, a_deg: float,
+               b_deg: float, solver: str = "rkf") -> Path:
+    """Writes sim/traj/scene decks reproducing `d` for the reference.  The
+    camera angles and FOV are passed in degrees (the deck's unit); `d` must
+    have been built from the same degrees."""
+    root = _safe_dir(base)
+    tex_paths = {}
+    for k, v in textures.items():
+        p = root / f"tex{k}.ppm"
+        write_ppm(p, v)
+        tex_paths[k] = p
+    sim = root / "sim.params"
+    traj = root / "traj.params"
+    scene = root / "scene.params"
+    bimage = str(tex_paths[d.background_id]) if d.background_id >= 0 else ""
+    ssaa = "none" if d.ssaa == abi.SSAA_NONE else "regular"
+    sim.write_text("\n".join([
+        "_tracer_",
+        f"<solver> = <{solver}>",
+        f"<hmin> = <{g9(d.hmin)}>",
+        f"<h> = <{g9(d.h)}>",
+        f"<hmax> = <{g9(d.hmax)}>",
+        f"<eps> = <{g9(d.eps)}>",
+        f"<rout1> = <{g9(d.rout)}>",
+        f"<rout2> = <{g9(d.rout)}>",
+        f"<bimage1> = <{bimage}>",
+        "<bimage2> = <>",
+        f"<out> = <{root}/>",
+        f"<traj> = <{traj}>",
+        f"<scene> = <{scene}>",
+        "",
+        "_spacetime_",
+        "<hasBlackHole> = <1>",
+        f"<mass> = <{g9(d.mass)}>",
+        f"<spin> = <{g9(d.spin)}>",
+        "<charge> = <0>",
+        "",
+        "_camera_",
+        f"<vfov> = <{g9(fov_deg)}>",
+        f"<width> = <{d.width}>",
+        f"<height> = <{d.height}>",
+        f"<SSAA> = <{ssaa}>",
+        f"<SSAAsamples> = <{d.samples}>",
+        "",
+    ]))
+    traj.write_text("\n".join([
+        "_frame0_",
+        f"<x> = <{g9(d.cam_pos[0])}>",
+        f"<y> = <{g9(d.cam_pos[1])}>",
+        f"<z> = <{g9(d.cam_pos[2])}>",
+        f"<a> = <{g9(a_deg)}>",
+        f"<b> = <{g9(b_deg)}>",
+        "",
+    ]))
+    lines = []
+    for k in range(d.nspheres):
+        s = d.spheres[k]
+        lines += [f"_sphere{k}_", f"<tex> = <{tex_paths[s.texture_id]}>", f"<x0> = <{g9(s.center[0])}>",
+                  f"<y0> = <{g9(s.center[1])}>", f"<z0> = <{g9(s.center[2])}>", f"<r0> = <{g9(s.radius)}>", ""]
+    scene.write_text("\n".join(lines) + "\n")
+    return sim
+
+
+class RefHost:
+    """The reference frame pipeline on the host (oracle/_ref)."""
+
+    def __init__(self, metric_tag: str = "schw"):
+        p = REF_DIR / f"libprr_ref_{metric_tag}.so"
+        if not p.exists():
+            raise FileNotFoundError(f"{p} missing: run oracle/ref/build_ref.sh")
+        lib = C.CDLL(str(p))
+        lib.prr_ref_load.restype = C.c_int
+        lib.prr_ref_load.argtypes = [C.c_char_p]
+        lib.prr_ref_info.restype = None
+        lib.prr_ref_info.argtypes = [_ip, _ip, _ip]
+        fp = C.POINTER(C.c_float)
+        lib.prr_ref_frame.restype = C.c_double
+        lib.prr_ref_frame.argtypes = [C.c_int, C.c_int, C.c_int, fp, fp, fp, fp]
+        self.lib = lib
+
+    def load(self, deck: Path) -> int:
+        return self.lib.prr_ref_load(str(deck).encode())
+
+    def frame(self, frame: int = 0, nthreads: int | None = None, rows_stride: int = 1, fxaa: bool = False):
+        w, h, s = C.c_int(), C.c_int(), C.c_int()
+        self.lib.prr_ref_info(C.byref(w), C.byref(h), C.byref(s))
+        n = w.value * h.value * s.value
+        state = np.zeros((n, 11), dtype=np.float32)
+        rgb = np.zeros((n, 3), dtype=np.float32)
+        img = np.zeros((h.value, w.value, 3), dtype=np.float32)
+        fx = np.zeros((h.value, w.value, 3), dtype=np.float32) if fxaa else None
+        fp = C.POINTER(C.c_float)
+        secs = self.lib.prr_ref_frame(frame, nthreads or os.cpu_count(), rows_stride, state.ctypes.data_as(fp),
+                                      rgb.ctypes.data_as(fp), img.ctypes.data_as(fp),
+                                      fx.ctypes.data_as(fp) if fxaa else None)
+        return {"state": state, "rgb": rgb, "image": img, "fxaa": fx, "seconds": secs}
