@@ -1,0 +1,364 @@
+"""Benchmark of the headline workload: Kerr a=0.95, 1920x1080, 2x2 SSAA
+(8,294,400 rays), RKF45 at tolerance 1e-6 in FP32, three textured spheres,
+2048x1024 starfield, FXAA.  One step = one full frame rendered through the
+C ABI (prr_render_device: ray generation, integration, colouring, SSAA
+combine, FXAA, quantisation).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 is launched with torch.distributed.run, one rank per GPU (NCCL only for
+the barrier and the max-over-ranks timing); every rank renders its own frame
+of a camera orbit (weak scaling, no data-path collective).
+
+Reported (one JSON line on rank 0):
+  value           whole-job Mrays/s, device time (CUDA events), inputs resident
+  e2e             Mrays/s through prr_render with host buffers: the frame
+                  descriptor in, the 8-bit image out (pinned), copies timed
+  roofline        FP32 FLOP/s of the tracing kernel: attempts x F_attempt /
+                  kernel time, against the measured FMA peak of the same GPU
+  plain           the plain one-ray-per-thread schedule on the same GPU
+  accuracy        fraction of pixels within 1/255 of an FP64 render
+  cpu_baseline    the reference's own solver (host build, Kerr plug-in) on a
+                  bounded sample of the same frame, on this host's cores
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "Mrays/s, Kerr a=0.95 1080p: plain vs batched FP32 at ≤1/255 err; adjoint ms"
+WORKLOAD = "kerr_a0.95_1920x1080_ssaa2x2_fxaa_rkf45_tol1e-6_fp32_3spheres"
+
+# Algorithmic FP32 work of one RKF45 attempt (FMA = 2 flop; sqrt, division,
+# reciprocal, pow = 1).  Stage combinations of the reference's formulation
+# (kernels/solver.cuh:163-176: 12 stage vectors, two 6-term sums for each of
+# x and u at 4th and 5th order, error max, step update) = 492; the Kerr
+# geodesic acceleration in the Kerr-Schild contraction form
+# (parrelray_b200/csrc/prr_device.cuh:geod_ks) = 168 per evaluation, 6 per
+# attempt.  Sphere tests are not counted.
+FLOPS_STAGES = 492
+FLOPS_GEOD_KERR = 168
+F_ATTEMPT = 6 * FLOPS_GEOD_KERR + FLOPS_STAGES
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_frames(rank: int, world: int, width: int, height: int):
+    from parrelray_b200 import scenes
+
+    # rank r renders the frame with the spheres advanced r/world of an orbit
+    from parrelray_b200 import abi
+
+    d = scenes.kerr_1080p_ssaa4(width, height)
+    if world > 1:
+        for k in range(d.nspheres):
+            s = d.spheres[k]
+            x, y = s.center[0], s.center[1]
+            ang = 2 * math.pi * rank / world
+            s.center[0] = scenes.f32(x * math.cos(ang) - y * math.sin(ang))
+            s.center[1] = scenes.f32(x * math.sin(ang) + y * math.cos(ang))
+    return d
+
+
+def cpu_reference_sample(frame, textures, budget_s: float, nthreads: int):
+    """The reference's solver (host build of its sources, Kerr plug-in header)
+    on a bounded sample of `frame`'s rays: 8-ray blocks in a fixed
+    pseudo-random order until `budget_s` of wall time is spent."""
+    sys.path.insert(0, str(REPO / "tests"))
+    from oracles import RefHost, ref_available, write_deck
+
+    from parrelray_b200 import abi, scenes
+
+    if not ref_available("kerr"):
+        return None
+    ref_frame = scenes.kerr_1080p_ssaa4(frame.width, frame.height, mode=abi.MODE_REFERENCE, eps=1e-6,
+                                        horizon_eps=0.001)
+    _, a_deg, b_deg = scenes.camera_pose(25.0, 80.0)
+    deck = write_deck(Path("/tmp/prrbench"), ref_frame, textures, fov_deg=50.0, a_deg=a_deg, b_deg=b_deg)
+    ref = RefHost("kerr")
+    assert ref.load(deck) == 1
+    ref.prepare(0, nthreads)
+    nbx = frame.samples * frame.width // 8
+    rng = np.random.default_rng(7)
+    order = rng.permutation(nbx * frame.height)[:4096]
+    done, secs = 0, 0.0
+    chunk = max(nthreads, 1)
+    while done < len(order) and secs < budget_s:
+        sel = order[done:done + chunk]
+        secs += ref.trace_blocks(sel % nbx, sel // nbx, nthreads)
+        done += len(sel)
+    rays = done * 8
+    results = np.array([ref.lib.prr_ref_ray_result(int((r * frame.width * frame.samples) + 8 * b + t))
+                        for b, r in zip(order[:done] % nbx, order[:done] // nbx) for t in range(8)])
+    return {"rays": rays, "seconds": secs, "mrays_s": rays / secs / 1e6 if secs > 0 else None,
+            "infinite_geo_fraction": float(np.mean(results == abi.RESULT_INFINITE_GEO)) if len(results) else None}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from parrelray_b200 import scenes
+
+    frame = scenes.kerr_1080p_ssaa4()
+    tex = scenes.standard_textures()
+    nthreads = os.cpu_count() or 1
+    vals = []
+    budget = float(os.environ.get("PRR_REF_STEP_SECONDS", "8"))
+    for it in range(args.warmup + args.steps):
+        r = cpu_reference_sample(frame, tex, budget if it >= args.warmup else 2.0, nthreads)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference host build (oracle/_ref) not built"}))
+            return 0
+        if it >= args.warmup:
+            vals.append(r)
+    mr = sum(v["rays"] for v in vals) / sum(v["seconds"] for v in vals) / 1e6
+    ms_per_step = 1e3 * frame.nrays / (mr * 1e6)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": mr, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural textures)",
+        "config": {"workload": WORKLOAD, "rays_per_frame": frame.nrays,
+                   "solver": "reference trace_RKF (kernels/solver.cuh) + Kerr-Schild plug-in, eps=1e-6 absolute"},
+        "cpu_baseline": {"value": mr, "unit": "Mrays/s", "cores": nthreads, "kind": "reference",
+                         "sample": f"{sum(v['rays'] for v in vals)} rays in 8-ray blocks drawn across the frame, "
+                                   f"{budget:.0f}s per step; ms_per_step extrapolates to the full frame",
+                         "infinite_geo_fraction": float(np.mean([v['infinite_geo_fraction'] for v in vals]))},
+        "e2e": {"value": mr, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    from parrelray_b200 import Context, LaunchConfig, abi, scenes
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    ctx = Context(dev)
+    tex = scenes.standard_textures()
+    ctx.upload_textures(tex)
+    frame = build_frames(rank, ws, args.width, args.height)
+    npx = frame.width * frame.height
+    out8 = torch.empty(npx * 3, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def render_device():
+        ctx.render_device(frame, out8.data_ptr(), stream=stream.cuda_stream)
+
+    # warm-up (also the stats of one frame: attempts for the roofline)
+    for _ in range(args.warmup):
+        flush.zero_()
+        render_device()
+    torch.cuda.synchronize()
+    _, _, st = ctx.render(frame)
+
+    sampler = ClockSampler(dev)
+    sampler.start()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        flush.zero_()
+        render_device()
+    ev1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    rays = frame.nrays
+    value = ws * rays / (ms * 1e-3) / 1e6
+
+    # ---- e2e through the public API with host buffers ----
+    host8 = torch.empty(npx * 3, dtype=torch.uint8, pin_memory=True).numpy()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.render(frame, out8=host8)
+    barrier()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": ws * rays / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
+           "h2d_bytes_per_step": int(abi.C.sizeof(abi.FrameDesc)), "d2h_bytes_per_step": int(npx * 3)}
+
+    extra = {}
+    if rank == 0:
+        fp32_peak, fp64_peak = ctx.measure_peak()
+        achieved = st.attempts * F_ATTEMPT / (st.trace_ms * 1e-3) / 1e12
+        roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp32_peak, "traffic": None,
+                    "kernel": "k_persistent<float,0,false>", "kernel_ms": st.trace_ms,
+                    "flop_per_attempt": F_ATTEMPT, "attempts": st.attempts,
+                    "peak_source": "measured on this GPU: FMA-chain kernel (prr_measure_peak), burst",
+                    "fp64_peak_tflops": fp64_peak}
+        extra["roofline"] = roofline
+        extra["stats"] = {k: v for k, v in st.as_dict().items()}
+        if not args.no_plain:
+            ctx.set_schedule(abi.SCHED_PLAIN)
+            ctx.render(frame)  # warm-up
+            ev0.record(stream)
+            ctx.render_device(frame, out8.data_ptr(), stream=stream.cuda_stream)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            plain_ms = ev0.elapsed_time(ev1)
+            # the Christoffel-table geodesic under the persistent schedule isolates the scheduler's share
+            ctx.set_schedule(abi.SCHED_PERSISTENT)
+            ctx.set_option(abi.OPT_GEOD_TABLE, 1)
+            ctx.render(frame)
+            ev0.record(stream)
+            ctx.render_device(frame, out8.data_ptr(), stream=stream.cuda_stream)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            table_ms = ev0.elapsed_time(ev1)
+            ctx.set_option(abi.OPT_GEOD_TABLE, 0)
+            extra["plain"] = {"value": rays / (plain_ms * 1e-3) / 1e6, "ms_per_step": plain_ms,
+                              "speedup": plain_ms / ms,
+                              "persistent_with_table_geodesic_ms": table_ms,
+                              "what": "one ray per thread, 64-row layers, AoS rays in HBM, Christoffel-table geodesic"}
+        if not args.no_accuracy:
+            f64 = build_frames(rank, ws, args.width, args.height)
+            f64.precision = abi.PREC_FP64
+            ref8, _, s64 = ctx.render(f64)
+            mine8, _, _ = ctx.render(frame)
+            d = np.abs(mine8[0].astype(np.int32) - ref8[0].astype(np.int32)).max(axis=-1)
+            extra["accuracy"] = {"pixels_within_1_255_of_fp64": float(np.mean(d <= 1)),
+                                 "max_abs_diff_255": int(d.max()), "fp64_ms": s64.kernel_ms}
+        if not args.no_cpu and ws == 1:
+            r = cpu_reference_sample(frame, tex, args.cpu_seconds, os.cpu_count() or 1)
+            if r:
+                extra["cpu_baseline"] = {"value": r["mrays_s"], "unit": "Mrays/s", "cores": os.cpu_count(),
+                                         "kind": "reference",
+                                         "sample": f"{r['rays']} rays (8-ray blocks across the frame) in "
+                                                   f"{r['seconds']:.1f}s; reference trace_RKF + Kerr-Schild plug-in at "
+                                                   f"eps=1e-6 (absolute, FP32)",
+                                         "infinite_geo_fraction": r["infinite_geo_fraction"]}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural textures)",
+            "config": {"workload": WORKLOAD, "rays_per_step": rays, "width": frame.width, "height": frame.height,
+                       "samples": frame.samples, "schedule": "persistent",
+                       "launch": {k: getattr(ctx.launch_config(), k) for k, _ in LaunchConfig._fields_},
+                       "l2": "256 MiB buffer written between timed steps (inside the timed region)"},
+            "e2e": e2e, "clocks": clocks, "gpu_launches": int(st.kernel_launches) * args.steps,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -149,6 +149,7 @@ typedef struct prr_stats {
     int64_t n_fp64;          /* rays re-integrated in FP64 (SPLIT) */
     double kernel_ms;        /* device time of the render, CUDA events */
     int64_t kernel_launches; /* kernels launched by the call */
+    double trace_ms;         /* device time of the tracing kernel(s) alone */
 } prr_stats;
 
 /* Launch shape of the persistent scheduler. */

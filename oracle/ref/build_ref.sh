@@ -89,3 +89,5 @@ build_one schw PRR_REF_METRIC_SCHW
 build_one flat PRR_REF_METRIC_FLAT
 build_one kerr PRR_REF_METRIC_KERR
 echo "built: $(ls "$OUT"/libprr_ref_*.so | tr '\n' ' ')"
+# the patched source copy is only a build intermediate: keep just the libraries
+rm -rf "$OUT/src"

@@ -200,6 +200,57 @@ double prr_ref_frame(int frame, int nthreads, int rows_stride,
     return secs;
 }
 
+// Frame set-up for a sampled trace: camera pose and scene update
+// (prr.cpp:245-253), createRays_* and initRays over the whole frame.
+int prr_ref_prepare(int frame, int nthreads)
+{
+    if (!g_loaded) return 1;
+    g_threads = nthreads > 0 ? nthreads : 1;
+    Ray *rays = g_rays;
+    i2 res = camera.getRes();
+    int samples = camera.getAAsamples();
+    std::string header = "frame" + to_string(frame);
+    camera.pos = f3(parf(header, "x"), parf(header, "y"), parf(header, "z"));
+    camera.a = parf(header, "a") * M_PI / 180.0f;
+    camera.b = parf(header, "b") * M_PI / 180.0f;
+    camera.computeVectors();
+    spacetime.updateScene(frame);
+    spacetime.setBhMass(parf(header, "mass", spacetime.getBhMass()));
+    dim3 blocks(res.x / 8 + 1, res.y / 8 + 1), threads(8, 8);
+    if (camera.getSSAADistr() == SSAA_DISTR::NONE) prr_ref_launch(blocks, threads, [&] { createRays_none(rays, res); });
+    else prr_ref_launch(blocks, threads, [&] { createRays_regular(rays, res, samples); });
+    blocks = dim3(samples * res.x / 8 + 1, res.y / 8 + 1);
+    prr_ref_launch(blocks, threads, [&] { initRays(rays, camera, spacetime, samples); });
+    return 0;
+}
+
+// Traces a sample of 8-ray blocks with the reference kernel: block k covers
+// rays x = 8*bx[k] .. 8*bx[k]+7 of row[k] (in the (samples*width, height)
+// ray image), i.e. trace_RKF/trace_Euler launched as a one-row layer with
+// blockIdx = (bx[k], 0) and blockDim = (8, 1).  Returns wall seconds.
+double prr_ref_trace_blocks(int nthreads, int nblocks, const int *bx, const int *row)
+{
+    if (!g_loaded) return -1.0;
+    Ray *rays = g_rays;
+    int samples = camera.getAAsamples();
+    auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+    for (int k = 0; k < nblocks; k++) {
+        gridDim = dim3(1, 1);
+        blockDim = dim3(8, 1);
+        blockIdx.x = (unsigned)bx[k]; blockIdx.y = 0; blockIdx.z = 0;
+        for (unsigned tx = 0; tx < 8; ++tx) {
+            threadIdx.x = tx; threadIdx.y = 0; threadIdx.z = 0;
+            if (trace.solver == SOLVER::EULER) trace_Euler(rays, camera, spacetime, trace, row[k], 1, samples);
+            else trace_RKF(rays, camera, spacetime, trace, row[k], 1, samples);
+        }
+    }
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Result enum of ray i after tracing.
+int prr_ref_ray_result(long long i) { return (g_loaded && i >= 0 && (size_t)i < g_nrays) ? (int)g_rays[i].result : -1; }
+
 // The reference's PNG path (tex2d::save -> Images::savePNGToFile,
 // cudamaths/tex2d.cuh:83-99, cudamaths/image.cu:28-39) on a host image.
 int prr_ref_save_png(const char *path, const float *image, int w, int h)

@@ -87,12 +87,16 @@ class Context:
         self._check(self.lib.prr_measure_peak(self.h, C.byref(f32), C.byref(f64)))
         return f32.value, f64.value
 
-    def render(self, frames, want_float: bool = False):
+    def render(self, frames, want_float: bool = False, out8: np.ndarray | None = None):
         """Renders one or more frames; returns (list of uint8 (h, w, 3)
-        images, list of float32 images or None, Stats)."""
+        images, list of float32 images or None, Stats).  `out8` may supply
+        the flat uint8 output buffer (e.g. pinned host memory)."""
         arr, fl = _frames_array(frames)
         npx = sum(f.width * f.height for f in fl)
-        out8 = np.empty(npx * 3, dtype=np.uint8)
+        if out8 is None:
+            out8 = np.empty(npx * 3, dtype=np.uint8)
+        elif out8.dtype != np.uint8 or out8.size < npx * 3 or not out8.flags.c_contiguous:
+            raise ValueError("out8 must be a contiguous uint8 array of at least 3*pixels elements")
         outf = np.empty(npx * 3, dtype=np.float32) if want_float else None
         stats = Stats()
         self._check(self.lib.prr_render(self.h, arr, len(fl), out8.ctypes.data_as(abi._u8p),

@@ -60,6 +60,7 @@ class Stats(C.Structure):
         ("rays", C.c_int64), ("attempts", C.c_int64), ("accepted", C.c_int64), ("n_escaped", C.c_int64),
         ("n_captured", C.c_int64), ("n_intersection", C.c_int64), ("n_infinite", C.c_int64),
         ("n_math_error", C.c_int64), ("n_fp64", C.c_int64), ("kernel_ms", C.c_double), ("kernel_launches", C.c_int64),
+        ("trace_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:

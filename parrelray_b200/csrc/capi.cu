@@ -121,7 +121,8 @@ prr_status prr_create(int device, prr_ctx **out)
     ctx->nsm = prop.multiProcessorCount;
     ctx->sm_clock_khz = prop.clockRate;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&ctx->e0) != cudaSuccess || cudaEventCreate(&ctx->e1) != cudaSuccess) {
+        cudaEventCreate(&ctx->e0) != cudaSuccess || cudaEventCreate(&ctx->e1) != cudaSuccess ||
+        cudaEventCreate(&ctx->t0) != cudaSuccess || cudaEventCreate(&ctx->t1) != cudaSuccess) {
         delete ctx;
         return PRR_ERR_CUDA;
     }
@@ -143,6 +144,8 @@ void prr_destroy(prr_ctx *ctx)
     for (DevBuf *b : ctx->all_buffers()) b->release();
     cudaEventDestroy(ctx->e0);
     cudaEventDestroy(ctx->e1);
+    cudaEventDestroy(ctx->t0);
+    cudaEventDestroy(ctx->t1);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

@@ -26,7 +26,7 @@ struct prr_ctx {
     int nsm = 0;
     int sm_clock_khz = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, t0 = nullptr, t1 = nullptr;
     std::string err;
     TexSlot tex[PRR_MAX_TEXTURES];
     int schedule = PRR_SCHED_PERSISTENT;
@@ -35,6 +35,7 @@ struct prr_ctx {
     long long watchdog_cycles = 0;
     int last_launches = 0;
     float last_ms = 0.f;
+    float last_trace_ms = 0.f;
     // device scratch, grown on demand and reused across calls
     DevBuf frames, frame_begin, counters, image, sample_rgb, rays, queue, state, out_u8, out_f, scratch;
     std::vector<DevBuf *> all_buffers()

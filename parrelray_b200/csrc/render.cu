@@ -198,6 +198,7 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
         return PRR_OK;
     };
 
+    bool trace_timed = false;
     if (plan.mode == PRR_MODE_REFERENCE || ctx->schedule == PRR_SCHED_PLAIN) {
         long long max_rays = 0;
         for (const auto &p : plan.fp) max_rays = std::max(max_rays, (long long)p.width * p.height * p.samples);
@@ -220,6 +221,7 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
             if ((s = finish(f, false)) != PRR_OK) return s;
         }
     } else {
+        trace_timed = timed;
         PersistentArgs a = persistent_args(ctx, plan);
         a.image = image;
         const int bpsm = resolve_bpsm(ctx, plan.precision);
@@ -229,8 +231,10 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
             a.sample_rgb = (float *)ctx->sample_rgb.p;
             a.fp64_queue = (unsigned long long *)ctx->queue.p;
             a.fp64_capacity = plan.total_rays;
+            if (timed) PRR_CK(ctx, cudaEventRecord(ctx->t0, st));
             PRR_CK(ctx, launch_persistent(a, PRR_PREC_SPLIT, ctx->cfg.block_size, bpsm, ctx->nsm, st));
             PRR_CK(ctx, launch_fp64_requeue(a, 128, ctx->nsm, st));
+            if (timed) PRR_CK(ctx, cudaEventRecord(ctx->t1, st));
             launches += 2;
             for (int f = 0; f < n; f++) {
                 const FrameParams &p = plan.fp[f];
@@ -240,7 +244,9 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
             }
         } else {
             a.rgb8 = d_rgb8;
+            if (timed) PRR_CK(ctx, cudaEventRecord(ctx->t0, st));
             PRR_CK(ctx, launch_persistent(a, plan.precision, ctx->cfg.block_size, bpsm, ctx->nsm, st));
+            if (timed) PRR_CK(ctx, cudaEventRecord(ctx->t1, st));
             launches++;
             for (int f = 0; f < n; f++)
                 if ((s = finish(f, true)) != PRR_OK) return s;
@@ -250,6 +256,8 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
         PRR_CK(ctx, cudaEventRecord(ctx->e1, st));
         PRR_CK(ctx, cudaEventSynchronize(ctx->e1));
         PRR_CK(ctx, cudaEventElapsedTime(&ctx->last_ms, ctx->e0, ctx->e1));
+        ctx->last_trace_ms = ctx->last_ms;
+        if (trace_timed) PRR_CK(ctx, cudaEventElapsedTime(&ctx->last_trace_ms, ctx->t0, ctx->t1));
     }
     ctx->last_launches = launches;
     if (ctx->watchdog_cycles > 0) {
@@ -298,6 +306,7 @@ prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, doub
     PRR_CK(ctx, cudaEventRecord(ctx->e1, st));
     PRR_CK(ctx, cudaEventSynchronize(ctx->e1));
     PRR_CK(ctx, cudaEventElapsedTime(&ctx->last_ms, ctx->e0, ctx->e1));
+    ctx->last_trace_ms = ctx->last_ms;
     if (plan.mode != PRR_MODE_REFERENCE && ctx->schedule == PRR_SCHED_PLAIN && !h_state64) {
         // ray records (48 B, main/base.h:172-176 layout) -> 12-float states
         std::vector<float> rec((size_t)nr * 12);
@@ -338,6 +347,7 @@ prr_status collect_stats(prr_ctx *ctx, const RenderPlan &plan, prr_stats *stats)
     stats->n_fp64 = (int64_t)c[C_FP64];
     stats->kernel_ms = ctx->last_ms;
     stats->kernel_launches = ctx->last_launches;
+    stats->trace_ms = ctx->last_trace_ms;
     return PRR_OK;
 }
 

