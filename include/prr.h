@@ -212,7 +212,9 @@ prr_status prr_get_launch_config(prr_ctx *ctx, prr_launch_config *cfg);
 prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, prr_launch_config *best);
 
 /* Context options (values for prr_set_option). */
-#define PRR_OPT_GEOD_TABLE 1      /* 1: persistent kernel uses the Christoffel-table geodesic (A/B runs) */
+#define PRR_OPT_GEOD_TABLE 1      /* geodesic form: -1 (default) PERSISTENT uses the register contraction and
+                                     PLAIN the Christoffel table; 0: contraction everywhere; 1: table
+                                     everywhere (A/B runs) */
 #define PRR_OPT_WATCHDOG_CYCLES 2 /* >0: persistent kernels stop after this many SM clock cycles and the
                                      call returns PRR_ERR_TIMEOUT; 0: off (default) */
 prr_status prr_set_option(prr_ctx *ctx, int option, long long value);

@@ -503,13 +503,14 @@ private:
     void rkf(RayState<T> &R) const
     {
         const Tableau tb;
-        const T A21 = (T)(float)tb.A21, A31 = (T)(float)tb.A31, A32 = (T)(float)tb.A32, A41 = (T)(float)tb.A41,
-                A42 = (T)(float)tb.A42, A43 = (T)(float)tb.A43, A51 = (T)(float)tb.A51, A52 = (T)(float)tb.A52,
-                A53 = (T)(float)tb.A53, A54 = (T)(float)tb.A54, A61 = (T)(float)tb.A61, A62 = (T)(float)tb.A62,
-                A63 = (T)(float)tb.A63, A64 = (T)(float)tb.A64, A65 = (T)(float)tb.A65;
-        const T K41 = (T)(float)tb.K41, K42 = (T)(float)tb.K42, K43 = (T)(float)tb.K43, K44 = (T)(float)tb.K44,
-                K45 = (T)(float)tb.K45, K46 = (T)(float)tb.K46, K51 = (T)(float)tb.K51, K52 = (T)(float)tb.K52,
-                K53 = (T)(float)tb.K53, K54 = (T)(float)tb.K54, K55 = (T)(float)tb.K55, K56 = (T)(float)tb.K56;
+        // REFERENCE mode: the reference stores the tableau as float
+        // (solver.cuh:125-131); PHYSICAL mode rounds the exact fractions to T.
+        auto c = [&](double v) { return ref_ ? (T)(float)v : (T)v; };
+        const T A21 = c(tb.A21), A31 = c(tb.A31), A32 = c(tb.A32), A41 = c(tb.A41), A42 = c(tb.A42), A43 = c(tb.A43),
+                A51 = c(tb.A51), A52 = c(tb.A52), A53 = c(tb.A53), A54 = c(tb.A54), A61 = c(tb.A61), A62 = c(tb.A62),
+                A63 = c(tb.A63), A64 = c(tb.A64), A65 = c(tb.A65);
+        const T K41 = c(tb.K41), K42 = c(tb.K42), K43 = c(tb.K43), K44 = c(tb.K44), K45 = c(tb.K45), K46 = c(tb.K46),
+                K51 = c(tb.K51), K52 = c(tb.K52), K53 = c(tb.K53), K54 = c(tb.K54), K55 = c(tb.K55), K56 = c(tb.K56);
         T h = (T)d_->h, hmin = (T)d_->hmin, hmax = (T)d_->hmax, _h = h;
         T eps = (T)d_->eps, rtol = (T)d_->rtol, atol = (T)d_->atol;
         T trace_h = (T)d_->h;

@@ -92,7 +92,7 @@ class Context:
         images, list of float32 images or None, Stats).  `out8` may supply
         the flat uint8 output buffer (e.g. pinned host memory)."""
         arr, fl = _frames_array(frames)
-        npx = sum(f.width * f.height for f in fl)
+        npx = sum(max(f.width, 0) * max(f.height, 0) for f in fl)  # the library validates sizes
         if out8 is None:
             out8 = np.empty(npx * 3, dtype=np.uint8)
         elif out8.dtype != np.uint8 or out8.size < npx * 3 or not out8.flags.c_contiguous:

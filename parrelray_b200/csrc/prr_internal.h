@@ -31,7 +31,7 @@ struct prr_ctx {
     TexSlot tex[PRR_MAX_TEXTURES];
     int schedule = PRR_SCHED_PERSISTENT;
     prr_launch_config cfg{};
-    int geod_table = 0;
+    int geod_table = -1;  // -1: per schedule (PERSISTENT contraction, PLAIN table); 0: contraction; 1: table
     long long watchdog_cycles = 0;
     int last_launches = 0;
     float last_ms = 0.f;

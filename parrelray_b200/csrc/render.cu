@@ -54,7 +54,7 @@ prr_status alloc(prr_ctx *ctx, DevBuf &b, size_t bytes, const char *what)
 int resolve_bpsm(prr_ctx *ctx, int precision)
 {
     if (ctx->cfg.blocks_per_sm > 0) return ctx->cfg.blocks_per_sm;
-    int b = persistent_occupancy(precision, ctx->geod_table, ctx->cfg.block_size);
+    int b = persistent_occupancy(precision, ctx->geod_table == 1, ctx->cfg.block_size);
     return b > 0 ? b : 1;
 }
 
@@ -166,7 +166,7 @@ static PersistentArgs persistent_args(prr_ctx *ctx, const RenderPlan &plan)
     a.nframes = (int)plan.fp.size();
     a.total_pixels = plan.total_pixels;
     a.counters = (unsigned long long *)ctx->counters.p;
-    a.geod_table = ctx->geod_table;
+    a.geod_table = ctx->geod_table == 1;
     a.compaction_interval = ctx->cfg.compaction_interval;
     a.watchdog_cycles = ctx->watchdog_cycles;
     return a;
@@ -214,7 +214,7 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
                 launches++;
             } else {
                 PlainBuffers b{ctx->rays.p, rgb};
-                PRR_CK(ctx, launch_plain_frame(d_fp, p, f, b, counters, ctx->geod_table, st, &launches));
+                PRR_CK(ctx, launch_plain_frame(d_fp, p, f, b, counters, ctx->geod_table != 0, st, &launches));
             }
             PRR_CK(ctx, launch_combine(rgb, p.width, p.height, p.samples, image + 3 * p.pix_begin, st));
             launches++;
@@ -290,7 +290,7 @@ prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, doub
         if ((s = alloc(ctx, ctx->rays, (size_t)nr * plain_ray_record_bytes(), "ray records")) != PRR_OK) return s;
         PlainBuffers b{ctx->rays.p, rgb};
         int launches = 0;
-        PRR_CK(ctx, launch_plain_frame(d_fp, p, 0, b, counters, ctx->geod_table, st, &launches));
+        PRR_CK(ctx, launch_plain_frame(d_fp, p, 0, b, counters, ctx->geod_table != 0, st, &launches));
         ctx->last_launches = launches;
     } else {
         if ((s = alloc(ctx, ctx->image, (size_t)plan.total_pixels * 3 * sizeof(float), "image")) != PRR_OK) return s;
@@ -367,7 +367,7 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
     const int blocks[3] = {64, 128, 256};
     const int intervals[3] = {1, 4, 16};
     for (int bi = 0; bi < 3; bi++) {
-        int occ = persistent_occupancy(plan.precision, ctx->geod_table, blocks[bi]);
+        int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi]);
         if (occ < 1) continue;
         const int bpsms[2] = {occ, std::max(1, occ / 2)};
         for (int pi = 0; pi < (occ > 1 ? 2 : 1); pi++)

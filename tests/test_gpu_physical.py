@@ -34,16 +34,29 @@ def kerr_oracle_fp64(oracle, small_textures):
     return d, st, rgb, img
 
 
+def escape_dirs(st):
+    u = st[:, 7:10]
+    return u / np.linalg.norm(u, axis=1, keepdims=True)
+
+
 def test_fp64_gpu_matches_fp64_oracle(gpu, small_textures, kerr_oracle_fp64):
+    """Outcome, escape direction (the observable the background lookup uses)
+    and hit colour.  The final POSITION is not compared: the last step
+    overshoots r = rout by up to one step, so it depends on the step sequence."""
     d, st, rgb, _ = kerr_oracle_fp64
     gpu.upload_textures(small_textures)
     gs, grgb, stats = gpu.trace_rays_f64(d)
     same = gs[:, 2] == st[:, 2]
     assert same.mean() >= 0.999
-    rel = np.abs(gs[same, 3:11] - st[same, 3:11]) / (np.abs(st[same, 3:11]) + 1.0)
-    close = rel.max(axis=1) < 1e-5
-    assert close.mean() >= 0.99, close.mean()
+    esc = same & (st[:, 2] == abi.RESULT_SUCCESS) & (np.linalg.norm(st[:, 3:6], axis=1) >= d.rout)
+    assert esc.sum() > 0.5 * len(st)
+    ang = np.arccos(np.clip(np.sum(escape_dirs(gs[esc]) * escape_dirs(st[esc]), 1), -1, 1))
+    assert np.mean(ang < 1e-7) >= 0.99, np.percentile(ang, [50, 99])
     assert np.mean(np.abs(grgb[same] - rgb[same]).max(axis=1) <= 1 / 255) >= 0.995
+    # same step count -> the whole state agrees
+    steps_same = same & (gs[:, 11] == st[:, 11])
+    rel = np.abs(gs[steps_same, 3:11] - st[steps_same, 3:11]) / (np.abs(st[steps_same, 3:11]) + 1.0)
+    assert np.mean(rel.max(axis=1) < 1e-8) >= 0.99
 
 
 @pytest.mark.parametrize("schedule", [abi.SCHED_PERSISTENT, abi.SCHED_PLAIN])
@@ -93,7 +106,7 @@ def test_table_and_contraction_geodesics_agree(gpu, small_textures):
     try:
         b, _, _ = gpu.render(d)
     finally:
-        gpu.set_option(abi.OPT_GEOD_TABLE, 0)
+        gpu.set_option(abi.OPT_GEOD_TABLE, -1)
     assert pixel_rule(a[0], b[0]) >= 0.999
 
 
