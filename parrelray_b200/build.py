@@ -53,19 +53,25 @@ def _run(cmd: list[str], verbose: bool) -> None:
     subprocess.run(cmd, check=True)
 
 
-def build_library(verbose: bool = False, ptxas_verbose: bool = False) -> Path:
-    BUILD.mkdir(parents=True, exist_ok=True)
-    LIBDIR.mkdir(parents=True, exist_ok=True)
+def build_library(verbose: bool = False, ptxas_verbose: bool = False, defines: list[str] | None = None,
+                  build_dir: Path | None = None, lib_path: Path | None = None) -> Path:
+    """Compiles every source and links the library.  `defines` (-D values)
+    with `build_dir`/`lib_path` build a variant elsewhere (tuning studies)."""
+    bdir = Path(build_dir) if build_dir else BUILD
+    lib = Path(lib_path) if lib_path else LIB
+    bdir.mkdir(parents=True, exist_ok=True)
+    lib.parent.mkdir(parents=True, exist_ok=True)
+    dflags = [f"-D{d}" for d in (defines or [])]
     hdrs = _headers()
     objs: list[Path] = []
     for src in CU_SOURCES:
         s = CSRC / src
-        o = BUILD / (src + ".o")
+        o = bdir / (src + ".o")
         objs.append(o)
         if _newer(o, [s] + hdrs) and not ptxas_verbose:
             continue
         cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-               "-I", str(INCLUDE), "-I", str(CSRC), "-c", str(s), "-o", str(o)]
+               *dflags, "-I", str(INCLUDE), "-I", str(CSRC), "-c", str(s), "-o", str(o)]
         if src in NO_FMAD:
             cmd.insert(1, "-fmad=false")
         if ptxas_verbose:
@@ -73,14 +79,14 @@ def build_library(verbose: bool = False, ptxas_verbose: bool = False) -> Path:
         _run(cmd, verbose)
     for src in CPP_SOURCES:
         s = CSRC / src
-        o = BUILD / (src + ".o")
+        o = bdir / (src + ".o")
         objs.append(o)
         if _newer(o, [s] + hdrs):
             continue
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-I", str(INCLUDE), "-c", str(s), "-o", str(o)], verbose)
-    if not _newer(LIB, objs):
-        _run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs)], verbose)
-    return LIB
+    if not _newer(lib, objs):
+        _run([nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs)], verbose)
+    return lib
 
 
 ORACLE_DIR = REPO / "oracle"

@@ -67,8 +67,17 @@ __device__ __forceinline__ void write_state(O *st, long long rid, const PhysRay<
     o[11] = (O)R.accepted;
 }
 
+// Launch bounds: at most PRR_PERSISTENT_MAXT threads per CTA, at least
+// PRR_PERSISTENT_MINB resident CTAs per SM (caps registers per thread).
+#ifndef PRR_PERSISTENT_MAXT
+#define PRR_PERSISTENT_MAXT 256
+#endif
+#ifndef PRR_PERSISTENT_MINB
+#define PRR_PERSISTENT_MINB 1
+#endif
+
 template <class T, int GEOD, bool SPLIT>
-__global__ void __launch_bounds__(256) k_persistent(PersistentArgs a)
+__global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_persistent(PersistentArgs a)
 {
     const int lane = threadIdx.x & 31;
     long long item = -1;

@@ -81,8 +81,8 @@ template <class T> PRR_DEV Hot<T> make_hot(const FrameParams &fp)
     return q;
 }
 
-template <class T> PRR_DEV T fast_rcp(T v) { return (T)1 / v; }
-template <> PRR_DEV float fast_rcp<float>(float v) { return __frcp_rn(v); }
+
+
 
 // Null initial data: position = camera, u = (dir, u^t), u^t the larger root
 // of g_tt (u^t)^2 + 2 g_ti u^i u^t + g_ij u^i u^j = 0 (initRays solves the
@@ -116,7 +116,7 @@ template <class T, int GEOD> PRR_DEV V4<T> phys_geod(const Hot<T> &q, const V4<T
 {
     if (q.metric == PRR_METRIC_FLAT) return {0, 0, 0, 0};
     if (GEOD == 1) return geod_table<T>(x, u, q.M, q.a);
-    return geod_ks<T>(x, u, q.M, q.a);
+    return geod_ks<T, true>(x, u, q.M, q.a);
 }
 
 // Distance d of Sphere::intersects (scene/sphere.h:40-48) along the unit
@@ -127,8 +127,19 @@ template <class T> PRR_DEV bool sphere_d(const DevSphere &S, T px, T py, T pz, T
     T dvp = vx * dx + vy * dy + vz * dz;
     T disc = dvp * dvp - v2 * ((dx * dx + dy * dy + dz * dz) - rad * rad);
     if (disc < (T)0) return false;
-    d = ((T)-2.0f * dvp - sqrt(disc)) / v2;
+    T sd = disc > (T)0 ? disc * frsqrt<T>(disc) : (T)0;
+    d = ((T)-2.0f * dvp - sd) * frcp<T>(v2);
     return d >= (T)0;
+}
+
+// True when the point p is too far from sphere S for Sphere::intersects to
+// accept it with any window h <= hmax: a hit needs the distance to the
+// centre D to satisfy D^2 <= ((sqrt(hmax) + R)/2)^2 + R^2 (S.far2 holds
+// that bound with a rounding margin), so skipping the test changes nothing.
+template <class T> PRR_DEV bool sphere_far(const DevSphere &S, T px, T py, T pz)
+{
+    T dx = px - (T)S.cx, dy = py - (T)S.cy, dz = pz - (T)S.cz;
+    return dx * dx + dy * dy + dz * dz > (T)S.far2;
 }
 
 // Sphere::getColor at p + v d (scene/sphere.h:59-64).
@@ -145,6 +156,17 @@ template <class T> PRR_DEV V3<float> sphere_colour(const DevSphere &S, T px, T p
     if (S.tex.p) col = tex_bilinear<T>(S.tex, uu, vv);
     T shade = fmax((T)0, fmin((T)0.5 + (T)0.5 * iz / rad, (T)1));
     return {(float)(col.x * shade), (float)(col.y * shade), (float)(col.z * shade)};
+}
+
+// Sky colour of an escaped ray from its direction of flight.
+template <class T> PRR_DEV V3<float> escape_colour(const FrameParams &fp, const V4<T> &u)
+{
+    if (!fp.bg.p) return {0.0f, 0.0f, 0.0f};
+    if (fp.bg_filter == PRR_BG_BILINEAR) {
+        V3<T> b = background_bilinear<T>(fp.bg, u.x, u.y, u.z);
+        return {(float)b.x, (float)b.y, (float)b.z};
+    }
+    return background_rms<T>(fp.bg, u.x, u.y, u.z);
 }
 
 template <class T> PRR_DEV void kahan_add(T &s, T &c, T v)
@@ -211,13 +233,13 @@ PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, 
         T ex = h * ((T)F::e1 * k1.c + (T)F::e2 * k2.c + (T)F::e3 * k3.c + (T)F::e4 * k4.c + (T)F::e5 * k5.c);  \
         T sx = q.atol + q.rtol * fmax(fabs(x.c), fabs(x.c + dx));                                                 \
         T su = q.atol + q.rtol * fmax(fabs(u.c), fabs(u.c + du));                                                 \
-        err = fmax(err, fabs(ex) * fast_rcp<T>(sx));                                                               \
-        err = fmax(err, fabs(eu) * fast_rcp<T>(su));                                                               \
+        err = fmax(err, fabs(ex) * frcp<T>(sx));                                                               \
+        err = fmax(err, fabs(eu) * frcp<T>(su));                                                               \
         dxv[j] = dx; duv[j] = du;                                                                                  \
     }
     PRR_FIN(x, 0) PRR_FIN(y, 1) PRR_FIN(z, 2) PRR_FIN(w, 3)
 #undef PRR_FIN
-    T hn = (T)0.9 * h * (T)pow(err, (T)-0.2);
+    T hn = (T)0.9 * h * fpow<T>(err, (T)-0.2);
     hn = fmin(fmax(hn, q.hmin), q.hmax);
 
     if (R.intersect && R.i > 10000) R.intersect = 0;
@@ -238,8 +260,10 @@ PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, 
     int candH = -1, candN = -1, candT = -1;
     T dH = (T)1e11, dN = (T)1e11, dT = (T)1e11;
     T vx = 0, vy = 0, vz = 0, v2 = 0;
-    if (q.nspheres > 0) {
-        T k = (T)1 / sqrt(un.x * un.x + un.y * un.y + un.z * un.z);
+    bool near = false;
+    for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn.x, xn.y, xn.z);
+    if (near) {
+        T k = frsqrt<T>(un.x * un.x + un.y * un.y + un.z * un.z);
         vx = un.x * k; vy = un.y * k; vz = un.z * k;
         v2 = vx * vx + vy * vy + vz * vz;
         for (int s = 0; s < q.nspheres; s++) {
@@ -266,11 +290,17 @@ PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, 
     } else {
         candE = candT; dE = dT;
     }
-    // User_ENDLOOP
-    T r = q.metric == PRR_METRIC_KERR ? ks_radius<T>(xn.x, xn.y, xn.z, q.a) : sqrt(xn.x * xn.x + xn.y * xn.y + xn.z * xn.z);
-    if (r >= q.rout || (q.metric != PRR_METRIC_FLAT && r <= q.rstop)) {
+    // User_ENDLOOP, on the squared radius (one square root for Kerr, none otherwise)
+    T r2 = xn.x * xn.x + xn.y * xn.y + xn.z * xn.z;
+    if (q.metric == PRR_METRIC_KERR) {
+        T b = r2 - q.a * q.a;
+        T S2 = b * b + (T)4 * q.a * q.a * xn.z * xn.z;
+        r2 = (T)0.5 * (b + S2 * frsqrt<T>(S2));
+    }
+    const bool escaped = r2 >= q.rout * q.rout;
+    if (escaped || (q.metric != PRR_METRIC_FLAT && r2 <= q.rstop * q.rstop)) {
         result = PRR_RESULT_SUCCESS;
-        colour = ray_colour<T>(fp, PRR_RESULT_SUCCESS, R.x, R.u);
+        colour = escaped ? escape_colour<T>(fp, R.u) : V3<float>{0.0f, 0.0f, 0.0f};
         return STEP_DONE;
     }
     if (candE >= 0) {
@@ -279,7 +309,7 @@ PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, 
         R.u = {(T)colour.x, (T)colour.y, (T)colour.z, (T)0};
         return STEP_DONE;
     }
-    if (r < flag_r) return STEP_FLAG64;
+    if (flag_r > (T)0 && r2 < flag_r * flag_r) return STEP_FLAG64;
     R.l += R.h;
     if (R.accepted >= q.max_steps) { result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0}; return STEP_DONE; }
     return STEP_CONTINUE;

@@ -28,6 +28,17 @@ constexpr double PI_SPHERE = 3.14159265359;          // scene/sphere.h:16 (redef
 template <class T> struct V3 { T x, y, z; };
 template <class T> struct V4 { T x, y, z, w; };
 
+// Reciprocal, reciprocal square root and power for the PHYSICAL-mode hot
+// loop.  FP32 uses the SFU approximations (rcp.approx / rsqrt.approx /
+// lg2+ex2: a few ulp, far below the 1e-6 integration tolerance) instead of
+// the IEEE-rounded multi-instruction sequences; FP64 stays exact.
+template <class T> PRR_DEV T frcp(T v) { return (T)1 / v; }
+template <> PRR_DEV float frcp<float>(float v) { return __fdividef(1.0f, v); }
+template <class T> PRR_DEV T frsqrt(T v) { return (T)1 / sqrt(v); }
+template <> PRR_DEV float frsqrt<float>(float v) { return rsqrtf(v); }
+template <class T> PRR_DEV T fpow(T b, T e) { return pow(b, e); }
+template <> PRR_DEV float fpow<float>(float b, float e) { return exp2f(e * __log2f(b)); }
+
 template <class T> PRR_HD V4<T> v4add(const V4<T> &a, const V4<T> &b) { return {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
 // f4 scaled by t; the reference's operator*(float, f4) multiplies each
 // component by t (cudamaths/f4.cuh:52).
@@ -80,6 +91,7 @@ template <class T> PRR_DEV V3<T> tex_bilinear(const DevTex &t, T u, T v)
 struct DevSphere {
     float cx, cy, cz, r;
     DevTex tex;  // tex.p == nullptr: untextured (grey 0.5)
+    float far2;  // squared distance beyond which no hit test can pass (PHYSICAL-mode early out)
 };
 
 // Everything a kernel needs about one frame, prepared on the host from a
@@ -213,18 +225,36 @@ PRR_DEV V4<float> geod_schw_ref(const V4<float> &p, const V4<float> &u, float rs
 //   du^k = -g^{km} G_m,  g^{km} = eta^{km} - f l^k l^m  (l^k = eta^{kk} l_k)
 // All quantities are scalars or 3-vectors held in registers.  Cost is about
 // 110 FP32 operations + 2 sqrt + 4 divisions (vs. ~1000 for the table).
-template <class T> PRR_DEV V4<T> geod_ks(const V4<T> &p, const V4<T> &u, T M, T a)
+// FAST selects the SFU reciprocal / rsqrt forms (PHYSICAL mode); the
+// REFERENCE-mode Kerr path keeps IEEE division and square root.
+#ifdef PRR_GEOD_NOINLINE
+#define PRR_GEOD_FN __device__ __noinline__
+#else
+#define PRR_GEOD_FN PRR_DEV
+#endif
+template <class T, bool FAST = false> PRR_GEOD_FN V4<T> geod_ks(const V4<T> &p, const V4<T> &u, T M, T a)
 {
     const T X = p.x, Y = p.y, Z = p.z;
     const T a2 = a * a;
     const T R2 = X * X + Y * Y + Z * Z;
     const T b = R2 - a2;
-    const T S = sqrt(b * b + (T)4 * a2 * Z * Z);
-    const T r2 = (T)0.5 * (b + S);
-    const T r = sqrt(r2);
-    const T ir = (T)1 / r, iS = (T)1 / S;
-    const T q = r2 + a2, iq = (T)1 / q;
-    const T Sig = r2 * r2 + a2 * Z * Z, iSig = (T)1 / Sig;
+    const T S2 = b * b + (T)4 * a2 * Z * Z;
+    T S, iS, r2, r, ir;
+    if (FAST) {
+        iS = frsqrt<T>(S2);
+        S = S2 * iS;
+        r2 = (T)0.5 * (b + S);
+        ir = frsqrt<T>(r2);
+        r = r2 * ir;
+    } else {
+        S = sqrt(S2);
+        iS = (T)1 / S;
+        r2 = (T)0.5 * (b + S);
+        r = sqrt(r2);
+        ir = (T)1 / r;
+    }
+    const T q = r2 + a2, iq = FAST ? frcp<T>(q) : (T)1 / q;
+    const T Sig = r2 * r2 + a2 * Z * Z, iSig = FAST ? frcp<T>(Sig) : (T)1 / Sig;
     // radius gradient
     const T rS = r * iS;
     const T drx = X * rS, dry = Y * rS, drz = Z * q * iS * ir;

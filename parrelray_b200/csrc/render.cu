@@ -111,7 +111,10 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
                 return bad(ctx, f, "sphere " + std::to_string(s) + " has a bad centre or radius");
             if (S.texture_id >= PRR_MAX_TEXTURES || (S.texture_id >= 0 && !ctx->tex[S.texture_id].buf.p))
                 return bad(ctx, f, "sphere " + std::to_string(s) + " texture id not uploaded");
-            p.sph[s] = {S.center[0], S.center[1], S.center[2], S.radius, dev_tex(ctx, S.texture_id)};
+            // a hit with any window h <= hmax needs |p - c|^2 <= ((sqrt(hmax) + R)/2)^2 + R^2
+            double reach = 0.5 * (std::sqrt((double)d.hmax) + S.radius);
+            float far2 = (float)((reach * reach + (double)S.radius * S.radius) * 1.01 + 1e-3);
+            p.sph[s] = {S.center[0], S.center[1], S.center[2], S.radius, dev_tex(ctx, S.texture_id), far2};
         }
         p.width = d.width; p.height = d.height; p.samples = d.samples; p.ssaa = d.ssaa;
         p.vfov = d.vfov; p.cam[0] = d.cam_pos[0]; p.cam[1] = d.cam_pos[1]; p.cam[2] = d.cam_pos[2];

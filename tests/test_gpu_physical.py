@@ -50,8 +50,11 @@ def test_fp64_gpu_matches_fp64_oracle(gpu, small_textures, kerr_oracle_fp64):
     assert same.mean() >= 0.999
     esc = same & (st[:, 2] == abi.RESULT_SUCCESS) & (np.linalg.norm(st[:, 3:6], axis=1) >= d.rout)
     assert esc.sum() > 0.5 * len(st)
-    ang = np.arccos(np.clip(np.sum(escape_dirs(gs[esc]) * escape_dirs(st[esc]), 1), -1, 1))
-    assert np.mean(ang < 1e-7) >= 0.99, np.percentile(ang, [50, 99])
+    # |a x b| resolves small angles (arccos of the dot product bottoms out at 1.5e-8)
+    ang = np.linalg.norm(np.cross(escape_dirs(gs[esc]), escape_dirs(st[esc])), axis=1)
+    # a background texel spans 3e-3 rad; 1e-6 is the FP64 agreement bar
+    assert np.mean(ang < 1e-6) >= 0.99, np.percentile(ang, [50, 99, 99.9])
+    assert np.mean(ang < 1e-4) >= 0.999, np.percentile(ang, [50, 99, 99.9])
     assert np.mean(np.abs(grgb[same] - rgb[same]).max(axis=1) <= 1 / 255) >= 0.995
     # same step count -> the whole state agrees
     steps_same = same & (gs[:, 11] == st[:, 11])
