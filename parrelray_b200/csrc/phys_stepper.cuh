@@ -191,37 +191,56 @@ PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, 
     R.i += 1;
     const T h = R.h;
     const V4<T> &x = R.x, &u = R.u;
-    // stage 1
-    V4<T> k1 = v4scl(h, phys_geod<T, GEOD>(q, x, u));
-    // stage 2
-    V4<T> zx, zu;
-    zx = {x.x + h * ((T)F::c2 * u.x), x.y + h * ((T)F::c2 * u.y), x.z + h * ((T)F::c2 * u.z), x.w + h * ((T)F::c2 * u.w)};
-    zu = {u.x + (T)F::A21 * k1.x, u.y + (T)F::A21 * k1.y, u.z + (T)F::A21 * k1.z, u.w + (T)F::A21 * k1.w};
-    V4<T> k2 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
+#define PRR_ST2(c)                                                                                                 \
+    zx.c = x.c + h * ((T)F::c2 * u.c);                                                                           \
+    zu.c = u.c + (T)F::A21 * k1.c;
 #define PRR_ST3(c)                                                                                                 \
     zx.c = x.c + h * ((T)F::c3 * u.c + (T)F::B31 * k1.c);                                                        \
     zu.c = u.c + (T)F::A31 * k1.c + (T)F::A32 * k2.c;
-    PRR_ST3(x) PRR_ST3(y) PRR_ST3(z) PRR_ST3(w)
-#undef PRR_ST3
-    V4<T> k3 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
 #define PRR_ST4(c)                                                                                                 \
     zx.c = x.c + h * ((T)F::c4 * u.c + (T)F::B41 * k1.c + (T)F::B42 * k2.c);                                     \
     zu.c = u.c + (T)F::A41 * k1.c + (T)F::A42 * k2.c + (T)F::A43 * k3.c;
-    PRR_ST4(x) PRR_ST4(y) PRR_ST4(z) PRR_ST4(w)
-#undef PRR_ST4
-    V4<T> k4 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
 #define PRR_ST5(c)                                                                                                 \
     zx.c = x.c + h * ((T)F::c5 * u.c + (T)F::B51 * k1.c + (T)F::B52 * k2.c + (T)F::B53 * k3.c);                 \
     zu.c = u.c + (T)F::A51 * k1.c + (T)F::A52 * k2.c + (T)F::A53 * k3.c + (T)F::A54 * k4.c;
-    PRR_ST5(x) PRR_ST5(y) PRR_ST5(z) PRR_ST5(w)
-#undef PRR_ST5
-    V4<T> k5 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
 #define PRR_ST6(c)                                                                                                 \
     zx.c = x.c + h * ((T)F::c6 * u.c + (T)F::B61 * k1.c + (T)F::B62 * k2.c + (T)F::B63 * k3.c + (T)F::B64 * k4.c); \
     zu.c = u.c + (T)F::A61 * k1.c + (T)F::A62 * k2.c + (T)F::A63 * k3.c + (T)F::A64 * k4.c + (T)F::A65 * k5.c;
+    V4<T> k1, k2, k3, k4, k5, k6, zx, zu;
+#ifdef PRR_STAGE_LOOP
+    // one geodesic call site; the stage index is warp-uniform, so the
+    // switch does not diverge, and every k stays in named registers
+    zx = x; zu = u;
+#pragma unroll 1
+    for (int s = 0; s < 6; s++) {
+        V4<T> g = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
+        switch (s) {
+        case 0: k1 = g; PRR_ST2(x) PRR_ST2(y) PRR_ST2(z) PRR_ST2(w) break;
+        case 1: k2 = g; PRR_ST3(x) PRR_ST3(y) PRR_ST3(z) PRR_ST3(w) break;
+        case 2: k3 = g; PRR_ST4(x) PRR_ST4(y) PRR_ST4(z) PRR_ST4(w) break;
+        case 3: k4 = g; PRR_ST5(x) PRR_ST5(y) PRR_ST5(z) PRR_ST5(w) break;
+        case 4: k5 = g; PRR_ST6(x) PRR_ST6(y) PRR_ST6(z) PRR_ST6(w) break;
+        default: k6 = g; break;
+        }
+    }
+#else
+    k1 = v4scl(h, phys_geod<T, GEOD>(q, x, u));
+    PRR_ST2(x) PRR_ST2(y) PRR_ST2(z) PRR_ST2(w)
+    k2 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
+    PRR_ST3(x) PRR_ST3(y) PRR_ST3(z) PRR_ST3(w)
+    k3 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
+    PRR_ST4(x) PRR_ST4(y) PRR_ST4(z) PRR_ST4(w)
+    k4 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
+    PRR_ST5(x) PRR_ST5(y) PRR_ST5(z) PRR_ST5(w)
+    k5 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
     PRR_ST6(x) PRR_ST6(y) PRR_ST6(z) PRR_ST6(w)
+    k6 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
+#endif
+#undef PRR_ST2
+#undef PRR_ST3
+#undef PRR_ST4
+#undef PRR_ST5
 #undef PRR_ST6
-    V4<T> k6 = v4scl(h, phys_geod<T, GEOD>(q, zx, zu));
 
     // increments, error estimate and scaled error norm
     T dxv[4], duv[4], err = 0;
