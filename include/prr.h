@@ -205,6 +205,31 @@ prr_status prr_trace_rays(prr_ctx *ctx, const prr_frame_desc *frame,
 prr_status prr_trace_rays_f64(prr_ctx *ctx, const prr_frame_desc *frame,
                               double *out_state, double *out_rgb, prr_stats *stats);
 
+/* ---- rendering without device allocation ----
+ * No counterpart in the reference (which allocates everything itself in
+ * main(), prr.cpp:359-378).  For callers that cannot allocate device memory
+ * while rendering - an application that reserves its whole device budget up
+ * front, work recorded into a CUDA graph, a real-time loop that must not pay
+ * cudaMalloc's implicit synchronisation.  Every input and output is the
+ * caller's: the frames (host array), the textures (PRR_MAX_TEXTURES device
+ * pointers to RGBA8 data, NULL = absent, with their sizes) and the outputs
+ * (device d_rgb8, and device d_rgbf, which frames with FXAA require: it
+ * receives the combined image the FXAA pass reads; without FXAA it receives
+ * the final float image and may be NULL).  PHYSICAL mode, FP32 or FP64,
+ * persistent schedule, no context.  The only scratch is one static device
+ * array of PRR_NOALLOC_SCRATCH_BYTES per device, so at most
+ * PRR_NOALLOC_MAX_FRAMES frames per call (more is PRR_ERR_INVALID).  Calls
+ * share that array: calls whose GPU work overlaps race, so order them on one
+ * stream.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  Asynchronous on `stream` (NULL = legacy default
+ * stream) once the frame table is on the device.  On failure a message is
+ * written to errbuf (errlen bytes, may be NULL). */
+#define PRR_NOALLOC_MAX_FRAMES 64
+#define PRR_NOALLOC_SCRATCH_BYTES 65536
+prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, const uint8_t *const *d_textures,
+                              const int32_t *tex_w, const int32_t *tex_h, uint8_t *d_rgb8, float *d_rgbf,
+                              void *stream, char *errbuf, size_t errlen);
+
 /* ---- scheduler tuning (new) ---- */
 prr_status prr_set_schedule(prr_ctx *ctx, int schedule, const prr_launch_config *cfg);
 prr_status prr_get_launch_config(prr_ctx *ctx, prr_launch_config *cfg);

@@ -27,7 +27,8 @@ INCLUDE = REPO / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NO_FMAD = {"k_reference.cu", "post.cu"}
-CU_SOURCES = ["capi.cu", "render.cu", "k_reference.cu", "post.cu", "k_persistent.cu", "k_plain.cu", "fma_peak.cu"]
+CU_SOURCES = ["capi.cu", "render.cu", "k_reference.cu", "post.cu", "k_persistent.cu", "k_plain.cu", "fma_peak.cu",
+              "noalloc.cu"]
 CPP_SOURCES = ["textures.cpp"]
 
 
