@@ -205,6 +205,22 @@ prr_status prr_trace_rays(prr_ctx *ctx, const prr_frame_desc *frame,
 prr_status prr_trace_rays_f64(prr_ctx *ctx, const prr_frame_desc *frame,
                               double *out_state, double *out_rgb, prr_stats *stats);
 
+/* ---- gradients (new; the reference has no derivative path) ----
+ * Discrete adjoint of a PHYSICAL-mode RKF45 frame (no FXAA): given
+ * dL_dimage (host, width*height*3 floats, the derivative of a scalar loss
+ * with respect to the combined image), returns in grads[5] the derivatives of
+ * the loss with respect to (spin a, mass M, camera inclination i [radians],
+ * camera distance r, orbital phase of sphere `sphere_index` about z
+ * [radians]; 0 when sphere_index is -1).  The frame must use an orbit camera:
+ * position (r sin i, 0, r cos i), yaw pi, pitch i - pi/2.  Step sizes and
+ * discrete events (accept/reject, termination, which sphere is hit) are
+ * frozen at the forward run; the forward run and the adjoint are FP64, the
+ * reduction is FP64.  The RMS2X2 sky is piecewise constant (zero gradient);
+ * use PRR_BG_BILINEAR for sky gradients.  stats->kernel_ms is the adjoint
+ * kernel time, stats->trace_ms the FP64 forward render time. */
+prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, const float *dL_dimage, int sphere_index,
+                       double grads[5], prr_stats *stats);
+
 /* ---- rendering without device allocation ----
  * No counterpart in the reference (which allocates everything itself in
  * main(), prr.cpp:359-378).  For callers that cannot allocate device memory

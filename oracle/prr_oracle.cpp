@@ -36,6 +36,78 @@
 
 namespace {
 
+// Unqualified math calls: float/double resolve to the std overloads (float
+// stays float, as in the reference's host build); the dual numbers of the
+// gradient path resolve to their own overloads.
+using std::acos;
+using std::atan2;
+using std::fabs;
+using std::floor;
+using std::fmax;
+using std::fmin;
+using std::isnan;
+using std::pow;
+using std::sqrt;
+using std::sin;
+using std::cos;
+
+// Forward-mode dual number v + sum_k d[k] e_k for the FP64 host gradient.
+// Comparisons use the value, so every branch (accept/reject, termination,
+// hit) is decided by the primal run; pow() carries no derivative, so the
+// step sizes the controller picks are frozen.
+template <int N> struct HD {
+    double v = 0.0;
+    double d[N] = {};
+    HD() = default;
+    HD(double x) : v(x) {}
+    static HD var(double x, int k) { HD r(x); r.d[k] = 1.0; return r; }
+    explicit operator double() const { return v; }
+    explicit operator float() const { return (float)v; }
+    explicit operator int() const { return (int)v; }
+};
+template <int N> HD<N> operator+(const HD<N> &a, const HD<N> &b) { HD<N> r(a.v + b.v); for (int k = 0; k < N; k++) r.d[k] = a.d[k] + b.d[k]; return r; }
+template <int N> HD<N> operator-(const HD<N> &a, const HD<N> &b) { HD<N> r(a.v - b.v); for (int k = 0; k < N; k++) r.d[k] = a.d[k] - b.d[k]; return r; }
+template <int N> HD<N> operator*(const HD<N> &a, const HD<N> &b) { HD<N> r(a.v * b.v); for (int k = 0; k < N; k++) r.d[k] = a.d[k] * b.v + a.v * b.d[k]; return r; }
+template <int N> HD<N> operator/(const HD<N> &a, const HD<N> &b) { HD<N> r(a.v / b.v); for (int k = 0; k < N; k++) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v; return r; }
+template <int N> HD<N> operator-(const HD<N> &a) { HD<N> r(-a.v); for (int k = 0; k < N; k++) r.d[k] = -a.d[k]; return r; }
+template <int N> HD<N> &operator+=(HD<N> &a, const HD<N> &b) { return a = a + b; }
+template <int N> HD<N> &operator-=(HD<N> &a, const HD<N> &b) { return a = a - b; }
+template <int N> HD<N> &operator*=(HD<N> &a, const HD<N> &b) { return a = a * b; }
+template <int N> HD<N> operator+(const HD<N> &a, double b) { return a + HD<N>(b); }
+template <int N> HD<N> operator-(const HD<N> &a, double b) { return a - HD<N>(b); }
+template <int N> HD<N> operator*(const HD<N> &a, double b) { return a * HD<N>(b); }
+template <int N> HD<N> operator/(const HD<N> &a, double b) { return a / HD<N>(b); }
+template <int N> HD<N> operator+(double a, const HD<N> &b) { return HD<N>(a) + b; }
+template <int N> HD<N> operator-(double a, const HD<N> &b) { return HD<N>(a) - b; }
+template <int N> HD<N> operator*(double a, const HD<N> &b) { return HD<N>(a) * b; }
+template <int N> HD<N> operator/(double a, const HD<N> &b) { return HD<N>(a) / b; }
+#define PRR_HD_CMP(OP)                                                                              \
+    template <int N> bool operator OP(const HD<N> &a, const HD<N> &b) { return a.v OP b.v; }      \
+    template <int N> bool operator OP(const HD<N> &a, double b) { return a.v OP b; }               \
+    template <int N> bool operator OP(double a, const HD<N> &b) { return a OP b.v; }
+PRR_HD_CMP(<) PRR_HD_CMP(>) PRR_HD_CMP(<=) PRR_HD_CMP(>=) PRR_HD_CMP(==) PRR_HD_CMP(!=)
+#undef PRR_HD_CMP
+template <int N> HD<N> hd_chain(const HD<N> &a, double f, double df) { HD<N> r(f); for (int k = 0; k < N; k++) r.d[k] = df * a.d[k]; return r; }
+template <int N> HD<N> sqrt(const HD<N> &a) { double s = std::sqrt(a.v); return hd_chain(a, s, s > 0 ? 0.5 / s : 0.0); }
+template <int N> HD<N> sin(const HD<N> &a) { return hd_chain(a, std::sin(a.v), std::cos(a.v)); }
+template <int N> HD<N> cos(const HD<N> &a) { return hd_chain(a, std::cos(a.v), -std::sin(a.v)); }
+template <int N> HD<N> acos(const HD<N> &a) { double s = 1 - a.v * a.v; return hd_chain(a, std::acos(a.v), s > 0 ? -1 / std::sqrt(s) : 0.0); }
+template <int N> HD<N> atan2(const HD<N> &y, const HD<N> &x)
+{
+    HD<N> r(std::atan2(y.v, x.v));
+    double den = x.v * x.v + y.v * y.v;
+    for (int k = 0; k < N; k++) r.d[k] = den > 0 ? (x.v * y.d[k] - y.v * x.d[k]) / den : 0.0;
+    return r;
+}
+template <int N> HD<N> fabs(const HD<N> &a) { return a.v < 0 ? -a : a; }
+template <int N> HD<N> fmax(const HD<N> &a, const HD<N> &b) { return a.v >= b.v ? a : b; }
+template <int N> HD<N> fmin(const HD<N> &a, const HD<N> &b) { return a.v <= b.v ? a : b; }
+template <int N> HD<N> floor(const HD<N> &a) { return HD<N>(std::floor(a.v)); }
+template <int N> HD<N> pow(const HD<N> &a, const HD<N> &b) { return HD<N>(std::pow(a.v, b.v)); }
+template <int N> bool isnan(const HD<N> &a) { return std::isnan(a.v); }
+template <int N> HD<N> add_d(HD<N> x, double c) { return x + c; }
+template <int N> HD<N> div_d(HD<N> x, double c) { return x / c; }
+
 const double PI_BASE = 3.14159265358979323846;  // main/base.h:20
 const double PI_SPHERE = 3.14159265359;          // scene/sphere.h:16 (redefines PI)
 
@@ -65,10 +137,15 @@ template <class T> inline V3<T> tex_at(const Tex &t, int i, int j)
 // tex2d::operator[](f2): bilinear; the cell index is clamped to [0, res-2]
 // AFTER the fraction is taken, so uv outside the interior extrapolates
 // (cudamaths/tex2d.cuh:112-119).
+// Texel cells read by the last colour lookup of this thread (hashed), part of
+// the per-pixel event signature of prr_oracle_grad.
+thread_local unsigned long long g_cells = 0;
+
 template <class T> inline V3<T> tex_bilinear(const Tex &t, T u, T v)
 {
     T ux = u * (T)t.w, uy = v * (T)t.h;
-    int ix = (int)std::floor(ux), iy = (int)std::floor(uy);
+    int ix = (int)floor(ux), iy = (int)floor(uy);
+    g_cells = g_cells * 1315423911ULL + (unsigned long long)(ix * 8191 + iy);
     T px = ux - (T)ix, py = uy - (T)iy;
     ix = ix < 0 ? 0 : (ix > t.w - 2 ? t.w - 2 : ix);
     iy = iy < 0 ? 0 : (iy > t.h - 2 ? t.h - 2 : iy);
@@ -82,8 +159,8 @@ template <class T> inline V3<T> tex_bilinear(const Tex &t, T u, T v)
     return r;
 }
 
-template <class T> inline T fmaxT(T a, T b) { return std::fmax(a, b); }
-template <class T> inline T fminT(T a, T b) { return std::fmin(a, b); }
+template <class T> inline T fmaxT(T a, T b) { return fmax(a, b); }
+template <class T> inline T fminT(T a, T b) { return fmin(a, b); }
 
 struct Scene {
     const prr_frame_desc *d;
@@ -97,22 +174,22 @@ template <class T> inline T ks_r(T x, T y, T z, T a)
 {
     T R2 = x * x + y * y + z * z;
     T b = R2 - a * a;
-    T S = std::sqrt(b * b + (T)4 * a * a * z * z);
-    return std::sqrt((T)0.5 * (b + S));
+    T S = sqrt(b * b + (T)4 * a * a * z * z);
+    return sqrt((T)0.5 * (b + S));
 }
 
 template <class T> inline T r_plus(T M, T a)
 {
     T d = M * M - a * a;
-    return M + std::sqrt(d > 0 ? d : (T)0);
+    return M + sqrt(d > 0 ? d : (T)0);
 }
 
 // f, l_mu and spatial derivatives (index order x, y, z, t).
 template <class T> void ks_fields(T x, T y, T z, T M, T a, T &f, T l[4], T df[3], T dl[4][3])
 {
     T R2 = x * x + y * y + z * z, a2 = a * a, b = R2 - a2;
-    T S = std::sqrt(b * b + (T)4 * a2 * z * z);
-    T r2 = (T)0.5 * (b + S), r = std::sqrt(r2);
+    T S = sqrt(b * b + (T)4 * a2 * z * z);
+    T r2 = (T)0.5 * (b + S), r = sqrt(r2);
     T dr[3] = {x * r / S, y * r / S, z * (r2 + a2) / (r * S)};
     T q = r2 + a2, Sig = r2 * r2 + a2 * z * z;
     f = (T)2 * M * r2 * r / Sig;
@@ -169,7 +246,7 @@ template <class T> V4<T> geod_table(const V4<T> &p, const V4<T> &u, T M, T a)
 inline V4<float> geod_schw_ref(const V4<float> &p, const V4<float> &u, float rs)
 {
     V4<float> du;
-    float r = std::sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
+    float r = sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
     float x2 = p.x * p.x, y2 = p.y * p.y, z2 = p.z * p.z;
     float Phi = (r * (x2 - 2.0f * y2 - 2.0f * z2) + rs * x2) * u.x * u.x
               + (r * (-2.0f * x2 + y2 - 2.0f * z2) + rs * y2) * u.y * u.y
@@ -206,7 +283,7 @@ template <class T> void metric_ks(const V4<T> &p, T M, T a, T g[16])
 // metrics/schwarzschild.cuh:123-141 in FP32 order.
 inline void metric_schw_ref(const V4<float> &p, float rs, float g[16])
 {
-    float ir = 1.0f / std::sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
+    float ir = 1.0f / sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
     float ir2 = ir * ir, ir3 = ir2 * ir;
     g[0] = 1.0f + rs * p.x * p.x * ir3; g[1] = rs * p.x * p.y * ir3; g[2] = rs * p.x * p.z * ir3; g[3] = rs * p.x * ir2;
     g[4] = g[1]; g[5] = 1.0f + rs * p.y * p.y * ir3; g[6] = rs * p.y * p.z * ir3; g[7] = rs * p.y * ir2;
@@ -219,7 +296,7 @@ template <class T> struct Metric {
     T M, a, rs;
     V4<T> geod(const V4<T> &p, const V4<T> &u, bool refmode) const;
     void metric(const V4<T> &p, T g[16], bool refmode) const;
-    T radius(const V4<T> &p) const { return kind == PRR_METRIC_KERR ? ks_r<T>(p.x, p.y, p.z, a) : std::sqrt(p.x * p.x + p.y * p.y + p.z * p.z); }
+    T radius(const V4<T> &p) const { return kind == PRR_METRIC_KERR ? ks_r<T>(p.x, p.y, p.z, a) : sqrt(p.x * p.x + p.y * p.y + p.z * p.z); }
     T horizon() const { return kind == PRR_METRIC_SCHWARZSCHILD ? rs : (kind == PRR_METRIC_KERR ? r_plus<T>(M, a) : (T)0); }
 };
 
@@ -243,39 +320,66 @@ template <> void Metric<double>::metric(const V4<double> &p, double g[16], bool)
 {
     metric_ks<double>(p, kind == PRR_METRIC_FLAT ? 0.0 : M, kind == PRR_METRIC_KERR ? a : 0.0, g);
 }
+// any other T (the dual numbers of the gradient path)
+template <class T> V4<T> Metric<T>::geod(const V4<T> &p, const V4<T> &u, bool) const
+{
+    if (kind == PRR_METRIC_FLAT) return {T(0.0), T(0.0), T(0.0), T(0.0)};
+    return geod_table<T>(p, u, M, kind == PRR_METRIC_KERR ? a : T(0.0));
+}
+template <class T> void Metric<T>::metric(const V4<T> &p, T g[16], bool) const
+{
+    metric_ks<T>(p, kind == PRR_METRIC_FLAT ? T(0.0) : M, kind == PRR_METRIC_KERR ? a : T(0.0), g);
+}
 
 // ---------------------------------------------------------------- scene
 
-struct Hit { bool hit; V3<float> c; };
+template <class T> struct Hit { bool hit; V3<T> c; };
+
+// `x + c` and `x / c` with a double constant, as the reference writes them
+// (float + double -> double, stored to float).  Dual numbers keep their
+// derivatives.
+template <class T> inline T add_d(T x, double c) { return (T)((double)x + c); }
+template <class T> inline T div_d(T x, double c) { return (T)((double)x / c); }
+
+// Orbit camera and sphere-phase parameters of the gradient path (T-valued so
+// that dual numbers carry d/dparameter through the initial data and the
+// hit point).
+template <class T> struct Orbit {
+    T cam_r, incl;     // camera at (r sin i, 0, r cos i), yaw pi, pitch i - pi/2
+    int sphere;        // index of the sphere on the orbit (-1: none)
+    T sph_R, sph_phase, sph_z;
+};
 
 // Sphere::intersects + Sphere::getColor (scene/sphere.h:34-64) and the
 // closest-hit loop of Spacetime::IntersectsScene (main/Spacetime.h:38-46).
 // The sphere geometry and texture arithmetic is done in T.
-template <class T> Hit intersect_scene(const Scene &sc, const V3<T> &p, V3<T> v, T h)
+template <class T> Hit<T> intersect_scene(const Scene &sc, const V3<T> &p, V3<T> v, T h, const Orbit<T> *orb = nullptr)
 {
     T best_d = (T)100000000000.0, cx = -1, cy = -1, cz = -1;
     bool any = false;
     const prr_frame_desc *d = sc.d;
     // v.normalize(): k = 1/|v|; v *= k
-    T k = (T)1 / std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+    T k = (T)1 / sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
     v.x *= k; v.y *= k; v.z *= k;
     for (int s = 0; s < d->nspheres; s++) {
         const prr_sphere &S = d->spheres[s];
         V3<T> c = {(T)S.center[0], (T)S.center[1], (T)S.center[2]};
+        if (orb && orb->sphere == s)
+            c = {orb->sph_R * cos(orb->sph_phase), orb->sph_R * sin(orb->sph_phase), orb->sph_z};
         T rad = (T)S.radius;
         T v2 = v.x * v.x + v.y * v.y + v.z * v.z;
         V3<T> pc = {p.x - c.x, p.y - c.y, p.z - c.z};
         T dvp = v.x * pc.x + v.y * pc.y + v.z * pc.z;
         T disc = dvp * dvp - v2 * ((pc.x * pc.x + pc.y * pc.y + pc.z * pc.z) - rad * rad);
         if (disc < 0) continue;
-        T dd = ((T)(-2.0f) * dvp - std::sqrt(disc)) / v2;
+        T dd = ((T)(-2.0f) * dvp - sqrt(disc)) / v2;
         if (dd * dd > v2 * h) continue;
         if (dd < 0) continue;
         // getColor((p + v*d) - c)
         V3<T> in = {(p.x + v.x * dd) - c.x, (p.y + v.y * dd) - c.y, (p.z + v.z * dd) - c.z};
-        T theta = std::acos(in.z / rad);
-        T phi = (T)((double)std::atan2(in.y, in.x) + PI_SPHERE);
-        T uu = (T)((double)phi / (2.0 * PI_SPHERE)), vv = (T)((double)theta / PI_SPHERE);
+        T theta = acos(in.z / rad);
+        T phi = add_d(atan2(in.y, in.x), PI_SPHERE);
+        T uu = div_d(phi, 2.0 * PI_SPHERE), vv = div_d(theta, PI_SPHERE);
         const T uvmax = (T)0.999999999f;
         uu = fminT<T>(fmaxT<T>(uu, (T)0), uvmax);
         vv = fminT<T>(fmaxT<T>(vv, (T)0), uvmax);
@@ -287,9 +391,9 @@ template <class T> Hit intersect_scene(const Scene &sc, const V3<T> &p, V3<T> v,
             best_d = dd; cx = col.x; cy = col.y; cz = col.z; any = true;
         }
     }
-    Hit r;
+    Hit<T> r;
     r.hit = any && cx >= 0;
-    r.c = {(float)cx, (float)cy, (float)cz};
+    r.c = {cx, cy, cz};
     return r;
 }
 
@@ -297,40 +401,41 @@ template <class T> Hit intersect_scene(const Scene &sc, const V3<T> &p, V3<T> v,
 // block at floor(uv); a single texel on the last row/column.
 template <class T> V3<T> background_rms(const Tex &t, const V4<T> &u)
 {
-    T k = (T)1 / std::sqrt(u.x * u.x + u.y * u.y + u.z * u.z);
+    T k = (T)1 / sqrt(u.x * u.x + u.y * u.y + u.z * u.z);
     V3<T> n = {u.x * k, u.y * k, u.z * k};
-    T theta = std::acos(n.z);
-    T phi = std::atan2(n.y, n.x);
+    T theta = acos(n.z);
+    T phi = atan2(n.y, n.x);
     phi = (phi >= 0 ? phi : (T)((double)phi + 2.0 * PI_BASE));
     if ((double)phi > 2.0 * PI_BASE || phi < 0) return {(T)0.5, (T)0.5, (T)0};
     if (theta < 0 || (double)theta > PI_BASE) return {(T)0, (T)0.5, (T)0.8};
     T ux = (T)((double)phi / (2.0 * PI_BASE) * t.w), uy = (T)((double)theta / PI_BASE * t.h);
-    int px = (int)std::floor(ux), py = (int)std::floor(uy);
+    int px = (int)floor(ux), py = (int)floor(uy);
     if (px == t.w) px -= 1;
     if (py == t.h) py -= 1;
     if (px < 0 || px >= t.w || py < 0 || py >= t.h) return {(T)0, (T)0.5, (T)0};
     if (px == t.w - 1 || py == t.h - 1) return tex_at<T>(t, px, py);
     V3<T> a = tex_at<T>(t, px, py), b = tex_at<T>(t, px, py + 1), c = tex_at<T>(t, px + 1, py), d = tex_at<T>(t, px + 1, py + 1);
     const T q = (T)0.25;
-    return {std::sqrt(q * (a.x * a.x + b.x * b.x + c.x * c.x + d.x * d.x)),
-            std::sqrt(q * (a.y * a.y + b.y * b.y + c.y * c.y + d.y * d.y)),
-            std::sqrt(q * (a.z * a.z + b.z * b.z + c.z * c.z + d.z * d.z))};
+    return {sqrt(q * (a.x * a.x + b.x * b.x + c.x * c.x + d.x * d.x)),
+            sqrt(q * (a.y * a.y + b.y * b.y + c.y * c.y + d.y * d.y)),
+            sqrt(q * (a.z * a.z + b.z * b.z + c.z * c.z + d.z * d.z))};
 }
 
 // Continuous lookup (PRR_BG_BILINEAR): bilinear over texel centres, wrap in
 // longitude, clamp in latitude.
 template <class T> V3<T> background_bilinear(const Tex &t, const V4<T> &u)
 {
-    T k = (T)1 / std::sqrt(u.x * u.x + u.y * u.y + u.z * u.z);
+    T k = (T)1 / sqrt(u.x * u.x + u.y * u.y + u.z * u.z);
     T nz = u.z * k;
     nz = nz > 1 ? 1 : (nz < -1 ? -1 : nz);
-    T theta = std::acos(nz);
-    T phi = std::atan2(u.y, u.x);
+    T theta = acos(nz);
+    T phi = atan2(u.y, u.x);
     if (phi < 0) phi += (T)(2.0 * PI_BASE);
     T fx = phi / (T)(2.0 * PI_BASE) * t.w - (T)0.5, fy = theta / (T)PI_BASE * t.h - (T)0.5;
-    T flx = std::floor(fx), fly = std::floor(fy);
+    T flx = floor(fx), fly = floor(fy);
     T wx = fx - flx, wy = fy - fly;
     int x0 = (int)flx, y0 = (int)fly;
+    g_cells = g_cells * 1315423911ULL + (unsigned long long)(x0 * 8191 + y0);
     int x1 = x0 + 1, y1 = y0 + 1;
     x0 = ((x0 % t.w) + t.w) % t.w; x1 = ((x1 % t.w) + t.w) % t.w;
     y0 = y0 < 0 ? 0 : (y0 > t.h - 1 ? t.h - 1 : y0);
@@ -349,6 +454,8 @@ template <class T> struct RayState {
     V4<T> r, u;
     long long accepted = 0, attempts = 0;
     V3<float> rgb;
+    V3<T> rgbT;  // the same colour in T (gradient path)
+    unsigned long long cells = 0;  // texel cells read for the colour (finite-difference tests)
 };
 
 // createRays_none / createRays_regular
@@ -393,10 +500,10 @@ struct Tableau {
 
 template <class T> inline V4<T> add(const V4<T> &a, const V4<T> &b) { return {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
 template <class T> inline V4<T> scl(T s, const V4<T> &a) { return {a.x * s, a.y * s, a.z * s, a.w * s}; }
-template <class T> inline bool isnan4(const V4<T> &a) { return std::isnan(a.x) || std::isnan(a.y) || std::isnan(a.z) || std::isnan(a.w); }
+template <class T> inline bool isnan4(const V4<T> &a) { return isnan(a.x) || isnan(a.y) || isnan(a.z) || isnan(a.w); }
 template <class T> inline T max4abs(const V4<T> &a, const V4<T> &b)
 {
-    return fmaxT<T>(fmaxT<T>(fmaxT<T>(std::fabs(a.x - b.x), std::fabs(a.y - b.y)), std::fabs(a.z - b.z)), std::fabs(a.w - b.w));
+    return fmaxT<T>(fmaxT<T>(fmaxT<T>(fabs(a.x - b.x), fabs(a.y - b.y)), fabs(a.z - b.z)), fabs(a.w - b.w));
 }
 
 template <class T> class Tracer {
@@ -412,6 +519,17 @@ public:
                                                                 : mt_.horizon() + (T)d_->horizon_eps;
     }
 
+    // Gradient path: mass and spin as given (dual numbers), camera and one
+    // sphere from `orb`.
+    Tracer(const Scene &sc, T M, T a, const Orbit<T> *orb) : Tracer(sc)
+    {
+        mt_.M = M;
+        mt_.a = a;
+        mt_.rs = (T)2 * M;
+        rstop_ = T((double)(mt_.horizon() + (T)d_->horizon_eps));  // the stop radius is an event threshold
+        orb_ = orb;
+    }
+
     RayState<T> run(long long rid) const
     {
         RayState<T> R;
@@ -422,7 +540,9 @@ public:
         init(R);
         if (d_->solver == PRR_SOLVER_EULER) euler(R);
         else rkf(R);
+        g_cells = 0;
         colour(R);
+        R.cells = g_cells;
         return R;
     }
 
@@ -432,19 +552,34 @@ private:
     Metric<T> mt_;
     bool ref_;
     T rstop_;
+    const Orbit<T> *orb_ = nullptr;
 
     // initRays (kernels/solver.cuh:26-56)
     void init(RayState<T> &R) const
     {
-        V3<float> dir = ray_dir(d_, (float)R.uvx, (float)R.uvy);
-        R.r = {(T)d_->cam_pos[0], (T)d_->cam_pos[1], (T)d_->cam_pos[2], (T)0};
-        V4<T> u = {(T)dir.x, (T)dir.y, (T)dir.z, (T)1};
+        V4<T> u;
+        if (orb_) {
+            // Camera::rayDir_Spherical with a = pi, b = i - pi/2, evaluated in T
+            const double PI = 3.14159265358979323846;
+            T beta = orb_->incl - (T)(0.5 * PI);
+            double nu = (0.5 - (double)R.uvy) * (double)d_->vfov;
+            double mu = (0.5 - (double)R.uvx) * (double)d_->width / (double)d_->height * (double)d_->vfov;
+            T cb = cos(beta + (T)nu);
+            T dx = cb * (T)std::cos(PI + mu), dy = cb * (T)std::sin(PI + mu), dz = sin(beta + (T)nu);
+            T k = (T)1 / sqrt(dx * dx + dy * dy + dz * dz);
+            R.r = {orb_->cam_r * sin(orb_->incl), (T)0, orb_->cam_r * cos(orb_->incl), (T)0};
+            u = {dx * k, dy * k, dz * k, (T)1};
+        } else {
+            V3<float> dir = ray_dir(d_, (float)R.uvx, (float)R.uvy);
+            R.r = {(T)d_->cam_pos[0], (T)d_->cam_pos[1], (T)d_->cam_pos[2], (T)0};
+            u = {(T)dir.x, (T)dir.y, (T)dir.z, (T)1};
+        }
         T g[16];
         mt_.metric(R.r, g, ref_);
         T a = g[15];
         T b = (T)2 * (g[12] * u.x + g[13] * u.y + g[14] * u.z);
         T c = g[0] * u.x * u.x + g[5] * u.y * u.y + g[10] * u.z * u.z + (T)2 * (g[1] * u.x * u.y + g[2] * u.x * u.z + g[6] * u.y * u.z);
-        T rt = std::sqrt(b * b - (T)4 * a * c);
+        T rt = sqrt(b * b - (T)4 * a * c);
         T u0 = fmaxT<T>((-b + rt) / ((T)2 * a), (-b - rt) / ((T)2 * a));
         if (u0 < 0) u0 = 1;
         if (ref_) u = scl(u0, u);  // whole 4-vector scaled (solver.cuh:54)
@@ -454,7 +589,7 @@ private:
 
     bool user_update(RayState<T> &R, T h) const
     {
-        Hit c = intersect_scene<T>(sc_, {R.r.x, R.r.y, R.r.z}, {R.u.x, R.u.y, R.u.z}, h);
+        Hit<T> c = intersect_scene<T>(sc_, {R.r.x, R.r.y, R.r.z}, {R.u.x, R.u.y, R.u.z}, h, orb_);
         if (c.hit) { R.result = PRR_RESULT_INTERSECTION; return false; }
         return true;
     }
@@ -464,9 +599,9 @@ private:
         T r = mt_.radius(R.r);
         bool horizon = d_->metric != PRR_METRIC_FLAT && r <= rstop_;
         if (r >= (T)d_->rout || horizon) { R.result = PRR_RESULT_SUCCESS; return false; }
-        Hit c = intersect_scene<T>(sc_, {R.r.x, R.r.y, R.r.z}, {R.u.x, R.u.y, R.u.z}, th);
+        Hit<T> c = intersect_scene<T>(sc_, {R.r.x, R.r.y, R.r.z}, {R.u.x, R.u.y, R.u.z}, th, orb_);
         if (c.hit) {
-            R.u = {(T)c.c.x, (T)c.c.y, (T)c.c.z, (T)0};
+            R.u = {c.c.x, c.c.y, c.c.z, (T)0};
             R.result = PRR_RESULT_INTERSECTION;
             return false;
         }
@@ -547,18 +682,18 @@ private:
             T maxerr;
             if (ref_) {
                 maxerr = fmaxT<T>(max4abs(__x, _x), max4abs(__u, _u));
-                _h = (T)0.9f * h * (T)std::pow((T)(eps / maxerr), (T)0.2f);
+                _h = (T)0.9f * h * (T)pow((T)(eps / maxerr), (T)0.2f);
             } else {
                 // mixed error norm: max_i |y5_i - y4_i| / (atol + rtol*max(|y_i|, |y4_i|))
                 const T *a0 = &x.x, *a1 = &_x.x, *a2 = &__x.x, *b0 = &u.x, *b1 = &_u.x, *b2 = &__u.x;
                 maxerr = 0;
                 for (int c = 0; c < 4; c++) {
-                    T sx = atol + rtol * fmaxT<T>(std::fabs(a0[c]), std::fabs(a1[c]));
-                    T su = atol + rtol * fmaxT<T>(std::fabs(b0[c]), std::fabs(b1[c]));
-                    maxerr = fmaxT<T>(maxerr, std::fabs(a2[c] - a1[c]) / sx);
-                    maxerr = fmaxT<T>(maxerr, std::fabs(b2[c] - b1[c]) / su);
+                    T sx = atol + rtol * fmaxT<T>(fabs(a0[c]), fabs(a1[c]));
+                    T su = atol + rtol * fmaxT<T>(fabs(b0[c]), fabs(b1[c]));
+                    maxerr = fmaxT<T>(maxerr, fabs(a2[c] - a1[c]) / sx);
+                    maxerr = fmaxT<T>(maxerr, fabs(b2[c] - b1[c]) / su);
                 }
-                _h = (T)0.9 * h * std::pow((T)1 / maxerr, (T)0.2);
+                _h = (T)0.9 * h * pow((T)1 / maxerr, (T)0.2);
             }
             _h = fminT<T>(fmaxT<T>(_h, hmin), hmax);
 
@@ -607,6 +742,7 @@ private:
         } else set_black = true;
         if (set_black) c = {black[0], black[1], black[2]};
         R.rgb = {(float)c.x, (float)c.y, (float)c.z};
+        R.rgbT = c;
     }
 };
 
@@ -753,6 +889,91 @@ int prr_oracle_trace(const prr_frame_desc *d, const uint8_t *const *tex, const i
 }
 
 // SSAA combine and optional FXAA of per-sample colours (rgb: W*H*S*3).
+// FP64 host gradient of sum(dL_dimage * image) with respect to (spin, mass,
+// camera inclination, camera distance, orbital phase of sphere
+// `sphere_index`), by forward-mode dual numbers through the PHYSICAL-mode
+// trace with the step sizes and discrete events of the primal run frozen -
+// the same discrete map the GPU adjoint differentiates in reverse.  The frame
+// must use an orbit camera (position (r sin i, 0, r cos i)).  image_out
+// (optional, W*H*3) receives the combined image of the primal run.
+// params (optional) overrides the parameter values taken from the frame:
+// (spin, mass, inclination, camera distance, sphere phase), in FP64 - the
+// finite-difference tests perturb them below float resolution.
+// loss_out (optional) receives sum(dL_dimage * image) in FP64; sig_out
+// (optional, one per pixel) a signature of the pixel's discrete events (each
+// sample's result and accepted-step count) for finite-difference tests.
+int prr_oracle_grad(const prr_frame_desc *d, const uint8_t *const *tex, const int *tw, const int *th,
+                    const float *dL_dimage, int sphere_index, int nthreads, double grads[5], double *image_out,
+                    const double *params, double *loss_out, long long *sig_out)
+{
+    typedef HD<5> D;
+    if (!d || !dL_dimage || !grads || d->mode != PRR_MODE_PHYSICAL || d->fxaa) return 1;
+    Scene sc = make_scene(d, tex, tw, th);
+    double px = d->cam_pos[0], py = d->cam_pos[1], pz = d->cam_pos[2];
+    double r = std::sqrt(px * px + py * py + pz * pz);
+    double pv[5] = {d->metric == PRR_METRIC_KERR ? (double)d->spin : 0.0, (double)d->mass, std::acos(pz / r), r, 0.0};
+    Orbit<D> orb;
+    orb.sphere = sphere_index;
+    if (sphere_index >= 0 && sphere_index < d->nspheres) {
+        const prr_sphere &S = d->spheres[sphere_index];
+        orb.sph_R = D(std::hypot((double)S.center[0], (double)S.center[1]));
+        pv[4] = std::atan2((double)S.center[1], (double)S.center[0]);
+        orb.sph_z = D((double)S.center[2]);
+    } else orb.sphere = -1;
+    if (params)
+        for (int k = 0; k < 5; k++) pv[k] = params[k];
+    orb.incl = D::var(pv[2], 2);
+    orb.cam_r = D::var(pv[3], 3);
+    orb.sph_phase = D::var(pv[4], 4);
+    D M = D::var(pv[1], 1), a = D::var(pv[0], 0);
+    Tracer<D> tr(sc, M, a, &orb);
+    const long long npx = (long long)d->width * d->height;
+    const int S = d->samples;
+    double acc[5] = {0, 0, 0, 0, 0}, loss = 0.0;
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+    {
+        double loc[5] = {0, 0, 0, 0, 0}, loc_loss = 0.0;
+#pragma omp for schedule(dynamic, 8)
+        for (long long p = 0; p < npx; p++) {
+            D I[3];
+            long long sig = 0;
+            if (S == 1) {
+                RayState<D> R = tr.run(p);
+                sig = R.result * 1000003LL + R.accepted + (long long)(R.cells * 7919ULL);
+                const D c[3] = {R.rgbT.x, R.rgbT.y, R.rgbT.z};
+                for (int k = 0; k < 3; k++) I[k] = c[k].v <= 0 ? D(0.0) : (c[k].v >= 1 ? D(1.0) : c[k]);
+            } else {
+                D sum[3] = {D(0.0), D(0.0), D(0.0)};
+                for (int s = 0; s < S; s++) {
+                    RayState<D> R = tr.run(p * S + s);
+                    sig = sig * 31 + R.result * 1000003LL + R.accepted + (long long)(R.cells * 7919ULL);
+                    const D c[3] = {R.rgbT.x, R.rgbT.y, R.rgbT.z};
+                    for (int k = 0; k < 3; k++) {
+                        D c2 = c[k] * c[k];
+                        sum[k] += c2.v <= 0 ? D(0.0) : (c2.v >= 1 ? D(1.0) : c2);
+                    }
+                }
+                for (int k = 0; k < 3; k++) I[k] = sqrt(sum[k] / (double)S);
+            }
+            for (int k = 0; k < 3; k++) {
+                double g = dL_dimage[3 * p + k];
+                for (int j = 0; j < 5; j++) loc[j] += g * I[k].d[j];
+                loc_loss += g * I[k].v;
+                if (image_out) image_out[3 * p + k] = I[k].v;
+            }
+            if (sig_out) sig_out[p] = sig;
+        }
+#pragma omp critical
+        {
+            for (int j = 0; j < 5; j++) acc[j] += loc[j];
+            loss += loc_loss;
+        }
+    }
+    for (int j = 0; j < 5; j++) grads[j] = acc[j];
+    if (loss_out) *loss_out = loss;
+    return 0;
+}
+
 int prr_oracle_post(const float *rgb, int w, int h, int samples, int do_fxaa, float *image)
 {
     size_t npix = (size_t)w * h;

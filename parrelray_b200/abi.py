@@ -97,6 +97,7 @@ SIGNATURES = {
     "prr_make_texture": (C.c_int, [C.c_int, C.c_uint32, C.c_int, C.c_int, _u8p]),
     "prr_frame_desc_defaults": (None, [C.POINTER(FrameDesc)]),
     "prr_sizeof": (C.c_size_t, [C.c_int]),
+    "prr_adjoint": (C.c_int, [_P, C.POINTER(FrameDesc), _fp, C.c_int, _dp, C.POINTER(Stats)]),
     "prr_render_noalloc": (C.c_int, [C.POINTER(FrameDesc), C.c_int, C.POINTER(_P), C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), _P, _P, _P, C.c_char_p, C.c_size_t]),
 }

@@ -73,6 +73,17 @@ cudaError_t launch_plain_frame(const FrameParams *d_fp, const FrameParams &h_fp,
                                unsigned long long *counters, int geod_table, cudaStream_t st, int *launches);
 size_t plain_ray_record_bytes();
 
+// k_adjoint.cu: discrete adjoint of one PHYSICAL frame (FP64).
+struct AdjointParamsHost {
+    double spin, mass, incl, cam_r, phase, sph_R, sph_z;
+    int sphere;
+};
+cudaError_t launch_adjoint(const FrameParams *d_fp, const AdjointParamsHost &p, const float *dL, const float *image,
+                           void *ckpt, int max_ckpt, int threads_total, double *grad, unsigned long long *counters,
+                           long long nrays, cudaStream_t st);
+size_t adjoint_checkpoint_bytes();
+constexpr int ADJ_CHECKPOINT_INTERVAL = 64;
+
 // fma_peak.cu
 cudaError_t launch_fma_peak(float *sink, int blocks, int threads, int iters, cudaStream_t st);
 cudaError_t launch_dfma_peak(double *sink, int blocks, int threads, int iters, cudaStream_t st);

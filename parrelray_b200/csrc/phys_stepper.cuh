@@ -182,9 +182,12 @@ enum StepStatus { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_FLAG64 = 2 };
 // One RKF45 attempt plus, when accepted, the hooks.  Returns STEP_DONE with
 // `result` and `colour` set when the ray has terminated, STEP_FLAG64 when a
 // split-precision render must re-integrate it in FP64.
+// hit_sphere: when non-null, an INTERSECTION stores the hit sphere's index
+// there and leaves the final state in R (otherwise R.u receives the colour,
+// as User_ENDLOOP does).
 template <class T, int GEOD>
 PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, int &result, V3<float> &colour,
-                         T flag_r)
+                         T flag_r, int *hit_sphere = nullptr)
 {
     using F = Fehlberg;
     if (!(R.l < (T)1000)) { result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0}; return STEP_DONE; }
@@ -325,7 +328,8 @@ PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, 
     if (candE >= 0) {
         result = PRR_RESULT_INTERSECTION;
         colour = sphere_colour<T>(fp.sph[candE], xn.x, xn.y, xn.z, vx, vy, vz, dE);
-        R.u = {(T)colour.x, (T)colour.y, (T)colour.z, (T)0};
+        if (hit_sphere) *hit_sphere = candE;  // the caller keeps the final state
+        else R.u = {(T)colour.x, (T)colour.y, (T)colour.z, (T)0};
         return STEP_DONE;
     }
     if (flag_r > (T)0 && r2 < flag_r * flag_r) return STEP_FLAG64;

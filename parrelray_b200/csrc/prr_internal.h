@@ -37,10 +37,11 @@ struct prr_ctx {
     float last_ms = 0.f;
     float last_trace_ms = 0.f;
     // device scratch, grown on demand and reused across calls
-    DevBuf frames, frame_begin, counters, image, sample_rgb, rays, queue, state, out_u8, out_f, scratch;
+    DevBuf frames, frame_begin, counters, image, sample_rgb, rays, queue, state, out_u8, out_f, scratch, adj_ckpt, adj_dl;
     std::vector<DevBuf *> all_buffers()
     {
-        return {&frames, &frame_begin, &counters, &image, &sample_rgb, &rays, &queue, &state, &out_u8, &out_f, &scratch};
+        return {&frames, &frame_begin, &counters, &image, &sample_rgb, &rays, &queue, &state, &out_u8, &out_f, &scratch,
+                &adj_ckpt, &adj_dl};
     }
 };
 

@@ -393,3 +393,78 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
     if (best) *best = winner;
     return PRR_OK;
 }
+
+// Discrete adjoint of one PHYSICAL frame.  The forward image is rendered in
+// FP64 first (its combined colours feed the SSAA-combine derivative), then
+// k_adjoint pulls dL/d(image) back to the five parameters.
+extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, const float *dL_dimage, int sphere_index,
+                                  double grads[5], prr_stats *stats)
+{
+    if (!ctx) return PRR_ERR_INVALID;
+    if (!frame || !dL_dimage || !grads) { ctx->err = "prr_adjoint: null frame, gradient or output"; return PRR_ERR_INVALID; }
+    const prr_frame_desc &d = *frame;
+    if (d.mode != PRR_MODE_PHYSICAL || d.solver != PRR_SOLVER_RKF45) { ctx->err = "prr_adjoint: PHYSICAL mode RKF45 frames only"; return PRR_ERR_INVALID; }
+    if (d.fxaa) { ctx->err = "prr_adjoint: FXAA is not differentiated; render the frame without FXAA"; return PRR_ERR_UNSUPPORTED; }
+    if (sphere_index < -1 || sphere_index >= d.nspheres) { ctx->err = "prr_adjoint: sphere_index out of range"; return PRR_ERR_INVALID; }
+    // orbit camera: position (r sin i, 0, r cos i), yaw pi, pitch i - pi/2
+    double px = d.cam_pos[0], py = d.cam_pos[1], pz = d.cam_pos[2];
+    double r = std::sqrt(px * px + py * py + pz * pz);
+    if (!(r > 0.0)) { ctx->err = "prr_adjoint: camera at the origin"; return PRR_ERR_INVALID; }
+    double incl = std::acos(pz / r);
+    if (std::fabs(py) > 1e-6 * r || px < 0.0 || std::fabs(d.cam_alpha - M_PI) > 1e-5 || std::fabs(d.cam_beta - (incl - 0.5 * M_PI)) > 1e-5) {
+        ctx->err = "prr_adjoint: needs an orbit camera (position (r sin i, 0, r cos i), yaw pi, pitch i - pi/2)";
+        return PRR_ERR_INVALID;
+    }
+    prr_frame_desc f64 = d;
+    f64.precision = PRR_PREC_FP64;
+    RenderPlan plan;
+    prr_status s = build_plan(ctx, &f64, 1, plan);
+    if (s != PRR_OK) return s;
+    PRR_CK(ctx, cudaSetDevice(ctx->device));
+    const int saved_sched = ctx->schedule;
+    ctx->schedule = PRR_SCHED_PERSISTENT;
+    s = run_plan(ctx, plan, nullptr, nullptr, ctx->stream, true);
+    ctx->schedule = saved_sched;
+    if (s != PRR_OK) return s;
+    const float forward_ms = ctx->last_ms;
+    const FrameParams &fp = plan.fp[0];
+    const long long npx = (long long)fp.width * fp.height, nrays = npx * fp.samples;
+    AdjointParamsHost ap{};
+    ap.spin = fp.a; ap.mass = fp.M; ap.incl = incl; ap.cam_r = r; ap.sphere = sphere_index;
+    if (sphere_index >= 0) {
+        const prr_sphere &S = d.spheres[sphere_index];
+        ap.sph_R = std::hypot((double)S.center[0], (double)S.center[1]);
+        ap.phase = std::atan2((double)S.center[1], (double)S.center[0]);
+        ap.sph_z = S.center[2];
+    }
+    const int threads = ctx->nsm * 2 * 128;
+    const int max_ckpt = d.max_steps / ADJ_CHECKPOINT_INTERVAL + 2;
+    if ((s = alloc(ctx, ctx->adj_ckpt, (size_t)threads * max_ckpt * adjoint_checkpoint_bytes(), "adjoint checkpoints")) != PRR_OK) return s;
+    if ((s = alloc(ctx, ctx->adj_dl, (size_t)npx * 3 * sizeof(float) + 8 * sizeof(double), "adjoint inputs")) != PRR_OK) return s;
+    float *d_dl = (float *)ctx->adj_dl.p;
+    double *d_grad = (double *)((char *)ctx->adj_dl.p + ((size_t)npx * 3 * sizeof(float) + 7) / 8 * 8);
+    cudaStream_t st = ctx->stream;
+    PRR_CK(ctx, cudaMemcpyAsync(d_dl, dL_dimage, (size_t)npx * 3 * sizeof(float), cudaMemcpyHostToDevice, st));
+    PRR_CK(ctx, cudaMemsetAsync(d_grad, 0, 5 * sizeof(double), st));
+    PRR_CK(ctx, cudaMemsetAsync(ctx->counters.p, 0, C_COUNT * sizeof(unsigned long long), st));
+    PRR_CK(ctx, cudaEventRecord(ctx->e0, st));
+    PRR_CK(ctx, launch_adjoint((const FrameParams *)ctx->frames.p, ap, d_dl, (const float *)ctx->image.p, ctx->adj_ckpt.p,
+                               max_ckpt, threads, d_grad, (unsigned long long *)ctx->counters.p, nrays, st));
+    PRR_CK(ctx, cudaEventRecord(ctx->e1, st));
+    PRR_CK(ctx, cudaMemcpyAsync(grads, d_grad, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PRR_CK(ctx, cudaStreamSynchronize(st));
+    float adj_ms = 0.f;
+    PRR_CK(ctx, cudaEventElapsedTime(&adj_ms, ctx->e0, ctx->e1));
+    if (stats) {
+        unsigned long long c[C_COUNT];
+        PRR_CK(ctx, cudaMemcpy(c, ctx->counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+        memset(stats, 0, sizeof(*stats));
+        stats->rays = nrays;
+        stats->accepted = (int64_t)c[C_ACCEPTED];
+        stats->n_math_error = (int64_t)c[C_MATH_ERROR];  // rays whose checkpoints did not fit
+        stats->kernel_ms = adj_ms;
+        stats->trace_ms = forward_ms;
+        stats->kernel_launches = ctx->last_launches + 1;
+    }
+    return PRR_OK;
+}

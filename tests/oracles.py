@@ -57,6 +57,10 @@ class Oracle:
         lib.prr_oracle_geod.restype = None
         lib.prr_oracle_geod.argtypes = [C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double),
                                         C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]
+        lib.prr_oracle_grad.restype = C.c_int
+        lib.prr_oracle_grad.argtypes = [C.POINTER(abi.FrameDesc), _u8pp, _ip, _ip, C.POINTER(C.c_float), C.c_int,
+                                        C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         lib.prr_oracle_metric.restype = None
         lib.prr_oracle_metric.argtypes = [C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         self.lib = lib
@@ -93,6 +97,26 @@ class Oracle:
         state, rgb = self.trace(d, textures, precision)
         img = self.post(rgb, d.width, d.height, d.samples, bool(d.fxaa))
         return state, rgb, img
+
+    def grad(self, d: abi.FrameDesc, textures, dL_dimage: np.ndarray, sphere_index: int = 0, params=None,
+             nthreads: int | None = None):
+        """FP64 forward-mode gradient (spin, mass, inclination, camera r,
+        sphere phase) of sum(dL_dimage * image); returns (grads, image)."""
+        tt = TexTable(textures)
+        g = np.zeros(5, dtype=np.float64)
+        img = np.zeros((d.height, d.width, 3), dtype=np.float64)
+        dl = np.ascontiguousarray(dL_dimage, dtype=np.float32)
+        pp = (C.c_double * 5)(*params) if params is not None else None
+        loss = C.c_double()
+        sig = np.zeros((d.height, d.width), dtype=np.int64)
+        rc = self.lib.prr_oracle_grad(C.byref(d), tt.ptrs, tt.w, tt.h, dl.ctypes.data_as(C.POINTER(C.c_float)),
+                                      sphere_index, nthreads or os.cpu_count(), g.ctypes.data_as(C.POINTER(C.c_double)),
+                                      img.ctypes.data_as(C.POINTER(C.c_double)), pp, C.byref(loss),
+                                      sig.ctypes.data_as(C.POINTER(C.c_longlong)))
+        if rc:
+            raise ValueError("oracle rejected the frame for gradients")
+        self.last_loss, self.last_sig = loss.value, sig
+        return g, img
 
     def geod(self, metric: int, M: float, a: float, p, u, refmode: bool = False) -> np.ndarray:
         pa = (C.c_double * 4)(*p)
