@@ -210,6 +210,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -325,6 +326,23 @@ def main():
                                       "Christoffel-table geodesic",
                               "breakdown_ms": {"plain_table": plain_ms, "plain_contraction": plain_contraction_ms,
                                                "persistent_table": table_ms, "persistent_contraction": ms}}
+        if not args.no_adjoint:
+            # discrete adjoint of the 512x512 differentiable-render workload: one gradient of an L2 image loss
+            import ctypes as C
+
+            _, tgt, _ = ctx.render(scenes.kerr_512_adjoint(spin=0.7, precision=abi.PREC_FP64), want_float=True)
+            start = scenes.kerr_512_adjoint(spin=0.3, incl_deg=45.0, precision=abi.PREC_FP64)
+            _, cur, _ = ctx.render(start, want_float=True)
+            dl = np.ascontiguousarray(2.0 * (cur[0] - tgt[0]), dtype=np.float32)
+            g = np.zeros(5, dtype=np.float64)
+            ast = abi.Stats()
+            for _ in range(2):  # the first call sizes the checkpoint buffer
+                abi.check(abi.load().prr_adjoint(ctx.h, C.byref(start), dl.ctypes.data_as(abi._fp), 0,
+                                                 g.ctypes.data_as(abi._dp), C.byref(ast)), ctx.h)
+            extra["adjoint"] = {"ms": ast.kernel_ms, "fp64_forward_ms": ast.trace_ms, "unit": "ms",
+                                "workload": "kerr a=0.3 i=45 r=20, 512x512, 1 sphere, bilinear sky, FP64, tol 1e-6; "
+                                            "d(L2 to the a=0.7 render)/d(a, M, i, r, phase)",
+                                "grad": g.tolist(), "accepted_steps": ast.accepted}
         if not args.no_accuracy:
             f64 = build_frames(rank, ws, args.width, args.height)
             f64.precision = abi.PREC_FP64

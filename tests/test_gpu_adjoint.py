@@ -48,12 +48,28 @@ def test_adjoint_matches_central_differences(gpu, oracle, small_textures):
         assert abs(g[k] - fd) <= 1e-3 * abs(fd) + 1e-9, (NAMES[k], g[k], fd)
 
 
+def smooth_sky(w=64, h=32):
+    """A low-frequency sky: with it the image is a smooth function of the
+    camera, so the inverse problem is well posed (a point-star sky makes the
+    L2 image loss nearly random in the inclination)."""
+    x = np.arange(w)[None, :]
+    y = np.arange(h)[:, None]
+    t = np.zeros((h, w, 4), np.uint8)
+    t[..., 0] = (128 + 90 * np.sin(2 * np.pi * x / w) * np.ones_like(y)).astype(np.uint8)
+    t[..., 1] = (128 + 90 * np.cos(np.pi * y / h) * np.ones_like(x)).astype(np.uint8)
+    t[..., 2] = (128 + 60 * np.sin(4 * np.pi * x / w + 2 * np.pi * y / h)).astype(np.uint8)
+    t[..., 3] = 255
+    return t
+
+
 def test_torch_wrapper_and_adam_fit(gpu, small_textures):
     import torch
 
     from torch_render import render
 
-    gpu.upload_textures(small_textures)
+    tex = dict(small_textures)
+    tex[scenes.SKY_ID] = smooth_sky()
+    gpu.upload_textures(tex)
     W = H = 48
     target_p = torch.tensor([0.7, 1.0, math.radians(60.0), 20.0, math.radians(30.0)], dtype=torch.float64)
     with torch.no_grad():
@@ -68,11 +84,11 @@ def test_torch_wrapper_and_adam_fit(gpu, small_textures):
     _, img, _ = gpu.render(d, want_float=True)
     g, _ = gpu_adjoint(gpu, d, 2.0 * (img[0] - target.numpy()))
     assert np.allclose(p.grad.numpy(), g, rtol=1e-6, atol=1e-9)
-    # Adam on (spin, inclination) towards the target
+    # Adam on (spin, inclination) from (0.3, 45 deg) towards (0.7, 60 deg)
     q = torch.tensor([0.3, math.radians(45.0)], dtype=torch.float64, requires_grad=True)
     opt = torch.optim.Adam([q], lr=0.02)
-    first = None
-    for it in range(40):
+    losses = []
+    for it in range(60):
         opt.zero_grad()
         full = torch.cat([q[:1], torch.tensor([1.0], dtype=torch.float64), q[1:],
                           torch.tensor([20.0, math.radians(30.0)], dtype=torch.float64)])
@@ -81,6 +97,7 @@ def test_torch_wrapper_and_adam_fit(gpu, small_textures):
         opt.step()
         with torch.no_grad():
             q[0].clamp_(0.0, 0.99)
-        first = first if first is not None else loss.item()
-    assert loss.item() < 0.5 * first, (first, loss.item())
-    assert abs(q[1].item() - math.radians(60.0)) < abs(math.radians(45.0) - math.radians(60.0))
+        losses.append(loss.item())
+    assert losses[-1] < 0.6 * losses[0], losses[::10]
+    assert abs(q[1].item() - math.radians(60.0)) < 0.5 * math.radians(15.0), math.degrees(q[1].item())
+    assert q[0].item() > 0.35
