@@ -163,6 +163,138 @@ def cpu_reference_sample(frame, textures, budget_s: float, nthreads: int):
             "infinite_geo_fraction": float(np.mean(results == abi.RESULT_INFINITE_GEO)) if len(results) else None}
 
 
+def bench_trajectory(ctx, torch, stream, plain_stride: int = 10):
+    """The 240-frame trajectory workload: Kerr a = 0.9, 960x540, no SSAA,
+    orbit radius 20M -> 8M, inclination 60 -> 88 deg, tolerance 1e-6, FP32.
+    (1) autotuned launch shape, whole trajectory recorded into one CUDA graph
+    and replayed (one persistent launch); (2) the same frames as 240
+    persistent launches, one per frame; (3) the plain one-ray-per-thread
+    schedule per frame on every `plain_stride`-th frame, scaled to 240."""
+    from parrelray_b200 import Graph, abi, scenes
+
+    frames = scenes.trajectory_240()
+    npx = sum(f.width * f.height for f in frames)
+    rays = sum(f.nrays for f in frames)
+    out8 = torch.empty(npx * 3, dtype=torch.uint8, device="cuda")
+    saved = ctx.launch_config()
+    t0 = time.perf_counter()
+    tuned = ctx.autotune(frames[len(frames) // 2])
+    tune_s = time.perf_counter() - t0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = {"workload": "trajectory_240: Kerr a=0.9, 240 frames 960x540, r 20M->8M, i 60->88 deg, tol 1e-6, FP32",
+           "rays": rays, "autotune_s": tune_s,
+           "tuned": {"block_size": tuned.block_size, "blocks_per_sm": tuned.blocks_per_sm,
+                     "compaction_interval": tuned.compaction_interval, "rays_per_thread": tuned.rays_per_thread}}
+    with Graph(ctx, frames, out8.data_ptr()) as g:
+        g.launch(stream.cuda_stream)  # warm-up replay
+        st = g.stats()
+        ev0.record(stream)
+        g.launch(stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        graph_ms = ev0.elapsed_time(ev1)
+    res["graph"] = {"ms": graph_ms, "mrays_s": rays / (graph_ms * 1e-3) / 1e6, "launches": int(st.kernel_launches),
+                    "attempts": int(st.attempts)}
+    # one persistent launch per frame (same tuned shape), no graph
+    ev0.record(stream)
+    for f in frames:
+        ctx.render_device(f, out8.data_ptr(), stream=stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    pf_ms = ev0.elapsed_time(ev1)
+    res["per_frame_persistent"] = {"ms": pf_ms, "mrays_s": rays / (pf_ms * 1e-3) / 1e6, "launches": len(frames)}
+    ctx.set_schedule(abi.SCHED_PERSISTENT, saved)
+    # plain schedule, one render call per frame, sampled
+    ctx.set_schedule(abi.SCHED_PLAIN)
+    sample = frames[::plain_stride]
+    ctx.render_device(sample[0], out8.data_ptr(), stream=stream.cuda_stream)  # warm-up
+    ev0.record(stream)
+    for f in sample:
+        ctx.render_device(f, out8.data_ptr(), stream=stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ctx.set_schedule(abi.SCHED_PERSISTENT, saved)
+    plain_sample_ms = ev0.elapsed_time(ev1)
+    sample_rays = sum(f.nrays for f in sample)
+    plain_rate = sample_rays / (plain_sample_ms * 1e-3) / 1e6
+    res["plain_per_frame"] = {"mrays_s": plain_rate, "ms_240_estimated": rays / (plain_rate * 1e6) * 1e3,
+                              "sampled_frames": len(sample), "sampled_ms": plain_sample_ms,
+                              "what": f"every {plain_stride}th frame rendered with the plain schedule, one call per "
+                                      f"frame; time scaled to the 240 frames by rays"}
+    res["speedup_vs_plain"] = res["graph"]["mrays_s"] / plain_rate
+    res["speedup_vs_per_frame_persistent"] = pf_ms / graph_ms
+    return res
+
+
+def bench_uneven(ctx, torch, stream, textures, oracle_rays_per_request: int = 64, oracle_seconds: float = 10.0):
+    """The 64-request workload (log-uniform 256x256..2048x1024, a ~ U[0, 0.998],
+    r ~ U[8M, 40M], i ~ U[10, 89] deg, tolerance 1e-7) in one batched render
+    per precision: SPLIT (FP32 bulk, FP64 re-integration near the critical
+    impact parameter or the horizon), all-FP64 and plain FP32.  Per request:
+    fraction of pixels within 1/255 of the all-FP64 GPU render, and the
+    per-sample colour error of the SPLIT render against the FP64 host oracle
+    on a seeded sample of rays (no SSAA, so a sample is a pixel)."""
+    from parrelray_b200 import abi, scenes
+
+    res = {"workload": "uneven_64: 64 requests, log-uniform 256^2..2048x1024, a~U[0,0.998], r~U[8,40]M, "
+                       "i~U[10,89] deg, tol 1e-7"}
+    imgs, stats, ms = {}, {}, {}
+    for name, p in (("split", abi.PREC_SPLIT), ("fp64", abi.PREC_FP64), ("fp32", abi.PREC_FP32)):
+        fr = scenes.uneven_64(precision=p)
+        im, _, st = ctx.render(fr)
+        imgs[name], stats[name], ms[name] = im, st, st.trace_ms
+    rays = int(stats["split"].rays)
+    res["rays"] = rays
+    for name in ms:
+        res[name] = {"ms": ms[name], "mrays_s": rays / (ms[name] * 1e-3) / 1e6,
+                     "render_call_ms": stats[name].kernel_ms, "attempts": int(stats[name].attempts)}
+    res["timing"] = "ms = tracing kernels (persistent pass, plus the FP64 pass for SPLIT), CUDA events; " \
+                    "render_call_ms adds combine/quantise and the first-call buffer growth"
+    res["split"]["fp64_rays"] = int(stats["split"].n_fp64)
+    res["speedup_split_vs_fp64"] = ms["fp64"] / ms["split"]
+    per = []
+    for a, b in zip(imgs["split"], imgs["fp64"]):
+        d = np.abs(a.astype(np.int32) - b.astype(np.int32)).max(axis=-1)
+        per.append(float(np.mean(d <= 1)))
+    per32 = []
+    for a, b in zip(imgs["fp32"], imgs["fp64"]):
+        d = np.abs(a.astype(np.int32) - b.astype(np.int32)).max(axis=-1)
+        per32.append(float(np.mean(d <= 1)))
+    tot = sum(a.shape[0] * a.shape[1] for a in imgs["fp64"])
+    res["vs_fp64_gpu"] = {"min_request_fraction_within_1_255": min(per),
+                          "all_pixels_fraction_within_1_255": sum(p * a.shape[0] * a.shape[1]
+                                                                  for p, a in zip(per, imgs["fp64"])) / tot,
+                          "per_request": [round(p, 6) for p in per],
+                          "fp32_min_request_fraction": min(per32),
+                          "fp32_all_pixels_fraction": sum(p * a.shape[0] * a.shape[1]
+                                                          for p, a in zip(per32, imgs["fp64"])) / tot}
+    # FP64 host oracle on a bounded seeded sample of rays of every request
+    try:
+        sys.path.insert(0, str(REPO / "tests"))
+        from oracles import Oracle
+
+        orc = Oracle()
+    except (ImportError, FileNotFoundError):
+        return res
+    fr64 = scenes.uneven_64(precision=abi.PREC_FP64)
+    rng = np.random.default_rng(11)
+    errs, n_done, t0 = [], 0, time.perf_counter()
+    for k, f in enumerate(fr64):
+        if time.perf_counter() - t0 > oracle_seconds:
+            break
+        ids = rng.choice(f.nrays, size=min(oracle_rays_per_request, f.nrays), replace=False)
+        _, rgb = orc.trace(f, textures, precision=1, ids=ids)
+        img = imgs["split"][k].reshape(-1, 3).astype(np.int32)
+        q = np.floor(np.float32(255.0) * np.clip(rgb, 0, 1).astype(np.float32) + 0.5).astype(np.int32)
+        errs.append(np.abs(img[ids] - q).max(axis=-1))
+        n_done += 1
+    e = np.concatenate(errs) if errs else np.zeros(0)
+    res["vs_fp64_host_oracle"] = {"requests": n_done, "rays": int(e.size),
+                                  "fraction_within_1_255": float(np.mean(e <= 1)) if e.size else None,
+                                  "max_diff_255": int(e.max()) if e.size else None}
+    return res
+
+
 def run_reference_arm(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -211,6 +343,8 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-trajectory", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -343,6 +477,10 @@ def main():
                                 "workload": "kerr a=0.3 i=45 r=20, 512x512, 1 sphere, bilinear sky, FP64, tol 1e-6; "
                                             "d(L2 to the a=0.7 render)/d(a, M, i, r, phase)",
                                 "grad": g.tolist(), "accepted_steps": ast.accepted}
+        if not args.no_trajectory and ws == 1:
+            extra["trajectory"] = bench_trajectory(ctx, torch, stream)
+        if not args.no_uneven and ws == 1:
+            extra["uneven"] = bench_uneven(ctx, torch, stream, tex)
         if not args.no_accuracy:
             f64 = build_frames(rank, ws, args.width, args.height)
             f64.precision = abi.PREC_FP64

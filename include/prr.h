@@ -246,6 +246,38 @@ prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, const uint8_t
                               const int32_t *tex_w, const int32_t *tex_h, uint8_t *d_rgb8, float *d_rgbf,
                               void *stream, char *errbuf, size_t errlen);
 
+/* ---- recorded batches (new; replaces the per-frame host loop of
+ *      prr.cpp:382-386, each iteration of which runs renderframe,
+ *      prr.cpp:237-341, as a dozen synchronised launches) ----
+ * prr_graph_create records the render of n PHYSICAL-mode frames (a camera
+ * trajectory, a set of uneven requests) into a CUDA graph: a counter reset,
+ * ONE persistent launch over all frames (frames fill each other's tails),
+ * the FP64 pass of SPLIT precision, and the per-frame combine/FXAA passes
+ * the frames need.  Outputs are device buffers, frames concatenated as in
+ * prr_render; at least one must be non-NULL.  The graph owns its device
+ * scratch and keeps the context's launch configuration of creation time
+ * (call prr_autotune first for a tuned shape).  It embeds the device
+ * addresses of the uploaded textures: do not re-upload a texture the frames
+ * use while the graph lives (or call prr_graph_set_frames afterwards).  The
+ * graph must be destroyed before its context.
+ * prr_graph_launch replays it asynchronously on `stream` (NULL = legacy
+ * default stream); replays on one graph must not overlap in time.
+ * prr_graph_set_frames replaces the frame parameters (same count, and per
+ * frame the same width, height, samples, FXAA flag, mode and precision),
+ * e.g. the next trajectory segment, without re-recording.
+ * prr_graph_stats waits for the last replay and returns its counters
+ * (kernel_ms is 0: time replays with events on your stream); it returns
+ * PRR_ERR_TIMEOUT when the context's watchdog fired during that replay. */
+typedef struct prr_graph prr_graph;
+prr_status prr_graph_create(prr_ctx *ctx, const prr_frame_desc *frames, int n, uint8_t *d_rgb8, float *d_rgbf,
+                            prr_graph **out);
+prr_status prr_graph_set_frames(prr_graph *g, const prr_frame_desc *frames, int n);
+prr_status prr_graph_launch(prr_graph *g, void *stream);
+prr_status prr_graph_stats(prr_graph *g, prr_stats *stats);
+/* The launch shape recorded in the graph (blocks_per_sm resolved). */
+prr_status prr_graph_get_launch_config(const prr_graph *g, prr_launch_config *cfg);
+void prr_graph_destroy(prr_graph *g);
+
 /* ---- scheduler tuning (new) ---- */
 prr_status prr_set_schedule(prr_ctx *ctx, int schedule, const prr_launch_config *cfg);
 prr_status prr_get_launch_config(prr_ctx *ctx, prr_launch_config *cfg);

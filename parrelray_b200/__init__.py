@@ -14,7 +14,7 @@ import numpy as np
 from . import abi
 from .abi import FrameDesc, LaunchConfig, PrrError, Stats
 
-__all__ = ["Context", "FrameDesc", "LaunchConfig", "PrrError", "Stats", "abi"]
+__all__ = ["Context", "FrameDesc", "Graph", "LaunchConfig", "PrrError", "Stats", "abi"]
 
 
 def _frames_array(frames) -> tuple[C.Array, list[FrameDesc]]:
@@ -135,3 +135,46 @@ class Context:
         self._check(self.lib.prr_trace_rays_f64(self.h, C.byref(frame), state.ctypes.data_as(abi._dp),
                                                 rgb.ctypes.data_as(abi._dp), C.byref(stats)))
         return state, rgb, stats
+
+
+class Graph:
+    """A batch of frames recorded into a CUDA graph (prr_graph_*): device
+    outputs given as raw pointers; replay with launch(stream)."""
+
+    def __init__(self, ctx: Context, frames, d_rgb8: int | None, d_rgbf: int | None = None):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        arr, fl = _frames_array(frames)
+        self.nframes = len(fl)
+        h = C.c_void_p()
+        ctx._check(self.lib.prr_graph_create(ctx.h, arr, len(fl), C.c_void_p(d_rgb8) if d_rgb8 else None,
+                                             C.c_void_p(d_rgbf) if d_rgbf else None, C.byref(h)))
+        self.h = h
+
+    def set_frames(self, frames) -> None:
+        arr, fl = _frames_array(frames)
+        self.ctx._check(self.lib.prr_graph_set_frames(self.h, arr, len(fl)))
+
+    def launch(self, stream: int | None = None) -> None:
+        self.ctx._check(self.lib.prr_graph_launch(self.h, C.c_void_p(stream) if stream else None))
+
+    def stats(self) -> Stats:
+        st = Stats()
+        self.ctx._check(self.lib.prr_graph_stats(self.h, C.byref(st)))
+        return st
+
+    def launch_config(self) -> LaunchConfig:
+        cfg = LaunchConfig()
+        self.ctx._check(self.lib.prr_graph_get_launch_config(self.h, C.byref(cfg)))
+        return cfg
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.prr_graph_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

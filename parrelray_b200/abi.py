@@ -98,6 +98,12 @@ SIGNATURES = {
     "prr_frame_desc_defaults": (None, [C.POINTER(FrameDesc)]),
     "prr_sizeof": (C.c_size_t, [C.c_int]),
     "prr_adjoint": (C.c_int, [_P, C.POINTER(FrameDesc), _fp, C.c_int, _dp, C.POINTER(Stats)]),
+    "prr_graph_create": (C.c_int, [_P, C.POINTER(FrameDesc), C.c_int, _P, _P, C.POINTER(_P)]),
+    "prr_graph_set_frames": (C.c_int, [_P, C.POINTER(FrameDesc), C.c_int]),
+    "prr_graph_launch": (C.c_int, [_P, _P]),
+    "prr_graph_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+    "prr_graph_get_launch_config": (C.c_int, [_P, C.POINTER(LaunchConfig)]),
+    "prr_graph_destroy": (None, [_P]),
     "prr_render_noalloc": (C.c_int, [C.POINTER(FrameDesc), C.c_int, C.POINTER(_P), C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), _P, _P, _P, C.c_char_p, C.c_size_t]),
 }
@@ -132,7 +138,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
 def header_functions(header: Path = HEADER) -> list[str]:
     """Names of the functions include/prr.h declares."""
     text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
-    return sorted(set(re.findall(r"\b(prr_[a-z0-9_]+)\s*\(", text)) - {"prr_ctx"})
+    return sorted(set(re.findall(r"\b(prr_[a-z0-9_]+)\s*\(", text)) - {"prr_ctx", "prr_graph"})
 
 
 def check(status: int, ctx=None) -> None:

@@ -65,3 +65,6 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
 // Single frame: per-ray states and per-sample colours to host buffers.
 prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, double *h_state64, float *h_rgb);
 prr_status collect_stats(prr_ctx *ctx, const RenderPlan &plan, prr_stats *stats);
+// Resident CTAs per SM of the persistent kernel under the context's launch
+// configuration (its blocks_per_sm, or the occupancy limit when that is 0).
+int resolve_bpsm(prr_ctx *ctx, int precision);

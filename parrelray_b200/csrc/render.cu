@@ -51,14 +51,14 @@ prr_status alloc(prr_ctx *ctx, DevBuf &b, size_t bytes, const char *what)
     return PRR_OK;
 }
 
+}  // namespace
+
 int resolve_bpsm(prr_ctx *ctx, int precision)
 {
     if (ctx->cfg.blocks_per_sm > 0) return ctx->cfg.blocks_per_sm;
     int b = persistent_occupancy(precision, ctx->geod_table == 1, ctx->cfg.block_size);
     return b > 0 ? b : 1;
 }
-
-}  // namespace
 
 prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderPlan &plan)
 {
@@ -89,7 +89,8 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
         if (!std::isfinite(d.cam_alpha) || !std::isfinite(d.cam_beta)) return bad(ctx, f, "camera angles are not finite");
         if (d.metric < PRR_METRIC_FLAT || d.metric > PRR_METRIC_KERR) return bad(ctx, f, "unknown metric");
         if (!std::isfinite(d.mass) || d.mass < 0.0f) return bad(ctx, f, "mass must be >= 0");
-        if (d.metric != PRR_METRIC_FLAT && d.mass <= 0.0f) return bad(ctx, f, "Schwarzschild/Kerr need mass > 0");
+        // M = 0 is allowed for Schwarzschild: the reference renders its example deck (input/sim.params:30,52) so
+        if (d.metric == PRR_METRIC_KERR && d.mass <= 0.0f) return bad(ctx, f, "Kerr needs mass > 0");
         if (d.metric == PRR_METRIC_KERR && !(std::fabs(d.spin) <= d.mass)) return bad(ctx, f, "Kerr needs |spin| <= mass");
         if (d.solver != PRR_SOLVER_EULER && d.solver != PRR_SOLVER_RKF45) return bad(ctx, f, "solver must be euler (0) or rkf45 (2)");
         if (d.mode != PRR_MODE_REFERENCE && d.mode != PRR_MODE_PHYSICAL) return bad(ctx, f, "unknown mode");
