@@ -296,6 +296,78 @@ prr_status prr_set_option(prr_ctx *ctx, int option, long long value);
  * with a dependent-chain FMA kernel; either pointer may be NULL. */
 prr_status prr_measure_peak(prr_ctx *ctx, double *fp32_tflops, double *fp64_tflops);
 
+/* ---- input decks (replaces main/io.h:21-58 readParams, the getters of
+ *      main/Parameters.cpp:20-44, checkFrame prr.cpp:139-153, createScene
+ *      prr.cpp:159-198, Spacetime::setupScene/updateScene
+ *      main/Spacetime.cpp:17-44 and renderframe's set-up prr.cpp:245-253).
+ *      No GPU needed. ----
+ * Decks are read with the reference's rules, quirks included: a line with
+ * neither '_' nor '<' is skipped; ANY line containing '_' opens a block named
+ * by the text between its first and last '_'; otherwise the key is the text
+ * between the first '<' and '>' left of '=', the value the same right of it.
+ * prr_deck_load also reads the decks named by tracer.traj and tracer.scene
+ * (paths relative to the working directory; an unreadable one adds nothing,
+ * as in the reference).  errbuf (errlen bytes) receives a message on failure
+ * and may be NULL. */
+typedef struct prr_deck prr_deck;
+prr_status prr_deck_load(const char *path, prr_deck **out, char *errbuf, size_t errlen);
+/* Same rules over an in-memory deck (no traj/scene files are followed). */
+prr_status prr_deck_parse_string(const char *text, prr_deck **out);
+void prr_deck_free(prr_deck *d);
+/* headerExists / parExists (main/Parameters.cpp:10-18): 1 or 0. */
+int prr_deck_has_block(const prr_deck *d, const char *block);
+int prr_deck_has(const prr_deck *d, const char *block, const char *key);
+/* par (main/Parameters.cpp:20-25): copies the value ("" when missing) into
+ * buf (len bytes, NUL-terminated, may be NULL) and returns its length. */
+size_t prr_deck_get(const prr_deck *d, const char *block, const char *key, char *buf, size_t len);
+/* pari / parf (main/Parameters.cpp:26-44): std::stoi / std::stof of the
+ * value; 0 (pari) or `dflt` (parf) when the key is missing or unparsable. */
+int prr_deck_geti(const prr_deck *d, const char *block, const char *key);
+float prr_deck_getf(const prr_deck *d, const char *block, const char *key, float dflt);
+/* checkFrame (prr.cpp:139-153): the first i without all of frame<i>.x y z a b. */
+int prr_deck_frame_count(const prr_deck *d);
+/* Spheres in the scene: the first i without a sphere<i> block. */
+int prr_deck_sphere_count(const prr_deck *d);
+/* sphere<i>.tex into buf as prr_deck_get; returns its length. */
+size_t prr_deck_sphere_texture(const prr_deck *d, int sphere, char *buf, size_t len);
+/* The descriptor of frame `frame`: camera, spacetime and tracer from their
+ * blocks; sphere<i> centres and radii after updateScene(0..frame), a key the
+ * deck lacks keeping the previous frame's value; frame<i>.mass overriding
+ * the mass from that frame on.  Angles in degrees are converted as the
+ * reference does (float(deg * M_PI / 180.0f)).  Texture ids: 0 = the sky
+ * (tracer.bimage1), 1, 2, ... = distinct sphere textures in sphere order,
+ * -1 = none.  Deck keys the reference lacks, all optional with defaults that
+ * reproduce it: spacetime.metric (flat|schwarzschild|kerr; schwarzschild, as
+ * main/metric.h:12 selects; no black hole = flat), tracer.mode
+ * (reference|physical), tracer.precision (fp32|fp64|split), tracer.rtol and
+ * tracer.atol (eps), tracer.maxsteps (10000), tracer.horizon (0.001, as
+ * metrics/schwarzschild.cuh:70), tracer.fxaa (0), tracer.bgfilter
+ * (rms2x2|bilinear).  Solvers rk/adams/gragg/dormand/taylor and SSAA
+ * random/poisson/jittered/rotated have no implementation in the reference's
+ * frame loop and return PRR_ERR_UNSUPPORTED; unknown names fall back to
+ * euler and regular as Parameters::getSolver/getSSAA do. */
+prr_status prr_deck_frame(const prr_deck *d, int frame, prr_frame_desc *out, char *errbuf, size_t errlen);
+
+/* The reference's main (prr.cpp:345-404): loads the deck at `path`, uploads
+ * the textures it names (prr_image_load), renders frames [first,
+ * first+count) (count < 0: to the last) in batches of `batch` frames per
+ * prr_render call (< 1: 16), and writes each as <prefix>image_<i>.png, the
+ * reference's name (prr.cpp:336); prefix NULL = tracer.out.  Texture ids 0 ..
+ * are (re)uploaded on the context.  stats (may be NULL) sums the calls. */
+prr_status prr_run_deck(prr_ctx *ctx, const char *path, int first, int count, const char *prefix, int batch,
+                        prr_stats *stats);
+
+/* ---- image files (replaces cudamaths/image.cu:13-39) ----
+ * prr_image_load decodes PNG (1/2/4/8/16-bit grey, grey+alpha, RGB, RGBA,
+ * palette; interlaced or not) and binary PNM (P6, P5; maxval <= 255) to
+ * RGBA8 (*rgba8 from malloc; free with prr_image_free), with stb_image's
+ * channel rules: grey replicated to RGB, 16-bit samples keep their high
+ * byte, low-bit grey scaled to 0..255.  JPEG returns PRR_ERR_UNSUPPORTED.
+ * prr_png_write writes 8-bit RGB rows (3*w bytes each) as a PNG file. */
+prr_status prr_image_load(const char *path, uint8_t **rgba8, int *w, int *h, char *errbuf, size_t errlen);
+void prr_image_free(uint8_t *rgba8);
+prr_status prr_png_write(const char *path, const uint8_t *rgb8, int w, int h);
+
 /* ---- host helpers (no GPU needed) ---- */
 /* Seeded procedural RGBA8 textures.  kind 0: sphere texture (checkerboard +
  * value noise); kind 1: equirectangular starfield (Poisson point stars with

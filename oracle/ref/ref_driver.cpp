@@ -258,4 +258,56 @@ int prr_ref_save_png(const char *path, const float *image, int w, int h)
     return Images::get().savePNGToFile(path, (f3 *)image, i2(w, h)) ? 0 : 1;
 }
 
+// ---- the reference's deck parser and getters, for parity tests of the
+//      product's deck reader (main/io.h:21-58, main/Parameters.cpp:10-44,
+//      prr.cpp:139-153) ----
+
+// readParams of one file into an emptied table (no traj/scene, no scene).
+int prr_ref_parse(const char *path)
+{
+    Parameters::get().parameters.clear();
+    readParams(path, &Parameters::get().parameters);
+    return 0;
+}
+
+int prr_ref_has_block(const char *block) { return headerExists(block) ? 1 : 0; }
+int prr_ref_has(const char *block, const char *key) { return parExists(block, key) ? 1 : 0; }
+
+size_t prr_ref_par(const char *block, const char *key, char *buf, size_t len)
+{
+    std::string v = par(block, key);
+    if (buf && len) {
+        size_t n = v.size() < len - 1 ? v.size() : len - 1;
+        memcpy(buf, v.data(), n);
+        buf[n] = 0;
+    }
+    return v.size();
+}
+
+int prr_ref_pari(const char *block, const char *key) { return pari(block, key); }
+float prr_ref_parf(const char *block, const char *key) { return parf(block, key); }
+float prr_ref_parf_d(const char *block, const char *key, float dflt) { return parf(block, key, dflt); }
+int prr_ref_check_frame(void) { return checkFrame(); }
+
+// Number of (block, key) entries and the i-th of them in map order.
+int prr_ref_entry_count(void)
+{
+    int n = 0;
+    for (auto &b : Parameters::get().parameters) n += (int)b.second.size();
+    return n;
+}
+
+int prr_ref_entry(int i, char *block, char *key, char *val, size_t len)
+{
+    for (auto &b : Parameters::get().parameters)
+        for (auto &kv : b.second) {
+            if (i-- != 0) continue;
+            snprintf(block, len, "%s", b.first.c_str());
+            snprintf(key, len, "%s", kv.first.c_str());
+            snprintf(val, len, "%s", kv.second.c_str());
+            return 0;
+        }
+    return 1;
+}
+
 }  // extern "C"

@@ -14,7 +14,8 @@ import numpy as np
 from . import abi
 from .abi import FrameDesc, LaunchConfig, PrrError, Stats
 
-__all__ = ["Context", "FrameDesc", "Graph", "LaunchConfig", "PrrError", "Stats", "abi"]
+__all__ = ["Context", "Deck", "FrameDesc", "Graph", "LaunchConfig", "PrrError", "Stats", "abi", "load_image",
+           "write_png"]
 
 
 def _frames_array(frames) -> tuple[C.Array, list[FrameDesc]]:
@@ -117,6 +118,13 @@ class Context:
                                                C.c_void_p(d_rgbf) if d_rgbf else None,
                                                C.c_void_p(stream) if stream else None))
 
+    def run_deck(self, path, first: int = 0, count: int = -1, prefix: str | None = None, batch: int = 16) -> Stats:
+        """prr_run_deck: renders a deck's frames to <prefix>image_<i>.png."""
+        st = Stats()
+        self._check(self.lib.prr_run_deck(self.h, str(path).encode(), first, count,
+                                          prefix.encode() if prefix is not None else None, batch, C.byref(st)))
+        return st
+
     def trace_rays(self, frame: FrameDesc):
         """Per-ray final states (n, 12) float32 and per-sample colours (n, 3)."""
         n = frame.nrays
@@ -178,3 +186,88 @@ class Graph:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class Deck:
+    """A reference-format deck (prr_deck_*): getters with the reference's
+    semantics and the frame descriptors it defines."""
+
+    def __init__(self, path=None, text: str | None = None):
+        self.lib = abi.load()
+        h = C.c_void_p()
+        if text is not None:
+            st = self.lib.prr_deck_parse_string(text.encode(), C.byref(h))
+            if st != abi.OK:
+                raise PrrError(st, "deck text could not be parsed")
+        else:
+            err = C.create_string_buffer(512)
+            st = self.lib.prr_deck_load(str(path).encode(), C.byref(h), err, 512)
+            if st != abi.OK:
+                raise PrrError(st, err.value.decode())
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.prr_deck_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def has_block(self, block: str) -> bool:
+        return bool(self.lib.prr_deck_has_block(self.h, block.encode()))
+
+    def has(self, block: str, key: str) -> bool:
+        return bool(self.lib.prr_deck_has(self.h, block.encode(), key.encode()))
+
+    def get(self, block: str, key: str) -> str:
+        n = self.lib.prr_deck_get(self.h, block.encode(), key.encode(), None, 0)
+        buf = C.create_string_buffer(n + 1)
+        self.lib.prr_deck_get(self.h, block.encode(), key.encode(), buf, n + 1)
+        return buf.raw[:n].decode("utf-8", "surrogateescape")
+
+    def geti(self, block: str, key: str) -> int:
+        return self.lib.prr_deck_geti(self.h, block.encode(), key.encode())
+
+    def getf(self, block: str, key: str, default: float = 0.0) -> float:
+        return self.lib.prr_deck_getf(self.h, block.encode(), key.encode(), default)
+
+    @property
+    def frame_count(self) -> int:
+        return self.lib.prr_deck_frame_count(self.h)
+
+    @property
+    def sphere_count(self) -> int:
+        return self.lib.prr_deck_sphere_count(self.h)
+
+    def frame(self, i: int) -> FrameDesc:
+        d = FrameDesc()
+        err = C.create_string_buffer(512)
+        st = self.lib.prr_deck_frame(self.h, i, C.byref(d), err, 512)
+        if st != abi.OK:
+            raise PrrError(st, err.value.decode())
+        return d
+
+
+def load_image(path) -> np.ndarray:
+    """prr_image_load: (h, w, 4) uint8 RGBA."""
+    lib = abi.load()
+    p, w, h = abi._u8p(), C.c_int(), C.c_int()
+    err = C.create_string_buffer(512)
+    st = lib.prr_image_load(str(path).encode(), C.byref(p), C.byref(w), C.byref(h), err, 512)
+    if st != abi.OK:
+        raise PrrError(st, err.value.decode())
+    try:
+        return np.ctypeslib.as_array(p, shape=(h.value, w.value, 4)).copy()
+    finally:
+        lib.prr_image_free(p)
+
+
+def write_png(path, rgb8: np.ndarray) -> None:
+    a = np.ascontiguousarray(rgb8, dtype=np.uint8)
+    if a.ndim != 3 or a.shape[2] != 3:
+        raise ValueError("need an (h, w, 3) uint8 array")
+    abi.check(abi.load().prr_png_write(str(path).encode(), a.ctypes.data_as(abi._u8p), a.shape[1], a.shape[0]))

@@ -104,6 +104,23 @@ SIGNATURES = {
     "prr_graph_stats": (C.c_int, [_P, C.POINTER(Stats)]),
     "prr_graph_get_launch_config": (C.c_int, [_P, C.POINTER(LaunchConfig)]),
     "prr_graph_destroy": (None, [_P]),
+    "prr_deck_load": (C.c_int, [C.c_char_p, C.POINTER(_P), C.c_char_p, C.c_size_t]),
+    "prr_deck_parse_string": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
+    "prr_deck_free": (None, [_P]),
+    "prr_deck_has_block": (C.c_int, [_P, C.c_char_p]),
+    "prr_deck_has": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
+    "prr_deck_get": (C.c_size_t, [_P, C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t]),
+    "prr_deck_geti": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
+    "prr_deck_getf": (C.c_float, [_P, C.c_char_p, C.c_char_p, C.c_float]),
+    "prr_deck_frame_count": (C.c_int, [_P]),
+    "prr_deck_sphere_count": (C.c_int, [_P]),
+    "prr_deck_sphere_texture": (C.c_size_t, [_P, C.c_int, C.c_char_p, C.c_size_t]),
+    "prr_deck_frame": (C.c_int, [_P, C.c_int, C.POINTER(FrameDesc), C.c_char_p, C.c_size_t]),
+    "prr_run_deck": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int, C.POINTER(Stats)]),
+    "prr_image_load": (C.c_int, [C.c_char_p, C.POINTER(_u8p), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p,
+                                 C.c_size_t]),
+    "prr_image_free": (None, [_u8p]),
+    "prr_png_write": (C.c_int, [C.c_char_p, _u8p, C.c_int, C.c_int]),
     "prr_render_noalloc": (C.c_int, [C.POINTER(FrameDesc), C.c_int, C.POINTER(_P), C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), _P, _P, _P, C.c_char_p, C.c_size_t]),
 }
@@ -138,7 +155,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
 def header_functions(header: Path = HEADER) -> list[str]:
     """Names of the functions include/prr.h declares."""
     text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
-    return sorted(set(re.findall(r"\b(prr_[a-z0-9_]+)\s*\(", text)) - {"prr_ctx", "prr_graph"})
+    return sorted(set(re.findall(r"\b(prr_[a-z0-9_]+)\s*\(", text)) - {"prr_ctx", "prr_graph", "prr_deck"})
 
 
 def check(status: int, ctx=None) -> None:

@@ -28,8 +28,8 @@ INCLUDE = REPO / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NO_FMAD = {"k_reference.cu", "post.cu"}
 CU_SOURCES = ["capi.cu", "render.cu", "k_reference.cu", "post.cu", "k_persistent.cu", "k_plain.cu", "fma_peak.cu",
-              "noalloc.cu", "k_adjoint.cu", "graph.cu"]
-CPP_SOURCES = ["textures.cpp"]
+              "noalloc.cu", "k_adjoint.cu", "graph.cu", "frame_loop.cu"]
+CPP_SOURCES = ["textures.cpp", "deck.cpp", "image_io.cpp"]
 
 
 def nvcc() -> str:
@@ -86,7 +86,13 @@ def build_library(verbose: bool = False, ptxas_verbose: bool = False, defines: l
             continue
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-I", str(INCLUDE), "-c", str(s), "-o", str(o)], verbose)
     if not _newer(lib, objs):
-        _run([nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs)], verbose)
+        _run([nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lz"], verbose)
+    # the `prr` command (the reference's executable, prr.cpp:345-404)
+    exe = lib.parent / "prr"
+    main_src = CSRC / "prr_main.cpp"
+    if not _newer(exe, [main_src, lib, INCLUDE / "prr.h"]):
+        _run(["g++", "-O2", "-std=c++17", "-I", str(INCLUDE), str(main_src), "-L", str(lib.parent),
+              "-l:" + lib.name, "-Wl,-rpath,$ORIGIN", "-o", str(exe)], verbose)
     return lib
 
 
