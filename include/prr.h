@@ -278,6 +278,28 @@ prr_status prr_graph_stats(prr_graph *g, prr_stats *stats);
 prr_status prr_graph_get_launch_config(const prr_graph *g, prr_launch_config *cfg);
 void prr_graph_destroy(prr_graph *g);
 
+/* ---- metric plug-ins (replaces the compile-time selection of
+ *      main/metric.h:12; the hooks a plug-in defines are the ones
+ *      kernels/solver.cuh:43,81,87,96,106,154,163-168,197,209 and
+ *      prr.cpp:319 call) ----
+ * A metric header written for the reference - getMetric, getGeod,
+ * User_LOOP, User_UPDATE, User_ENDLOOP and the rayToRGB kernel, including
+ * "../main/base.h", "../main/Camera.h", "../main/Spacetime.h" and
+ * "../cudamaths/mats.h" - is compiled UNCHANGED against this library's
+ * compatibility tree (parrelray_b200/compat) into libprr_metric_<name>.so
+ * (python -m parrelray_b200.build --metric <header>).  prr_load_metric_plugin
+ * loads such a library into the context and returns in *metric_id the value
+ * to put in prr_frame_desc.metric (PRR_METRIC_PLUGIN0 + k).  Plug-in frames
+ * render in REFERENCE mode: the solver of kernels/solver.cuh calling the
+ * header's hooks, then the header's rayToRGB, then the usual SSAA combine /
+ * FXAA / quantisation.  The Spacetime the hooks see carries mass, spin
+ * (prr_frame_desc.spin, for any plug-in) and the frame's spheres.  Loading
+ * the same path twice returns the same id; libraries stay loaded until the
+ * process exits. */
+#define PRR_METRIC_PLUGIN0 16
+#define PRR_MAX_PLUGINS 8
+prr_status prr_load_metric_plugin(prr_ctx *ctx, const char *path, int *metric_id);
+
 /* ---- scheduler tuning (new) ---- */
 prr_status prr_set_schedule(prr_ctx *ctx, int schedule, const prr_launch_config *cfg);
 prr_status prr_get_launch_config(prr_ctx *ctx, prr_launch_config *cfg);

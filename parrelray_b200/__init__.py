@@ -118,6 +118,12 @@ class Context:
                                                C.c_void_p(d_rgbf) if d_rgbf else None,
                                                C.c_void_p(stream) if stream else None))
 
+    def load_metric_plugin(self, path) -> int:
+        """prr_load_metric_plugin: returns the metric id for frames."""
+        mid = C.c_int()
+        self._check(self.lib.prr_load_metric_plugin(self.h, str(path).encode(), C.byref(mid)))
+        return mid.value
+
     def run_deck(self, path, first: int = 0, count: int = -1, prefix: str | None = None, batch: int = 16) -> Stats:
         """prr_run_deck: renders a deck's frames to <prefix>image_<i>.png."""
         st = Stats()

@@ -25,6 +25,7 @@ RESULT_SUCCESS, RESULT_MATH_ERROR, RESULT_IO_ERROR, RESULT_INFINITE_GEO, RESULT_
 SOLVER_EULER, SOLVER_RKF45 = 0, 2
 SSAA_NONE, SSAA_REGULAR = 0, 1
 METRIC_FLAT, METRIC_SCHWARZSCHILD, METRIC_KERR = 0, 1, 2
+METRIC_PLUGIN0 = 16
 MODE_REFERENCE, MODE_PHYSICAL = 0, 1
 PREC_FP32, PREC_FP64, PREC_SPLIT = 0, 1, 2
 SCHED_PLAIN, SCHED_PERSISTENT = 0, 1
@@ -121,6 +122,7 @@ SIGNATURES = {
                                  C.c_size_t]),
     "prr_image_free": (None, [_u8p]),
     "prr_png_write": (C.c_int, [C.c_char_p, _u8p, C.c_int, C.c_int]),
+    "prr_load_metric_plugin": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int)]),
     "prr_render_noalloc": (C.c_int, [C.POINTER(FrameDesc), C.c_int, C.POINTER(_P), C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), _P, _P, _P, C.c_char_p, C.c_size_t]),
 }

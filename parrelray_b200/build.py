@@ -86,7 +86,7 @@ def build_library(verbose: bool = False, ptxas_verbose: bool = False, defines: l
             continue
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-I", str(INCLUDE), "-c", str(s), "-o", str(o)], verbose)
     if not _newer(lib, objs):
-        _run([nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lz"], verbose)
+        _run([nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lz", "-ldl"], verbose)
     # the `prr` command (the reference's executable, prr.cpp:345-404)
     exe = lib.parent / "prr"
     main_src = CSRC / "prr_main.cpp"
@@ -94,6 +94,55 @@ def build_library(verbose: bool = False, ptxas_verbose: bool = False, defines: l
         _run(["g++", "-O2", "-std=c++17", "-I", str(INCLUDE), str(main_src), "-L", str(lib.parent),
               "-l:" + lib.name, "-Wl,-rpath,$ORIGIN", "-o", str(exe)], verbose)
     return lib
+
+
+COMPAT = PKG / "compat"
+
+
+def build_metric_plugin(header: Path, name: str | None = None, verbose: bool = False,
+                        lib_dir: Path | None = None) -> Path:
+    """Compiles an unchanged ParRelRay metric plug-in header (the files the
+    reference's main/metric.h selects, e.g. metrics/schwarzschild.cuh) into
+    libprr_metric_<name>.so for prr_load_metric_plugin.  The header is copied
+    into a staging tree whose main/, cudamaths/ and scene/ are this package's
+    compatibility headers, so its "../main/base.h"-style includes resolve to
+    them; the staging copy is deleted after the build."""
+    header = Path(header)
+    name = name or header.stem.replace(" ", "").replace("-", "")
+    out = Path(lib_dir or LIBDIR) / f"libprr_metric_{name}.so"
+    deps = [header, COMPAT / "prr_plugin.cuh"] + sorted(COMPAT.rglob("*.h")) + sorted(COMPAT.rglob("*.cuh")) + _headers()
+    if _newer(out, deps):
+        return out
+    stage = BUILD / "plugins" / name
+    if stage.exists():
+        shutil.rmtree(stage)
+    for sub in ("main", "cudamaths", "scene"):
+        shutil.copytree(COMPAT / sub, stage / sub)
+    (stage / "metrics").mkdir(parents=True)
+    shutil.copy(header, stage / "metrics" / header.name)
+    tu = stage / f"plugin_{name}.cu"
+    tu.write_text(f'#include "metrics/{header.name}"\n#include "prr_plugin.cuh"\n')
+    out.parent.mkdir(parents=True, exist_ok=True)
+    try:
+        _run([nvcc(), "-fmad=false", *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+              "--expt-relaxed-constexpr", "-w", f'-DPRR_PLUGIN_NAME="{name}"', "-I", str(stage), "-I", str(COMPAT),
+              "-I", str(CSRC), "-I", str(INCLUDE), str(tu), "-o", str(out)], verbose)
+    finally:
+        shutil.rmtree(stage, ignore_errors=True)
+    return out
+
+
+def build_plugins(verbose: bool = False) -> list[Path]:
+    """The Kerr plug-in shipped in compat/metrics, and - where the reference
+    tree is mounted - the reference's own Schwarzschild and flat headers,
+    compiled unchanged."""
+    outs = [build_metric_plugin(COMPAT / "metrics" / "kerr.cuh", "kerr", verbose)]
+    ref = Path(os.environ.get("PRR_REFERENCE", "/root/reference"))
+    for stem in ("schwarzschild", "flat"):
+        h = ref / "metrics" / f"{stem}.cuh"
+        if h.exists():
+            outs.append(build_metric_plugin(h, stem, verbose))
+    return outs
 
 
 ORACLE_DIR = REPO / "oracle"
@@ -134,6 +183,7 @@ def main(argv: list[str] | None = None) -> int:
     ap.add_argument("--ptxas", action="store_true", help="rebuild with -Xptxas -v (register/spill report)")
     a = ap.parse_args(argv)
     build_library(a.verbose, a.ptxas)
+    build_plugins(a.verbose)
     if a.oracle:
         build_oracle(a.verbose)
         build_reference(a.verbose)

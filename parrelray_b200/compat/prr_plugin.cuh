@@ -1,0 +1,231 @@
+#pragma once
+// prr_plugin.cuh - a REFERENCE-mode renderer built around an unchanged
+// ParRelRay metric plug-in header.
+//
+// The reference's "plug-in API" is compile-time: main/metric.h includes one
+// header from metrics/ that defines getMetric, getGeod, User_LOOP,
+// User_UPDATE, User_ENDLOOP and the rayToRGB kernel, and the solver
+// (kernels/solver.cuh) and frame loop (prr.cpp:237-341) call them.  The
+// plug-in build (parrelray_b200/build.py: build_metric_plugin) places such a
+// header in a directory beside this library's compatibility tree
+// (compat/main, compat/cudamaths, compat/scene: the reference's type shapes)
+// and compiles one translation unit:
+//
+//     #include "metrics/<header>"   // the plug-in, unchanged
+//     #include "prr_plugin.cuh"     // this file
+//
+// into libprr_metric_<name>.so.  prr_load_metric_plugin() loads it into a
+// context; frames whose metric is the id it returns are traced here:
+//   k_plugin_trace  ray placement (createRays_none/regular), initRays with the
+//                   header's getMetric, and trace_RKF / trace_Euler with the
+//                   header's getGeod and hooks (the library's solver, which
+//                   follows kernels/solver.cuh step for step, instantiated on
+//                   the header's hooks); writes the 48-byte Ray records;
+//   rayToRGB        the header's own kernel, launched as prr.cpp:317-319 does;
+//   k_plugin_collect per-sample colours and counters.
+// SSAA combine, FXAA and quantisation then run in the library as for the
+// built-in metrics.  Built with -fmad=false, as the built-in REFERENCE path.
+#include "kernels.cuh"
+#include "ref_stepper.cuh"
+
+#ifndef PRR_PLUGIN_NAME
+#define PRR_PLUGIN_NAME "plugin"
+#endif
+
+namespace prr_plugin {
+
+using prr::FrameParams;
+using prr::RefRay;
+using prr::V4;
+
+// The reference's by-value kernel arguments for one frame.  `d_fp` is the
+// frame's parameter block in device memory (the scene's spheres).
+__host__ __device__ inline Camera make_camera(const FrameParams &fp)
+{
+    Camera c(f3(fp.cam[0], fp.cam[1], fp.cam[2]), fp.alpha, fp.beta, fp.vfov, i2(fp.width, fp.height),
+             fp.ssaa == 0 ? SSAA_DISTR::NONE : SSAA_DISTR::REGULAR, fp.samples);
+    c.computeVectors();
+    return c;
+}
+
+__host__ __device__ inline Spacetime make_space(const FrameParams &fp, const FrameParams *d_fp)
+{
+    Spacetime s;
+    s.setBhMass(fp.M);
+    s.setBhSpin(fp.a);
+    s.fp = d_fp;
+    return s;
+}
+
+__host__ __device__ inline Tracer make_tracer(const FrameParams &fp)
+{
+    Tracer t;
+    t.h = fp.h; t.hmin = fp.hmin; t.hmax = fp.hmax; t.eps = fp.eps;
+    t.sph1.tex = tex2d(fp.bg);
+    t.sph1.rout = fp.rout;
+    t.sph2.tex = tex2d();
+    t.sph2.rout = fp.rout;
+    t.solver = fp.solver == PRR_SOLVER_EULER ? SOLVER::EULER : SOLVER::RUNGE_KUTTA_FEHLBERG;
+    return t;
+}
+
+__device__ inline void to_ray(const RefRay &R, Ray &T)
+{
+    T.uv = f2(R.uvx, R.uvy);
+    T.result = (RESULT)R.result;
+    T.r = f4(R.r.x, R.r.y, R.r.z, R.r.w);
+    T.u = f4(R.u.x, R.u.y, R.u.z, R.u.w);
+    T.I = 0.0f;
+}
+
+__device__ inline void from_ray(const Ray &T, RefRay &R)
+{
+    R.result = (int)T.result;
+    R.r = {T.r.x, T.r.y, T.r.z, T.r.w};
+    R.u = {T.u.x, T.u.y, T.u.z, T.u.w};
+}
+
+// The header's functions as the solver's hook set (ref_stepper.cuh).
+struct PluginHooks {
+    Camera cam;
+    Spacetime space;
+    Tracer trace;
+
+    __device__ void metric(const RefRay &R, float g[16]) const
+    {
+        Ray T;
+        to_ray(R, T);
+        mat4 m = getMetric(&T, space);
+        for (int i = 0; i < 16; i++) g[i] = m.e[i];
+    }
+    __device__ V4<float> geod(const V4<float> &x, const V4<float> &u) const
+    {
+        f4 d = getGeod(f4(x.x, x.y, x.z, x.w), f4(u.x, u.y, u.z, u.w), space);
+        return {d.x, d.y, d.z, d.w};
+    }
+    __device__ bool loop(RefRay &R) const
+    {
+        Ray T;
+        to_ray(R, T);
+        bool go = User_LOOP(&T, cam, space);
+        from_ray(T, R);
+        return go;
+    }
+    __device__ bool update(RefRay &R, float h) const
+    {
+        Ray T;
+        to_ray(R, T);
+        bool go = User_UPDATE(&T, cam, space, h);
+        from_ray(T, R);
+        return go;
+    }
+    __device__ bool endloop(RefRay &R, float trace_h) const
+    {
+        Ray T;
+        to_ray(R, T);
+        Tracer t = trace;
+        t.h = trace_h;  // trace_RKF passes its tracer with h = the last accepted step (solver.cuh:199)
+        bool go = User_ENDLOOP(&T, cam, space, t);
+        from_ray(T, R);
+        return go;
+    }
+};
+
+__device__ __forceinline__ void warp_add(unsigned long long *p, unsigned long long v)
+{
+    unsigned mask = __activemask();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    if ((threadIdx.x & 31) == (__ffs(mask) - 1)) atomicAdd(p, v);
+}
+
+__global__ void __launch_bounds__(128) k_plugin_trace(const FrameParams *__restrict__ fps, int frame, long long nrays,
+                                                      Ray *__restrict__ rays, float *__restrict__ state,
+                                                      unsigned long long *__restrict__ counters)
+{
+    long long rid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (rid >= nrays) return;
+    const FrameParams &fp = fps[frame];
+    const int S = fp.samples;
+    long long pix = rid / S;
+    int s = (int)(rid - pix * S);
+    int x = (int)(pix % fp.width), y = (int)(pix / fp.width);
+    PluginHooks hk{make_camera(fp), make_space(fp, &fps[frame]), make_tracer(fp)};
+    RefRay R;
+    prr::ref_init_h(fp, hk, x, y, s, R);
+    if (fp.solver == PRR_SOLVER_EULER) prr::ref_euler_h(fp, hk, R);
+    else prr::ref_rkf_h(fp, hk, R);
+    Ray T;
+    to_ray(R, T);
+    rays[rid] = T;
+    if (state) {
+        float *o = state + 12 * rid;
+        o[0] = R.uvx; o[1] = R.uvy; o[2] = (float)R.result;
+        o[3] = R.r.x; o[4] = R.r.y; o[5] = R.r.z; o[6] = R.r.w;
+        o[7] = R.u.x; o[8] = R.u.y; o[9] = R.u.z; o[10] = R.u.w;
+        o[11] = (float)R.accepted;
+    }
+    if (counters) {
+        warp_add(&counters[prr::C_RAYS], 1ull);
+        warp_add(&counters[prr::C_ATTEMPTS], (unsigned long long)R.attempts);
+        warp_add(&counters[prr::C_ACCEPTED], (unsigned long long)R.accepted);
+    }
+}
+
+// Per-sample colour (Ray::u after rayToRGB) and outcome counters.
+__global__ void k_plugin_collect(const Ray *__restrict__ rays, long long nrays, float rout, float *__restrict__ rgb,
+                                 unsigned long long *__restrict__ counters)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrays) return;
+    Ray T = rays[i];
+    if (rgb) { rgb[3 * i] = T.u.x; rgb[3 * i + 1] = T.u.y; rgb[3 * i + 2] = T.u.z; }
+    if (counters) {
+        int cls;
+        switch (T.result) {
+        case RESULT::SUCCESS: cls = T.r.xyz().norm() >= rout ? prr::C_ESCAPED : prr::C_CAPTURED; break;
+        case RESULT::INTERSECTION: cls = prr::C_INTERSECTION; break;
+        case RESULT::INFINITE_GEO: cls = prr::C_INFINITE; break;
+        default: cls = prr::C_MATH_ERROR;
+        }
+        atomicAdd(&counters[cls], 1ull);
+    }
+}
+
+}  // namespace prr_plugin
+
+// ---- the plug-in library's C entry points (loaded by prr_load_metric_plugin) ----
+
+extern "C" int prr_plugin_abi_version(void) { return PRR_ABI_VERSION; }
+extern "C" size_t prr_plugin_frame_params_size(void) { return sizeof(prr::FrameParams); }
+extern "C" size_t prr_plugin_ray_bytes(void) { return sizeof(Ray); }
+extern "C" const char *prr_plugin_name(void) { return PRR_PLUGIN_NAME; }
+
+// Traces frame `frame` of the device frame table d_fps (h_fp: the same block
+// on the host) into d_rays (nrays Ray records), and writes the per-sample
+// colours d_rgb (3 floats/ray) and, when non-null, the per-ray states d_state
+// (12 floats/ray) and counters.  Asynchronous on `stream`; returns a
+// cudaError_t.
+extern "C" int prr_plugin_trace(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays,
+                                float *d_state, float *d_rgb, unsigned long long *d_counters, void *stream)
+{
+    using namespace prr_plugin;
+    if (nrays <= 0) return (int)cudaSuccess;
+    cudaStream_t st = (cudaStream_t)stream;
+    const FrameParams &fp = *(const FrameParams *)h_fp;
+    const FrameParams *dfp = (const FrameParams *)d_fps;
+    Ray *rays = (Ray *)d_rays;
+    const int block = 128;
+    k_plugin_trace<<<(unsigned)((nrays + block - 1) / block), block, 0, st>>>(dfp, frame, nrays, rays, d_state, d_counters);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return (int)e;
+    // rayToRGB as renderframe launches it (prr.cpp:317-319)
+    Camera cam = make_camera(fp);
+    Spacetime space = make_space(fp, dfp + frame);
+    Tracer trace = make_tracer(fp);
+    dim3 blocks(fp.samples * fp.width / 8 + 1, fp.height / 8 + 1), threads(8, 8);
+    rayToRGB<<<blocks, threads, 0, st>>>(rays, cam, space, trace, fp.samples);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    k_plugin_collect<<<(unsigned)((nrays + 255) / 256), 256, 0, st>>>(rays, nrays, fp.rout, d_rgb, d_counters);
+    return (int)cudaGetLastError();
+}

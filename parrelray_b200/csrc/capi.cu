@@ -1,5 +1,7 @@
 // capi.cu - the C ABI of include/prr.h: context, textures, frame
 // validation, dispatch to the REFERENCE / PLAIN / PERSISTENT paths, stats.
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -151,6 +153,41 @@ void prr_destroy(prr_ctx *ctx)
 }
 
 const char *prr_last_error(const prr_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+prr_status prr_load_metric_plugin(prr_ctx *ctx, const char *path, int *metric_id)
+{
+    if (!ctx) return PRR_ERR_INVALID;
+    if (!path || !metric_id) { fail(ctx, "prr_load_metric_plugin: null path or output"); return PRR_ERR_INVALID; }
+    for (size_t k = 0; k < ctx->plugins.size(); k++)
+        if (ctx->plugins[k].path == path) { *metric_id = PRR_METRIC_PLUGIN0 + (int)k; return PRR_OK; }
+    if ((int)ctx->plugins.size() >= PRR_MAX_PLUGINS) { fail(ctx, "prr_load_metric_plugin: PRR_MAX_PLUGINS plug-ins already loaded"); return PRR_ERR_INVALID; }
+    void *h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+    if (!h) { fail(ctx, std::string("prr_load_metric_plugin: ") + dlerror()); return PRR_ERR_IO; }
+    auto abi = (int (*)(void))dlsym(h, "prr_plugin_abi_version");
+    auto fps = (size_t (*)(void))dlsym(h, "prr_plugin_frame_params_size");
+    auto rb = (size_t (*)(void))dlsym(h, "prr_plugin_ray_bytes");
+    auto nm = (const char *(*)(void))dlsym(h, "prr_plugin_name");
+    void *tr = dlsym(h, "prr_plugin_trace");
+    if (!abi || !fps || !rb || !nm || !tr) {
+        dlclose(h);
+        fail(ctx, std::string("prr_load_metric_plugin: ") + path + " is not a prr metric plug-in (missing prr_plugin_* symbols)");
+        return PRR_ERR_INVALID;
+    }
+    if (abi() != PRR_ABI_VERSION || fps() != sizeof(FrameParams) || rb() != 48) {
+        dlclose(h);
+        fail(ctx, std::string("prr_load_metric_plugin: ") + path + " was built for another library version; rebuild it");
+        return PRR_ERR_INVALID;
+    }
+    MetricPlugin pl;
+    pl.path = path;
+    pl.name = nm();
+    pl.handle = h;
+    pl.ray_bytes = rb();
+    pl.trace = (decltype(pl.trace))tr;
+    ctx->plugins.push_back(pl);
+    *metric_id = PRR_METRIC_PLUGIN0 + (int)ctx->plugins.size() - 1;
+    return PRR_OK;
+}
 
 prr_status prr_upload_texture(prr_ctx *ctx, int id, const uint8_t *rgba8, int w, int h)
 {

@@ -21,6 +21,15 @@ struct TexSlot {
     int w = 0, h = 0;
 };
 
+// A loaded metric plug-in library (compat/prr_plugin.cuh).
+struct MetricPlugin {
+    std::string path, name;
+    void *handle = nullptr;
+    size_t ray_bytes = 0;
+    int (*trace)(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays, float *d_state,
+                 float *d_rgb, unsigned long long *d_counters, void *stream) = nullptr;
+};
+
 struct prr_ctx {
     int device = 0;
     int nsm = 0;
@@ -33,6 +42,7 @@ struct prr_ctx {
     prr_launch_config cfg{};
     int geod_table = -1;  // -1: per schedule (PERSISTENT contraction, PLAIN table); 0: contraction; 1: table
     long long watchdog_cycles = 0;
+    std::vector<MetricPlugin> plugins;
     int last_launches = 0;
     float last_ms = 0.f;
     float last_trace_ms = 0.f;
@@ -56,6 +66,13 @@ struct RenderPlan {
     int precision = PRR_PREC_FP32;
     bool any_fxaa = false;
 };
+
+// The plug-in of a frame's metric id, or null for a built-in metric.
+inline const MetricPlugin *frame_plugin(const prr_ctx *ctx, int metric)
+{
+    int k = metric - PRR_METRIC_PLUGIN0;
+    return (k >= 0 && k < (int)ctx->plugins.size()) ? &ctx->plugins[k] : nullptr;
+}
 
 // render.cu
 prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderPlan &plan);

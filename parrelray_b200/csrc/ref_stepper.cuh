@@ -44,16 +44,24 @@ PRR_DEV V4<float> ref_geod(const FrameParams &fp, const V4<float> &x, const V4<f
 
 PRR_DEV bool isnan4(const V4<float> &a) { return isnan(a.x) || isnan(a.y) || isnan(a.z) || isnan(a.w); }
 
+// The solver below calls the metric through a hooks object H with the
+// reference's hook set (kernels/solver.cuh:43,81,87,96,106,154,163-168,197,
+// 209): metric(R, g) = getMetric, geod(x, u) = getGeod, loop(R) = User_LOOP,
+// update(R, h) = User_UPDATE, endloop(R, trace_h) = User_ENDLOOP.
+// BuiltinHooks are the library's flat / Schwarzschild / Kerr hooks; a metric
+// plug-in header supplies its own (parrelray_b200/compat/prr_plugin.cuh).
+
 // initRays
-PRR_DEV void ref_init(const FrameParams &fp, int x, int y, int s, RefRay &R)
+template <class H> PRR_DEV void ref_init_h(const FrameParams &fp, const H &hk, int x, int y, int s, RefRay &R)
 {
     ray_uv(fp, x, y, s, R.uvx, R.uvy);
     V3<float> dir = ray_dir(fp, R.uvx, R.uvy);
     R.r = {fp.cam[0], fp.cam[1], fp.cam[2], 0.0f};
+    R.u = {0.0f, 0.0f, 0.0f, 0.0f};
+    R.result = PRR_RESULT_SUCCESS;
     V4<float> u = {dir.x, dir.y, dir.z, 1.0f};
     float g[16];
-    if (fp.metric == PRR_METRIC_SCHWARZSCHILD) metric_schw_ref(R.r.x, R.r.y, R.r.z, fp.rs, g);
-    else metric_ks<float>(R.r.x, R.r.y, R.r.z, fp.metric == PRR_METRIC_FLAT ? 0.0f : fp.M, fp.a, g);
+    hk.metric(R, g);
     float a = g[15];
     float b = 2.0f * (g[12] * u.x + g[13] * u.y + g[14] * u.z);
     float c = g[0] * u.x * u.x + g[5] * u.y * u.y + g[10] * u.z * u.z + 2.0f * (g[1] * u.x * u.y + g[2] * u.x * u.z + g[6] * u.y * u.z);
@@ -64,6 +72,12 @@ PRR_DEV void ref_init(const FrameParams &fp, int x, int y, int s, RefRay &R)
     R.result = PRR_RESULT_SUCCESS;
     R.accepted = 0;
     R.attempts = 0;
+}
+
+PRR_DEV void ref_metric(const FrameParams &fp, const RefRay &R, float g[16])
+{
+    if (fp.metric == PRR_METRIC_SCHWARZSCHILD) metric_schw_ref(R.r.x, R.r.y, R.r.z, fp.rs, g);
+    else metric_ks<float>(R.r.x, R.r.y, R.r.z, fp.metric == PRR_METRIC_FLAT ? 0.0f : fp.M, fp.a, g);
 }
 
 // User_UPDATE
@@ -84,10 +98,20 @@ PRR_DEV bool ref_endloop(const FrameParams &fp, RefRay &R, float th)
     return true;
 }
 
+struct BuiltinHooks {
+    const FrameParams &fp;
+    PRR_DEV void metric(const RefRay &R, float g[16]) const { ref_metric(fp, R, g); }
+    PRR_DEV V4<float> geod(const V4<float> &x, const V4<float> &u) const { return ref_geod(fp, x, u); }
+    PRR_DEV bool loop(RefRay &) const { return true; }
+    PRR_DEV bool update(RefRay &R, float h) const { return ref_update(fp, R, h); }
+    PRR_DEV bool endloop(RefRay &R, float trace_h) const { return ref_endloop(fp, R, trace_h); }
+};
+
 // trace_RKF
-PRR_DEV void ref_rkf(const FrameParams &fp, RefRay &R)
+template <class H> PRR_DEV void ref_rkf_h(const FrameParams &fp, const H &hk, RefRay &R)
 {
     using K = RefTab;
+    if (!hk.loop(R)) { R.result = PRR_RESULT_INFINITE_GEO; return; }
     float h = fp.h, hmin = fp.hmin, hmax = fp.hmax, _h = h, eps = fp.eps, trace_h = fp.h;
     V4<float> x = R.r, u = R.u, _x = x, _u = u, __x, __u;
     bool intersect = false;
@@ -96,21 +120,21 @@ PRR_DEV void ref_rkf(const FrameParams &fp, RefRay &R)
         i += 1;
         R.attempts = i;
         V4<float> kx1 = v4scl(h, u);
-        V4<float> ku1 = v4scl(h, ref_geod(fp, x, u));
+        V4<float> ku1 = v4scl(h, hk.geod(x, u));
         V4<float> z2x = v4add(x, v4scl(K::A21, kx1)), z2u = v4add(u, v4scl(K::A21, kx1));
-        V4<float> kx2 = v4scl(h, z2u), ku2 = v4scl(h, ref_geod(fp, z2x, z2u));
+        V4<float> kx2 = v4scl(h, z2u), ku2 = v4scl(h, hk.geod(z2x, z2u));
         V4<float> z3x = v4add(v4add(x, v4scl(K::A31, kx1)), v4scl(K::A32, kx2));
         V4<float> z3u = v4add(v4add(u, v4scl(K::A31, kx1)), v4scl(K::A32, ku2));
-        V4<float> kx3 = v4scl(h, z3u), ku3 = v4scl(h, ref_geod(fp, z3x, z3u));
+        V4<float> kx3 = v4scl(h, z3u), ku3 = v4scl(h, hk.geod(z3x, z3u));
         V4<float> z4x = v4add(v4add(v4add(x, v4scl(K::A41, kx1)), v4scl(K::A42, kx2)), v4scl(K::A43, kx3));
         V4<float> z4u = v4add(v4add(v4add(u, v4scl(K::A41, kx1)), v4scl(K::A42, ku2)), v4scl(K::A43, ku3));
-        V4<float> kx4 = v4scl(h, z4u), ku4 = v4scl(h, ref_geod(fp, z4x, z4u));
+        V4<float> kx4 = v4scl(h, z4u), ku4 = v4scl(h, hk.geod(z4x, z4u));
         V4<float> z5x = v4add(v4add(v4add(v4add(x, v4scl(K::A51, kx1)), v4scl(K::A52, kx2)), v4scl(K::A53, kx3)), v4scl(K::A54, kx4));
         V4<float> z5u = v4add(v4add(v4add(v4add(u, v4scl(K::A51, kx1)), v4scl(K::A52, ku2)), v4scl(K::A53, ku3)), v4scl(K::A54, ku4));
-        V4<float> kx5 = v4scl(h, z5u), ku5 = v4scl(h, ref_geod(fp, z5x, z5u));
+        V4<float> kx5 = v4scl(h, z5u), ku5 = v4scl(h, hk.geod(z5x, z5u));
         V4<float> z6x = v4add(v4add(v4add(v4add(v4add(x, v4scl(K::A61, kx1)), v4scl(K::A62, kx2)), v4scl(K::A63, kx3)), v4scl(K::A64, kx4)), v4scl(K::A65, kx5));
         V4<float> z6u = v4add(v4add(v4add(v4add(v4add(u, v4scl(K::A61, kx1)), v4scl(K::A62, ku2)), v4scl(K::A63, ku3)), v4scl(K::A64, ku4)), v4scl(K::A65, ku5));
-        V4<float> kx6 = v4scl(h, z6u), ku6 = v4scl(h, ref_geod(fp, z6x, z6u));
+        V4<float> kx6 = v4scl(h, z6u), ku6 = v4scl(h, hk.geod(z6x, z6u));
 
         _x = v4add(v4add(v4add(v4add(v4add(v4add(x, v4scl(K::K41, kx1)), v4scl(K::K42, kx2)), v4scl(K::K43, kx3)), v4scl(K::K44, kx4)), v4scl(K::K45, kx5)), v4scl(K::K46, kx6));
         _u = v4add(v4add(v4add(v4add(v4add(v4add(u, v4scl(K::K41, ku1)), v4scl(K::K42, ku2)), v4scl(K::K43, ku3)), v4scl(K::K44, ku4)), v4scl(K::K45, ku5)), v4scl(K::K46, ku6));
@@ -130,13 +154,13 @@ PRR_DEV void ref_rkf(const FrameParams &fp, RefRay &R)
 
         R.r = _x; R.u = _u;
         R.accepted += 1;
-        if (ref_update(fp, R, h)) {
+        if (hk.update(R, h)) {
             if (!intersect) h = _h;
             x = _x; u = _u; R.r = x; R.u = u; trace_h = h;
         } else if (R.result == PRR_RESULT_INTERSECTION && !intersect) {
             intersect = true; h = hmin; continue;
         }
-        if (!ref_endloop(fp, R, trace_h)) return;
+        if (!hk.endloop(R, trace_h)) return;
         x = R.r; u = R.u;
         l += h;
     }
@@ -144,23 +168,28 @@ PRR_DEV void ref_rkf(const FrameParams &fp, RefRay &R)
 }
 
 // trace_Euler
-PRR_DEV void ref_euler(const FrameParams &fp, RefRay &R)
+template <class H> PRR_DEV void ref_euler_h(const FrameParams &fp, const H &hk, RefRay &R)
 {
+    if (!hk.loop(R)) { R.result = PRR_RESULT_INFINITE_GEO; return; }
     bool intersect = false;
     float h = fp.h;
     for (float l = 0.0f; l < 5000.0f; l += h) {
-        V4<float> du = ref_geod(fp, R.r, R.u);
+        V4<float> du = hk.geod(R.r, R.u);
         R.attempts += 1;
         if (isnan4(du)) { R.result = PRR_RESULT_MATH_ERROR; return; }
         R.r = v4add(R.r, v4scl(h, R.u));
         R.u = v4add(R.u, v4scl(h, du));
         R.accepted += 1;
-        if (!ref_update(fp, R, h)) {
+        if (!hk.update(R, h)) {
             if (R.result == PRR_RESULT_INTERSECTION && !intersect) { intersect = true; h = fp.hmin; continue; }
         }
-        if (!ref_endloop(fp, R, fp.h)) return;
+        if (!hk.endloop(R, fp.h)) return;
     }
     R.result = PRR_RESULT_INFINITE_GEO;
 }
+
+PRR_DEV void ref_init(const FrameParams &fp, int x, int y, int s, RefRay &R) { ref_init_h(fp, BuiltinHooks{fp}, x, y, s, R); }
+PRR_DEV void ref_rkf(const FrameParams &fp, RefRay &R) { ref_rkf_h(fp, BuiltinHooks{fp}, R); }
+PRR_DEV void ref_euler(const FrameParams &fp, RefRay &R) { ref_euler_h(fp, BuiltinHooks{fp}, R); }
 
 }  // namespace prr

@@ -87,7 +87,10 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
         if (!finite_pos(d.vfov) || d.vfov >= 6.3f) return bad(ctx, f, "vfov must be in (0, 2*pi) radians");
         for (int k = 0; k < 3; k++) if (!std::isfinite(d.cam_pos[k])) return bad(ctx, f, "camera position is not finite");
         if (!std::isfinite(d.cam_alpha) || !std::isfinite(d.cam_beta)) return bad(ctx, f, "camera angles are not finite");
-        if (d.metric < PRR_METRIC_FLAT || d.metric > PRR_METRIC_KERR) return bad(ctx, f, "unknown metric");
+        const MetricPlugin *plugin = frame_plugin(ctx, d.metric);
+        if ((d.metric < PRR_METRIC_FLAT || d.metric > PRR_METRIC_KERR) && !plugin)
+            return bad(ctx, f, "unknown metric (built-in 0-2, or an id from prr_load_metric_plugin)");
+        if (plugin && d.mode != PRR_MODE_REFERENCE) return bad(ctx, f, "metric plug-ins render in REFERENCE mode");
         if (!std::isfinite(d.mass) || d.mass < 0.0f) return bad(ctx, f, "mass must be >= 0");
         // M = 0 is allowed for Schwarzschild: the reference renders its example deck (input/sim.params:30,52) so
         if (d.metric == PRR_METRIC_KERR && d.mass <= 0.0f) return bad(ctx, f, "Kerr needs mass > 0");
@@ -120,9 +123,9 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
         p.width = d.width; p.height = d.height; p.samples = d.samples; p.ssaa = d.ssaa;
         p.vfov = d.vfov; p.cam[0] = d.cam_pos[0]; p.cam[1] = d.cam_pos[1]; p.cam[2] = d.cam_pos[2];
         p.alpha = d.cam_alpha; p.beta = d.cam_beta;
-        p.metric = d.metric; p.M = d.mass; p.a = d.metric == PRR_METRIC_KERR ? d.spin : 0.0f;
+        p.metric = d.metric; p.M = d.mass; p.a = (d.metric == PRR_METRIC_KERR || plugin) ? d.spin : 0.0f;
         p.rs = 2.0f * d.mass;  // Spacetime::setBhMass (main/Spacetime.h:23)
-        float rplus = d.metric == PRR_METRIC_KERR ? kerr_r_plus<float>(d.mass, d.spin) : (d.metric == PRR_METRIC_SCHWARZSCHILD ? p.rs : 0.0f);
+        float rplus = d.metric == PRR_METRIC_KERR ? kerr_r_plus<float>(d.mass, d.spin) : (d.metric == PRR_METRIC_FLAT ? 0.0f : p.rs);
         p.rstop = rplus + d.horizon_eps;
         p.rblack = rplus * 1.01f;
         p.solver = d.solver; p.mode = d.mode; p.precision = d.precision;
@@ -213,7 +216,11 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
         for (int f = 0; f < n; f++) {
             const FrameParams &p = plan.fp[f];
             long long nr = (long long)p.width * p.height * p.samples;
-            if (plan.mode == PRR_MODE_REFERENCE) {
+            if (const MetricPlugin *pl = frame_plugin(ctx, p.metric)) {
+                if ((s = alloc(ctx, ctx->rays, (size_t)nr * pl->ray_bytes, "plug-in ray records")) != PRR_OK) return s;
+                PRR_CK(ctx, (cudaError_t)pl->trace(&p, d_fp, f, nr, ctx->rays.p, nullptr, rgb, counters, st));
+                launches += 3;
+            } else if (plan.mode == PRR_MODE_REFERENCE) {
                 PRR_CK(ctx, launch_ref_trace(d_fp, f, nr, nullptr, rgb, counters, st));
                 launches++;
             } else {
@@ -287,7 +294,11 @@ prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, doub
     if ((s = alloc(ctx, ctx->sample_rgb, (size_t)nr * 3 * sizeof(float), "per-sample colours")) != PRR_OK) return s;
     float *rgb = (float *)ctx->sample_rgb.p;
     PRR_CK(ctx, cudaEventRecord(ctx->e0, st));
-    if (plan.mode == PRR_MODE_REFERENCE) {
+    if (const MetricPlugin *pl = frame_plugin(ctx, p.metric)) {
+        if ((s = alloc(ctx, ctx->rays, (size_t)nr * pl->ray_bytes, "plug-in ray records")) != PRR_OK) return s;
+        PRR_CK(ctx, (cudaError_t)pl->trace(&p, d_fp, 0, nr, ctx->rays.p, (float *)ctx->state.p, rgb, counters, st));
+        ctx->last_launches = 3;
+    } else if (plan.mode == PRR_MODE_REFERENCE) {
         PRR_CK(ctx, launch_ref_trace(d_fp, 0, nr, (float *)ctx->state.p, rgb, counters, st));
         ctx->last_launches = 1;
     } else if (ctx->schedule == PRR_SCHED_PLAIN && !h_state64) {

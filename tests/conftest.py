@@ -21,6 +21,7 @@ def built():
     from parrelray_b200 import build
 
     build.build_library()
+    build.build_plugins()
     build.build_oracle()
     build.build_reference()
     return True
