@@ -346,6 +346,9 @@ def main():
     ap.add_argument("--no-trajectory", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--launch", default=None,
+                    help="block,blocks_per_sm,compaction_interval,rays_per_thread for the persistent renderer "
+                         "(default: prr_autotune on a quarter-size copy of the frame, outside the timed region)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -371,6 +374,16 @@ def main():
     ctx.upload_textures(tex)
     frame = build_frames(rank, ws, args.width, args.height)
     npx = frame.width * frame.height
+    t_tune = time.perf_counter()
+    if args.launch:
+        b, bp, ci, rpt = (int(v) for v in args.launch.split(","))
+        ctx.set_schedule(abi.SCHED_PERSISTENT, LaunchConfig(b, bp, ci, rpt))
+        tuned_on = "given on the command line"
+    else:
+        # the launch shape does not change the arithmetic of a ray; tune it on a smaller copy of the frame
+        ctx.autotune(build_frames(rank, ws, max(args.width // 4, 8), max(args.height // 4, 8)))
+        tuned_on = f"prr_autotune on the same frame at {max(args.width // 4, 8)}x{max(args.height // 4, 8)}"
+    t_tune = time.perf_counter() - t_tune
     out8 = torch.empty(npx * 3, dtype=torch.uint8, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     stream = torch.cuda.current_stream()
@@ -506,6 +519,7 @@ def main():
             "config": {"workload": WORKLOAD, "rays_per_step": rays, "width": frame.width, "height": frame.height,
                        "samples": frame.samples, "schedule": "persistent",
                        "launch": {k: getattr(ctx.launch_config(), k) for k, _ in LaunchConfig._fields_},
+                       "launch_source": tuned_on, "autotune_s": round(t_tune, 2),
                        "l2": "256 MiB buffer written between timed steps (inside the timed region)"},
             "e2e": e2e, "clocks": clocks, "gpu_launches": int(st.kernel_launches) * args.steps,
         }

@@ -157,7 +157,9 @@ typedef struct prr_launch_config {
     int32_t block_size;          /* threads per CTA (multiple of 32) */
     int32_t blocks_per_sm;       /* resident CTAs per SM requested */
     int32_t compaction_interval; /* attempts between warp refills */
-    int32_t rays_per_thread;     /* 1 or 2 interleaved rays per lane */
+    int32_t rays_per_thread;     /* FP32 renders: pixels in flight per thread, 1 or 2 (2: the two
+                                    rays' stages share paired FP32 instructions); results do not
+                                    depend on it */
 } prr_launch_config;
 
 /* ---- lifetime (replaces prr.cpp:main 345-404, init 203-227) ---- */

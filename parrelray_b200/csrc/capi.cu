@@ -212,9 +212,9 @@ prr_status prr_set_schedule(prr_ctx *ctx, int schedule, const prr_launch_config 
     if (schedule != PRR_SCHED_PLAIN && schedule != PRR_SCHED_PERSISTENT) { fail(ctx, "unknown schedule"); return PRR_ERR_INVALID; }
     if (cfg) {
         if (cfg->block_size < 32 || cfg->block_size > 256 || cfg->block_size % 32 || cfg->blocks_per_sm < 0 ||
-            cfg->blocks_per_sm > 64 || cfg->compaction_interval < 1 || cfg->rays_per_thread != 1) {
+            cfg->blocks_per_sm > 64 || cfg->compaction_interval < 1 || cfg->rays_per_thread < 1 || cfg->rays_per_thread > 2) {
             fail(ctx, "prr_set_schedule: block_size must be a multiple of 32 in [32,256], blocks_per_sm in [0,64], "
-                      "compaction_interval >= 1, rays_per_thread == 1");
+                      "compaction_interval >= 1, rays_per_thread 1 or 2");
             return PRR_ERR_INVALID;
         }
         ctx->cfg = *cfg;

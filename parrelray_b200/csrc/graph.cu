@@ -87,6 +87,7 @@ prr_status record(prr_graph *g, cudaStream_t st)
     a.geod_table = ctx->geod_table == 1;
     a.compaction_interval = g->cfg.compaction_interval;
     a.watchdog_cycles = ctx->watchdog_cycles;
+    a.rays_per_thread = g->cfg.rays_per_thread;
     a.image = (float *)g->image.p;
     float *image = (float *)g->image.p;
     if (plan.precision == PRR_PREC_SPLIT) {

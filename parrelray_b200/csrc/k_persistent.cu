@@ -267,17 +267,17 @@ cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block,
     if (precision == PRR_PREC_FP64) return launch_one<double, 0, false>(a, block, blocks_per_sm, nsm, st);
     if (precision == PRR_PREC_SPLIT) return launch_one<float, 0, true>(a, block, blocks_per_sm, nsm, st);
     if (a.geod_table) return launch_one<float, 1, false>(a, block, blocks_per_sm, nsm, st);
-    return launch_one<float, 0, false>(a, block, blocks_per_sm, nsm, st);
+    return launch_pair(a, a.rays_per_thread == 2 ? 2 : 1, block, blocks_per_sm, nsm, st);
 }
 
-int persistent_occupancy(int precision, int geod_table, int block)
+int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread)
 {
     int n = 0;
     cudaError_t e;
     if (precision == PRR_PREC_FP64) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<double, 0, false>, block, 0);
     else if (precision == PRR_PREC_SPLIT) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 0, true>, block, 0);
     else if (geod_table) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 1, false>, block, 0);
-    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 0, false>, block, 0);
+    else return pair_occupancy(rays_per_thread == 2 ? 2 : 1, block);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
 }

@@ -55,11 +55,19 @@ struct PersistentArgs {
     int geod_table;              // 1 = Christoffel-table geodesic (for comparisons)
     int compaction_interval;     // attempts between warp refills (>= 1)
     long long watchdog_cycles;   // 0 = off
+    int rays_per_thread;         // FP32: pixel slots in flight per thread (1 or 2; 0 = 1)
 };
+// Dispatches to the kernel of the precision: FP32 with the register
+// contraction -> k_pair (k_pair.cu, rays_per_thread slots per thread);
+// FP64, SPLIT and the Christoffel-table variant -> k_persistent.
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st);
 
-// k_persistent.cu: resident CTAs per SM of the persistent kernel variant.
-int persistent_occupancy(int precision, int geod_table, int block);
+// k_persistent.cu: resident CTAs per SM of the kernel launch_persistent picks.
+int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread = 1);
+
+// k_pair.cu: the FP32 renderer with `rpt` pixel slots per thread.
+cudaError_t launch_pair(const PersistentArgs &a, int rpt, int block, int blocks_per_sm, int nsm, cudaStream_t st);
+int pair_occupancy(int rpt, int block);
 
 // k_persistent.cu: FP64 re-integration of the queued rays of a split render.
 cudaError_t launch_fp64_requeue(const PersistentArgs &a, int block, int nsm, cudaStream_t st);

@@ -185,13 +185,30 @@ enum StepStatus { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_FLAG64 = 2 };
 // hit_sphere: when non-null, an INTERSECTION stores the hit sphere's index
 // there and leaves the final state in R (otherwise R.u receives the colour,
 // as User_ENDLOOP does).
+// An attempt is split in three parts so the FP32 path can evaluate the
+// stages of two rays at once (phys_pair.cuh): phys_precheck (caps before
+// the attempt), the stages (increments dxv/duv, scaled error err and next
+// step hn), and phys_accept (accept/reject, state update, hooks).
+
+// The loop bound of trace_RKF (l < 1000, solver.cuh:158) and the attempt
+// counter; STEP_DONE when the ray ends before this attempt.
+template <class T> PRR_DEV int phys_precheck(PhysRay<T> &R, int &result, V3<float> &colour)
+{
+    if (!(R.l < (T)1000)) { result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0}; return STEP_DONE; }
+    R.i += 1;
+    return STEP_CONTINUE;
+}
+
+template <class T>
+PRR_DEV int phys_accept(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, const T dxv[4], const T duv[4], T err,
+                        T hn, int &result, V3<float> &colour, T flag_r, int *hit_sphere);
+
 template <class T, int GEOD>
 PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, int &result, V3<float> &colour,
                          T flag_r, int *hit_sphere = nullptr)
 {
     using F = Fehlberg;
-    if (!(R.l < (T)1000)) { result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0}; return STEP_DONE; }
-    R.i += 1;
+    if (phys_precheck<T>(R, result, colour) == STEP_DONE) return STEP_DONE;
     const T h = R.h;
     const V4<T> &x = R.x, &u = R.u;
 #define PRR_ST2(c)                                                                                                 \
@@ -263,7 +280,14 @@ PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, 
 #undef PRR_FIN
     T hn = (T)0.9 * h * fpow<T>(err, (T)-0.2);
     hn = fmin(fmax(hn, q.hmin), q.hmax);
+    return phys_accept<T>(fp, q, R, dxv, duv, err, hn, result, colour, flag_r, hit_sphere);
+}
 
+template <class T>
+PRR_DEV int phys_accept(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, const T dxv[4], const T duv[4], T err,
+                        T hn, int &result, V3<float> &colour, T flag_r, int *hit_sphere)
+{
+    const T h = R.h;
     if (R.intersect && R.i > 10000) R.intersect = 0;
     if (R.i > 8 * q.max_steps) { result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0}; return STEP_DONE; }
     if (err > (T)1 && h != q.hmin && !R.intersect) { R.h = hn; return STEP_CONTINUE; }

@@ -56,7 +56,7 @@ prr_status alloc(prr_ctx *ctx, DevBuf &b, size_t bytes, const char *what)
 int resolve_bpsm(prr_ctx *ctx, int precision)
 {
     if (ctx->cfg.blocks_per_sm > 0) return ctx->cfg.blocks_per_sm;
-    int b = persistent_occupancy(precision, ctx->geod_table == 1, ctx->cfg.block_size);
+    int b = persistent_occupancy(precision, ctx->geod_table == 1, ctx->cfg.block_size, ctx->cfg.rays_per_thread);
     return b > 0 ? b : 1;
 }
 
@@ -176,6 +176,7 @@ static PersistentArgs persistent_args(prr_ctx *ctx, const RenderPlan &plan)
     a.geod_table = ctx->geod_table == 1;
     a.compaction_interval = ctx->cfg.compaction_interval;
     a.watchdog_cycles = ctx->watchdog_cycles;
+    a.rays_per_thread = ctx->cfg.rays_per_thread;
     return a;
 }
 
@@ -381,8 +382,11 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
     float best_ms = 1e30f;
     const int blocks[3] = {64, 128, 256};
     const int intervals[3] = {1, 4, 16};
+    // two pixel slots per thread only where the kernel has them (FP32, register contraction)
+    const int nrpt = (plan.precision == PRR_PREC_FP32 && ctx->geod_table != 1) ? 2 : 1;
+    for (int rpt = 1; rpt <= nrpt; rpt++)
     for (int bi = 0; bi < 3; bi++) {
-        int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi]);
+        int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi], rpt);
         if (occ < 1) continue;
         const int bpsms[2] = {occ, std::max(1, occ / 2)};
         for (int pi = 0; pi < (occ > 1 ? 2 : 1); pi++)
@@ -390,7 +394,7 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
                 ctx->cfg.block_size = blocks[bi];
                 ctx->cfg.blocks_per_sm = bpsms[pi];
                 ctx->cfg.compaction_interval = intervals[ii];
-                ctx->cfg.rays_per_thread = 1;
+                ctx->cfg.rays_per_thread = rpt;
                 float ms = 1e30f;
                 for (int rep = 0; rep < 2; rep++) {
                     s = run_plan(ctx, plan, nullptr, nullptr, ctx->stream, true);
