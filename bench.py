@@ -345,6 +345,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-trajectory", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--adjoint-size", type=int, default=512, help="side of the square differentiable-render frame")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--launch", default=None,
                     help="block,blocks_per_sm,compaction_interval,rays_per_thread for the persistent renderer "
@@ -443,7 +444,7 @@ def main():
         achieved = st.attempts * F_ATTEMPT / (st.trace_ms * 1e-3) / 1e12
         roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                     "frac": achieved / fp32_peak, "traffic": None,
-                    "kernel": "k_persistent<float,0,false>", "kernel_ms": st.trace_ms,
+                    "kernel": f"k_pair<{max(1, ctx.launch_config().rays_per_thread)}>", "kernel_ms": st.trace_ms,
                     "flop_per_attempt": F_ATTEMPT, "attempts": st.attempts,
                     "peak_source": "measured on this GPU: FMA-chain kernel (prr_measure_peak), burst",
                     "fp64_peak_tflops": fp64_peak}
@@ -477,8 +478,9 @@ def main():
             # discrete adjoint of the 512x512 differentiable-render workload: one gradient of an L2 image loss
             import ctypes as C
 
-            _, tgt, _ = ctx.render(scenes.kerr_512_adjoint(spin=0.7, precision=abi.PREC_FP64), want_float=True)
-            start = scenes.kerr_512_adjoint(spin=0.3, incl_deg=45.0, precision=abi.PREC_FP64)
+            n = args.adjoint_size
+            _, tgt, _ = ctx.render(scenes.kerr_512_adjoint(spin=0.7, precision=abi.PREC_FP64, size=n), want_float=True)
+            start = scenes.kerr_512_adjoint(spin=0.3, incl_deg=45.0, precision=abi.PREC_FP64, size=n)
             _, cur, _ = ctx.render(start, want_float=True)
             dl = np.ascontiguousarray(2.0 * (cur[0] - tgt[0]), dtype=np.float32)
             g = np.zeros(5, dtype=np.float64)
@@ -487,7 +489,7 @@ def main():
                 abi.check(abi.load().prr_adjoint(ctx.h, C.byref(start), dl.ctypes.data_as(abi._fp), 0,
                                                  g.ctypes.data_as(abi._dp), C.byref(ast)), ctx.h)
             extra["adjoint"] = {"ms": ast.kernel_ms, "fp64_forward_ms": ast.trace_ms, "unit": "ms",
-                                "workload": "kerr a=0.3 i=45 r=20, 512x512, 1 sphere, bilinear sky, FP64, tol 1e-6; "
+                                "workload": f"kerr a=0.3 i=45 r=20, {n}x{n}, 1 sphere, bilinear sky, FP64, tol 1e-6; "
                                             "d(L2 to the a=0.7 render)/d(a, M, i, r, phase)",
                                 "grad": g.tolist(), "accepted_steps": ast.accepted}
         if not args.no_trajectory and ws == 1:

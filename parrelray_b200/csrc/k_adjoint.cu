@@ -13,19 +13,19 @@
 //   3. reverse: for each segment, last first, the ADJ_K steps are recomputed
 //      from the checkpoint (bit-identical: same stepper) and lambda is pulled
 //      back through each step y_{n+1} = y_n + sum_i b_i k_i, k_i = h f(z_i),
-//      z_i = y_n + sum_j a_ij k_j (Fehlberg, 4th order); the stage Jacobians
-//      of the geodesic acceleration come from forward-mode dual numbers run
-//      through the same geod_ks template the renderer uses;
+//      z_i = y_n + sum_j a_ij k_j (Fehlberg, 4th order); the products
+//      lambda^T dG/dz of the geodesic acceleration come from its hand-written
+//      reverse sweep (geod_vjp.cuh);
 //   4. lambda_0 is pulled back through the initial data (camera position,
 //      ray direction, null u^t), also by dual numbers.
 // Gradients are accumulated per thread and reduced in FP64.
 #include "dual.cuh"
+#include "geod_vjp.cuh"
 #include "kernels.cuh"
 #include "phys_stepper.cuh"
 
 namespace prr {
 
-using DG = Dual<10>;  // stage Jacobians: 8 state components + spin + mass
 using DC = Dual<13>;  // initial data / colour: 8 state components + 5 parameters
 enum { P_SPIN = 0, P_MASS = 1, P_INCL = 2, P_CAMR = 3, P_PHASE = 4 };
 
@@ -95,23 +95,6 @@ __device__ void initial_state(const FrameParams &fp, const AdjParams &ap, float 
     }
 }
 
-// f(z) = (z_u, G(z_x, z_u)); returns G and fills J[4][10] = dG/d(z, spin, mass).
-__device__ void geod_jac(const Hot<double> &q, const double z[8], double G[4], double J[4][10])
-{
-    DG zz[8];
-    for (int c = 0; c < 8; c++) zz[c] = DG::var(z[c], c);
-    DG a = DG::var(q.a, 8), M = DG::var(q.M, 9);
-    V4<DG> x = {zz[0], zz[1], zz[2], zz[3]}, u = {zz[4], zz[5], zz[6], zz[7]};
-    V4<DG> g;
-    if (q.metric == PRR_METRIC_FLAT) g = {DG(0.0), DG(0.0), DG(0.0), DG(0.0)};
-    else g = geod_ks<DG, false>(x, u, M, a);
-    const DG *gg = &g.x;
-    for (int r = 0; r < 4; r++) {
-        G[r] = gg[r].v;
-        for (int c = 0; c < 10; c++) J[r][c] = gg[r].d[c];
-    }
-}
-
 __device__ void geod_val(const Hot<double> &q, const double z[8], double G[4])
 {
     if (q.metric == PRR_METRIC_FLAT) { G[0] = G[1] = G[2] = G[3] = 0.0; return; }
@@ -138,20 +121,19 @@ __device__ void step_vjp(const Hot<double> &q, const double y[8], double h, doub
     for (int i = 0; i < 6; i++)
         for (int c = 0; c < 8; c++) kb[i][c] = c_rkB[i] * lam[c];
     for (int i = 5; i >= 0; i--) {
-        double G[4], J[4][10], zb[8];
-        geod_jac(q, z[i], G, J);
-        // k_i = h (z_u, G(z)):  zb = h (d f/dz)^T kb_i
-        for (int c = 0; c < 8; c++) {
-            double s = 0.0;
-            for (int r = 0; r < 4; r++) s += J[r][c] * kb[i][4 + r];
-            zb[c] = h * s;
+        double zb[8];
+        // k_i = h (z_u, G(z)):  zb = h (d f/dz)^T kb_i, by the reverse sweep of the geodesic
+        if (q.metric == PRR_METRIC_FLAT) {
+            for (int c = 0; c < 8; c++) zb[c] = 0.0;
+        } else {
+            double gx[4], gu[4], gM, ga;
+            const double wv[4] = {kb[i][4], kb[i][5], kb[i][6], kb[i][7]};
+            geod_vjp({z[i][0], z[i][1], z[i][2], z[i][3]}, {z[i][4], z[i][5], z[i][6], z[i][7]}, q.M, q.a, wv, gx, gu, gM, ga);
+            for (int c = 0; c < 4; c++) { zb[c] = h * gx[c]; zb[4 + c] = h * gu[c]; }
+            th[0] += h * ga;
+            th[1] += h * gM;
         }
         for (int c = 0; c < 4; c++) zb[4 + c] += h * kb[i][c];
-        for (int p = 0; p < 2; p++) {
-            double s = 0.0;
-            for (int r = 0; r < 4; r++) s += J[r][8 + p] * kb[i][4 + r];
-            th[p] += h * s;
-        }
         for (int c = 0; c < 8; c++) yb[c] += zb[c];
         for (int j = 0; j < i; j++)
             for (int c = 0; c < 8; c++) kb[j][c] += c_rkA[i][j] * zb[c];

@@ -140,12 +140,17 @@ template <> __device__ __forceinline__ void load_in<float2>(pv::StageIn<float2> 
 
 }  // namespace
 
+// Launch bounds: at most PRR_PAIR_MAXT threads per CTA, at least
+// PRR_PAIR_MINB resident CTAs per SM (together they cap registers per thread).
+#ifndef PRR_PAIR_MAXT
+#define PRR_PAIR_MAXT 256
+#endif
 #ifndef PRR_PAIR_MINB
 #define PRR_PAIR_MINB 1
 #endif
 
 template <int RPT>
-__global__ void __launch_bounds__(256, PRR_PAIR_MINB) k_pair(PersistentArgs a)
+__global__ void __launch_bounds__(PRR_PAIR_MAXT, PRR_PAIR_MINB) k_pair(PersistentArgs a)
 {
     using V = typename std::conditional<RPT == 2, float2, float>::type;
     const int lane = threadIdx.x & 31;

@@ -144,11 +144,11 @@ def uneven_64(n: int = 64, seed: int = 4, max_pixels: int | None = None, **kw) -
 
 
 def kerr_512_adjoint(spin: float = 0.7, incl_deg: float = 60.0, r: float = 20.0, phase_deg: float = 30.0,
-                     **kw) -> abi.FrameDesc:
+                     size: int = 512, **kw) -> abi.FrameDesc:
     args = dict(r=r, incl_deg=incl_deg, fov_deg=40.0, metric=abi.METRIC_KERR, mass=1.0, spin=spin,
                 spheres=[(*orbit_point(9.0, phase_deg), 1.0, SPHERE_ID0)], bg_filter=abi.BG_BILINEAR)
     args.update(kw)
-    return make_frame(512, 512, **args)
+    return make_frame(size, size, **args)
 
 
 def make_texture(kind: int, seed: int, w: int, h: int) -> np.ndarray:
