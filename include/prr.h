@@ -218,8 +218,10 @@ prr_status prr_trace_rays_f64(prr_ctx *ctx, const prr_frame_desc *frame,
  * discrete events (accept/reject, termination, which sphere is hit) are
  * frozen at the forward run; the forward run and the adjoint are FP64, the
  * reduction is FP64.  The RMS2X2 sky is piecewise constant (zero gradient);
- * use PRR_BG_BILINEAR for sky gradients.  stats->kernel_ms is the adjoint
- * kernel time, stats->trace_ms the FP64 forward render time. */
+ * use PRR_BG_BILINEAR for sky gradients.  The rays are visited longest first
+ * (ordered by their forward step counts) so rays sharing a warp have similar
+ * lengths.  stats->kernel_ms is the device time of that ordering plus the
+ * adjoint kernel, stats->trace_ms the FP64 forward render time. */
 prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, const float *dL_dimage, int sphere_index,
                        double grads[5], prr_stats *stats);
 

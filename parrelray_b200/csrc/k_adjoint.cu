@@ -19,6 +19,8 @@
 //   4. lambda_0 is pulled back through the initial data (camera position,
 //      ray direction, null u^t), also by dual numbers.
 // Gradients are accumulated per thread and reduced in FP64.
+#include <cub/device/device_radix_sort.cuh>
+
 #include "dual.cuh"
 #include "geod_vjp.cuh"
 #include "kernels.cuh"
@@ -151,6 +153,7 @@ struct AdjointArgs {
     double *grad;              // 5 doubles, accumulated
     unsigned long long *counters;
     long long nrays;
+    const unsigned *order;     // ray visit order (null: 0, 1, 2, ...)
 };
 
 constexpr int ADJ_K = 64;
@@ -168,7 +171,8 @@ __global__ void __launch_bounds__(128) k_adjoint(AdjointArgs A)
     unsigned long long n_bad = 0, n_steps = 0;
     const int S = fp.samples;
     double ystore[ADJ_K][8], hstore[ADJ_K];
-    for (long long rid = tid; rid < A.nrays; rid += nth) {
+    for (long long k = tid; k < A.nrays; k += nth) {
+        const long long rid = A.order ? (long long)A.order[k] : k;
         long long pix = rid / S;
         int s = (int)(rid - pix * S);
         int px = (int)(pix % fp.width), py = (int)(pix / fp.width);
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(128) k_adjoint(AdjointArgs A)
 
 cudaError_t launch_adjoint(const FrameParams *d_fp, const AdjointParamsHost &p, const float *dL, const float *image,
                            void *ckpt, int max_ckpt, int threads_total, double *grad, unsigned long long *counters,
-                           long long nrays, cudaStream_t st)
+                           long long nrays, const unsigned *order, cudaStream_t st)
 {
     AdjointArgs A;
     A.frame = d_fp;
@@ -297,8 +301,42 @@ cudaError_t launch_adjoint(const FrameParams *d_fp, const AdjointParamsHost &p, 
     A.grad = grad;
     A.counters = counters;
     A.nrays = nrays;
+    A.order = order;
     k_adjoint<<<threads_total / 128, 128, 0, st>>>(A);
     return cudaGetLastError();
+}
+
+__global__ void k_iota(unsigned *v, long long n)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (unsigned)i;
+}
+
+// scratch layout: [iota values | sorted keys | cub temporary storage]
+size_t adjoint_order_bytes(long long nrays)
+{
+    size_t temp = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, temp, (const int *)nullptr, (int *)nullptr,
+                                              (const unsigned *)nullptr, (unsigned *)nullptr, (int)nrays);
+    const size_t n4 = ((size_t)nrays * 4 + 255) / 256 * 256;
+    return 2 * n4 + temp + 256;
+}
+
+cudaError_t launch_adjoint_order(const int *steps, long long nrays, unsigned *order, void *scratch, cudaStream_t st)
+{
+    if (nrays <= 0) return cudaSuccess;
+    const size_t n4 = ((size_t)nrays * 4 + 255) / 256 * 256;
+    unsigned *iota = (unsigned *)scratch;
+    int *keys_out = (int *)((char *)scratch + n4);
+    void *temp = (char *)scratch + 2 * n4;
+    k_iota<<<(unsigned)((nrays + 255) / 256), 256, 0, st>>>(iota, nrays);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t temp_bytes = 0;
+    e = cub::DeviceRadixSort::SortPairsDescending(nullptr, temp_bytes, steps, keys_out, iota, order, (int)nrays);
+    if (e != cudaSuccess) return e;
+    return cub::DeviceRadixSort::SortPairsDescending(temp, temp_bytes, steps, keys_out, iota, order, (int)nrays, 0,
+                                                     32, st);
 }
 
 size_t adjoint_checkpoint_bytes() { return sizeof(PhysRay<double>); }

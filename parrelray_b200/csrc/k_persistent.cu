@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
         } else {
             if (st == STEP_FLAG64) { result = PRR_RESULT_INFINITE_GEO; col = {0.f, 0.f, 0.f}; }
             cnt.add(result, result == PRR_RESULT_SUCCESS && metric_radius<T>(fp, R.x.x, R.x.y, R.x.z) >= q.rout);
+            if (a.ray_steps) a.ray_steps[fp.ray_begin + rid] = R.accepted;
             if (a.ray_state) write_state<T, float>(a.ray_state, rid, R, result, uv);
             if (a.ray_state64) write_state<T, double>(a.ray_state64, rid, R, result, uv);
             if (a.sample_rgb) {

@@ -56,6 +56,7 @@ struct PersistentArgs {
     int compaction_interval;     // attempts between warp refills (>= 1)
     long long watchdog_cycles;   // 0 = off
     int rays_per_thread;         // FP32: pixel slots in flight per thread (1 or 2; 0 = 1)
+    int *ray_steps;              // optional: accepted steps per ray (FP64/table/split kernels, single frame)
 };
 // Dispatches to the kernel of the precision: FP32 with the register
 // contraction -> k_pair (k_pair.cu, rays_per_thread slots per thread);
@@ -88,7 +89,13 @@ struct AdjointParamsHost {
 };
 cudaError_t launch_adjoint(const FrameParams *d_fp, const AdjointParamsHost &p, const float *dL, const float *image,
                            void *ckpt, int max_ckpt, int threads_total, double *grad, unsigned long long *counters,
-                           long long nrays, cudaStream_t st);
+                           long long nrays, const unsigned *order, cudaStream_t st);
+// k_adjoint.cu: ray order for the adjoint, longest first: `order` receives the
+// ray indices sorted by descending accepted-step count `steps` (nrays
+// entries), so the rays a warp processes together have similar lengths.
+// scratch: adjoint_order_bytes(nrays) bytes.
+size_t adjoint_order_bytes(long long nrays);
+cudaError_t launch_adjoint_order(const int *steps, long long nrays, unsigned *order, void *scratch, cudaStream_t st);
 size_t adjoint_checkpoint_bytes();
 constexpr int ADJ_CHECKPOINT_INTERVAL = 64;
 

@@ -43,15 +43,17 @@ struct prr_ctx {
     int geod_table = -1;  // -1: per schedule (PERSISTENT contraction, PLAIN table); 0: contraction; 1: table
     long long watchdog_cycles = 0;
     std::vector<MetricPlugin> plugins;
+    int *ray_steps_out = nullptr;  // set by prr_adjoint around its forward render: per-ray accepted steps
     int last_launches = 0;
     float last_ms = 0.f;
     float last_trace_ms = 0.f;
     // device scratch, grown on demand and reused across calls
-    DevBuf frames, frame_begin, counters, image, sample_rgb, rays, queue, state, out_u8, out_f, scratch, adj_ckpt, adj_dl;
+    DevBuf frames, frame_begin, counters, image, sample_rgb, rays, queue, state, out_u8, out_f, scratch, adj_ckpt, adj_dl,
+        adj_sort;
     std::vector<DevBuf *> all_buffers()
     {
         return {&frames, &frame_begin, &counters, &image, &sample_rgb, &rays, &queue, &state, &out_u8, &out_f, &scratch,
-                &adj_ckpt, &adj_dl};
+                &adj_ckpt, &adj_dl, &adj_sort};
     }
 };
 

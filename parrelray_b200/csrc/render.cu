@@ -177,6 +177,7 @@ static PersistentArgs persistent_args(prr_ctx *ctx, const RenderPlan &plan)
     a.compaction_interval = ctx->cfg.compaction_interval;
     a.watchdog_cycles = ctx->watchdog_cycles;
     a.rays_per_thread = ctx->cfg.rays_per_thread;
+    a.ray_steps = ctx->ray_steps_out;
     return a;
 }
 
@@ -437,14 +438,22 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
     prr_status s = build_plan(ctx, &f64, 1, plan);
     if (s != PRR_OK) return s;
     PRR_CK(ctx, cudaSetDevice(ctx->device));
+    const FrameParams &fp = plan.fp[0];
+    const long long npx = (long long)fp.width * fp.height, nrays = npx * fp.samples;
+    // per-ray step counts of the forward render order the adjoint's rays (longest first)
+    const size_t nr4 = ((size_t)nrays * sizeof(int) + 255) / 256 * 256;
+    if ((s = alloc(ctx, ctx->adj_sort, 2 * nr4 + adjoint_order_bytes(nrays), "adjoint ray order")) != PRR_OK) return s;
+    int *d_steps = (int *)ctx->adj_sort.p;
+    unsigned *d_order = (unsigned *)((char *)ctx->adj_sort.p + nr4);
+    void *d_sort_scratch = (char *)ctx->adj_sort.p + 2 * nr4;
     const int saved_sched = ctx->schedule;
     ctx->schedule = PRR_SCHED_PERSISTENT;
+    ctx->ray_steps_out = d_steps;
     s = run_plan(ctx, plan, nullptr, nullptr, ctx->stream, true);
+    ctx->ray_steps_out = nullptr;
     ctx->schedule = saved_sched;
     if (s != PRR_OK) return s;
     const float forward_ms = ctx->last_ms;
-    const FrameParams &fp = plan.fp[0];
-    const long long npx = (long long)fp.width * fp.height, nrays = npx * fp.samples;
     AdjointParamsHost ap{};
     ap.spin = fp.a; ap.mass = fp.M; ap.incl = incl; ap.cam_r = r; ap.sphere = sphere_index;
     if (sphere_index >= 0) {
@@ -464,8 +473,9 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
     PRR_CK(ctx, cudaMemsetAsync(d_grad, 0, 5 * sizeof(double), st));
     PRR_CK(ctx, cudaMemsetAsync(ctx->counters.p, 0, C_COUNT * sizeof(unsigned long long), st));
     PRR_CK(ctx, cudaEventRecord(ctx->e0, st));
+    PRR_CK(ctx, launch_adjoint_order(d_steps, nrays, d_order, d_sort_scratch, st));
     PRR_CK(ctx, launch_adjoint((const FrameParams *)ctx->frames.p, ap, d_dl, (const float *)ctx->image.p, ctx->adj_ckpt.p,
-                               max_ckpt, threads, d_grad, (unsigned long long *)ctx->counters.p, nrays, st));
+                               max_ckpt, threads, d_grad, (unsigned long long *)ctx->counters.p, nrays, d_order, st));
     PRR_CK(ctx, cudaEventRecord(ctx->e1, st));
     PRR_CK(ctx, cudaMemcpyAsync(grads, d_grad, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
     PRR_CK(ctx, cudaStreamSynchronize(st));
@@ -480,7 +490,7 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
         stats->n_math_error = (int64_t)c[C_MATH_ERROR];  // rays whose checkpoints did not fit
         stats->kernel_ms = adj_ms;
         stats->trace_ms = forward_ms;
-        stats->kernel_launches = ctx->last_launches + 1;
+        stats->kernel_launches = ctx->last_launches + 2;  // + the ray-order iota and the adjoint (the radix sort's own kernels not counted)
     }
     return PRR_OK;
 }
