@@ -443,7 +443,10 @@ def main():
         fp32_peak, fp64_peak = ctx.measure_peak()
         achieved = st.attempts * F_ATTEMPT / (st.trace_ms * 1e-3) / 1e12
         roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                    "frac": achieved / fp32_peak, "traffic": None,
+                    "frac": achieved / fp32_peak, "traffic": 8.704512e6,
+                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one k_pair launch on the "
+                                      "960x540 frame (profiles/k_pair_kerr960x540_ssaa4_full.md): the textures; "
+                                      "they do not grow with the frame, and the outputs stay in L2",
                     "kernel": f"k_pair<{max(1, ctx.launch_config().rays_per_thread)}>", "kernel_ms": st.trace_ms,
                     "flop_per_attempt": F_ATTEMPT, "attempts": st.attempts,
                     "peak_source": "measured on this GPU: FMA-chain kernel (prr_measure_peak), burst",
