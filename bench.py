@@ -53,6 +53,13 @@ FLOPS_GEOD_KERR = 168
 F_ATTEMPT = 6 * FLOPS_GEOD_KERR + FLOPS_STAGES
 
 
+def pair_kernel_name(cfg) -> str:
+    """The FP32 renderer instantiation a launch shape selects (k_pair.cu: launch_pair)."""
+    if cfg.rays_per_thread == 2:
+        return "k_pair<2,256,1>"
+    return "k_pair<1,64,8>" if cfg.block_size <= 64 else "k_pair<1,256,1>"
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -382,8 +389,9 @@ def main():
         tuned_on = "given on the command line"
     else:
         # the launch shape does not change the arithmetic of a ray; tune it on a smaller copy of the frame
-        ctx.autotune(build_frames(rank, ws, max(args.width // 4, 8), max(args.height // 4, 8)))
-        tuned_on = f"prr_autotune on the same frame at {max(args.width // 4, 8)}x{max(args.height // 4, 8)}"
+        tw, th = max(args.width // 2, 8), max(args.height // 2, 8)
+        ctx.autotune(build_frames(rank, ws, tw, th))
+        tuned_on = f"prr_autotune on the same frame at {tw}x{th}"
     t_tune = time.perf_counter() - t_tune
     out8 = torch.empty(npx * 3, dtype=torch.uint8, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
@@ -447,7 +455,7 @@ def main():
                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one k_pair launch on the "
                                       "960x540 frame (profiles/k_pair_kerr960x540_ssaa4_full.md): the textures; "
                                       "they do not grow with the frame, and the outputs stay in L2",
-                    "kernel": f"k_pair<{max(1, ctx.launch_config().rays_per_thread)}>", "kernel_ms": st.trace_ms,
+                    "kernel": pair_kernel_name(ctx.launch_config()), "kernel_ms": st.trace_ms,
                     "flop_per_attempt": F_ATTEMPT, "attempts": st.attempts,
                     "peak_source": "measured on this GPU: FMA-chain kernel (prr_measure_peak), burst",
                     "fp64_peak_tflops": fp64_peak}

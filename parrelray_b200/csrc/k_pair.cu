@@ -140,17 +140,19 @@ template <> __device__ __forceinline__ void load_in<float2>(pv::StageIn<float2> 
 
 }  // namespace
 
-// Launch bounds: at most PRR_PAIR_MAXT threads per CTA, at least
-// PRR_PAIR_MINB resident CTAs per SM (together they cap registers per thread).
-#ifndef PRR_PAIR_MAXT
-#define PRR_PAIR_MAXT 256
-#endif
-#ifndef PRR_PAIR_MINB
-#define PRR_PAIR_MINB 1
+// One-slot threads pair the components of their ray's 4-vectors on the
+// paired FP32 instructions (phys_pair.cuh: stages_xy) unless built with
+// PRR_PAIR_XY=0.
+#ifndef PRR_PAIR_XY
+#define PRR_PAIR_XY 1
 #endif
 
-template <int RPT>
-__global__ void __launch_bounds__(PRR_PAIR_MAXT, PRR_PAIR_MINB) k_pair(PersistentArgs a)
+// Launch bounds (MAXT threads per CTA at most, MINB resident CTAs per SM at
+// least) cap the registers per thread.  One-slot threads in CTAs of up to 64
+// threads use the instantiation capped at 127 registers (8 CTAs = 16 warps
+// per SM, no spills; 4 % faster than 141 registers and 12 warps).
+template <int RPT, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
 {
     using V = typename std::conditional<RPT == 2, float2, float>::type;
     const int lane = threadIdx.x & 31;
@@ -241,7 +243,13 @@ __global__ void __launch_bounds__(PRR_PAIR_MAXT, PRR_PAIR_MINB) k_pair(Persisten
         // ---- stages of every slot at once ----
         pv::StageIn<V> in;
         load_in<V>(in, sl);
+#if PRR_PAIR_XY
+        pv::StageOut<V> out;
+        if constexpr (RPT == 1) out = pv::stages_xy(in);
+        else out = pv::stages<V>(in);
+#else
         const pv::StageOut<V> out = pv::stages<V>(in);
+#endif
 
         // ---- accept/reject, hooks, colour (per slot) ----
 #pragma unroll
@@ -273,8 +281,9 @@ cudaError_t launch_pair(const PersistentArgs &a, int rpt, int block, int blocks_
     if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
     int grid = nsm * blocks_per_sm;
     if (grid < 1) grid = 1;
-    if (rpt == 2) k_pair<2><<<grid, block, 0, st>>>(a);
-    else if (rpt == 1) k_pair<1><<<grid, block, 0, st>>>(a);
+    if (rpt == 2) k_pair<2, 256, 1><<<grid, block, 0, st>>>(a);
+    else if (rpt == 1 && block <= 64) k_pair<1, 64, 8><<<grid, block, 0, st>>>(a);
+    else if (rpt == 1) k_pair<1, 256, 1><<<grid, block, 0, st>>>(a);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
@@ -282,8 +291,9 @@ cudaError_t launch_pair(const PersistentArgs &a, int rpt, int block, int blocks_
 int pair_occupancy(int rpt, int block)
 {
     int n = 0;
-    cudaError_t e = rpt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<2>, block, 0)
-                             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1>, block, 0);
+    cudaError_t e = rpt == 2     ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<2, 256, 1>, block, 0)
+                    : block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8>, block, 0)
+                                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1>, block, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
 }

@@ -190,6 +190,70 @@ template <class V> PRR_DEV StageOut<V> stages(const StageIn<V> &in)
     return o;
 }
 
+// One ray with its 4-vector components paired, (x, y) and (z, t), on the
+// paired instructions: the stage combinations, the increments and the error
+// estimate are component-wise, so half of their instructions go away; the
+// geodesic stays scalar (its operands mix components).  Same mathematics as
+// stages<float>; rounding differs in the last bits.
+PRR_DEV float2 f2(float a, float b) { return make_float2(a, b); }
+PRR_DEV float2 sp(float a) { return make_float2(a, a); }
+
+PRR_DEV StageOut<float> stages_xy(const StageIn<float> &in)
+{
+    using F = Fehlberg;
+    const float h = in.h;
+    const float2 H = sp(h);
+    const float2 x01 = f2(in.x.x, in.x.y), x23 = f2(in.x.z, in.x.w);
+    const float2 u01 = f2(in.u.x, in.u.y), u23 = f2(in.u.z, in.u.w);
+#define PC(v) sp((float)(v))
+    // k_i = h G(z_i), held as pairs
+#define GEOD(Kp, Kq, zx01, zx23, zu01, zu23)                                                                           {                                                                                                                      const Vec4<float> g = geod<float>({zx01.x, zx01.y, zx23.x, 0.0f}, {zu01.x, zu01.y, zu23.x, zu23.y}, in.M, in.a);         Kp = mul_(H, f2(g.x, g.y));                                                                                        Kq = mul_(H, f2(g.z, g.w));                                                                                    }
+    float2 k1p, k1q, k2p, k2q, k3p, k3q, k4p, k4q, k5p, k5q, k6p, k6q;
+    float2 zxp, zxq, zup, zuq;
+    GEOD(k1p, k1q, x01, x23, u01, u23)
+    zxp = fma_(H, mul_(PC(F::c2), u01), x01); zxq = fma_(H, mul_(PC(F::c2), u23), x23);
+    zup = fma_(PC(F::A21), k1p, u01); zuq = fma_(PC(F::A21), k1q, u23);
+    GEOD(k2p, k2q, zxp, zxq, zup, zuq)
+    zxp = fma_(H, fma_(PC(F::c3), u01, mul_(PC(F::B31), k1p)), x01);
+    zxq = fma_(H, fma_(PC(F::c3), u23, mul_(PC(F::B31), k1q)), x23);
+    zup = fma_(PC(F::A32), k2p, fma_(PC(F::A31), k1p, u01));
+    zuq = fma_(PC(F::A32), k2q, fma_(PC(F::A31), k1q, u23));
+    GEOD(k3p, k3q, zxp, zxq, zup, zuq)
+    zxp = fma_(H, fma_(PC(F::c4), u01, fma_(PC(F::B42), k2p, mul_(PC(F::B41), k1p))), x01);
+    zxq = fma_(H, fma_(PC(F::c4), u23, fma_(PC(F::B42), k2q, mul_(PC(F::B41), k1q))), x23);
+    zup = fma_(PC(F::A43), k3p, fma_(PC(F::A42), k2p, fma_(PC(F::A41), k1p, u01)));
+    zuq = fma_(PC(F::A43), k3q, fma_(PC(F::A42), k2q, fma_(PC(F::A41), k1q, u23)));
+    GEOD(k4p, k4q, zxp, zxq, zup, zuq)
+    zxp = fma_(H, fma_(PC(F::c5), u01, fma_(PC(F::B53), k3p, fma_(PC(F::B52), k2p, mul_(PC(F::B51), k1p)))), x01);
+    zxq = fma_(H, fma_(PC(F::c5), u23, fma_(PC(F::B53), k3q, fma_(PC(F::B52), k2q, mul_(PC(F::B51), k1q)))), x23);
+    zup = fma_(PC(F::A54), k4p, fma_(PC(F::A53), k3p, fma_(PC(F::A52), k2p, fma_(PC(F::A51), k1p, u01))));
+    zuq = fma_(PC(F::A54), k4q, fma_(PC(F::A53), k3q, fma_(PC(F::A52), k2q, fma_(PC(F::A51), k1q, u23))));
+    GEOD(k5p, k5q, zxp, zxq, zup, zuq)
+    zxp = fma_(H, fma_(PC(F::c6), u01, fma_(PC(F::B64), k4p, fma_(PC(F::B63), k3p, fma_(PC(F::B62), k2p,
+                                                                                       mul_(PC(F::B61), k1p))))), x01);
+    zxq = fma_(H, fma_(PC(F::c6), u23, fma_(PC(F::B64), k4q, fma_(PC(F::B63), k3q, fma_(PC(F::B62), k2q,
+                                                                                       mul_(PC(F::B61), k1q))))), x23);
+    zup = fma_(PC(F::A65), k5p, fma_(PC(F::A64), k4p, fma_(PC(F::A63), k3p, fma_(PC(F::A62), k2p,
+                                                                                fma_(PC(F::A61), k1p, u01)))));
+    zuq = fma_(PC(F::A65), k5q, fma_(PC(F::A64), k4q, fma_(PC(F::A63), k3q, fma_(PC(F::A62), k2q,
+                                                                                fma_(PC(F::A61), k1q, u23)))));
+    GEOD(k6p, k6q, zxp, zxq, zup, zuq)
+#undef GEOD
+    StageOut<float> o;
+    float2 err2 = sp(0.0f);
+    const float2 rtol = sp(in.rtol), atol = sp(in.atol);
+#define FIN(kk, xx, uu, j0)                                                                                            {                                                                                                                      const float2 du = fma_(PC(F::K45), k5##kk, fma_(PC(F::K44), k4##kk, fma_(PC(F::K43), k3##kk,                                                                                               mul_(PC(F::K41), k1##kk))));            const float2 dx = mul_(H, fma_(PC(F::b4), k4##kk, fma_(PC(F::b3), k3##kk, fma_(PC(F::b2), k2##kk,                                                                                          fma_(PC(F::b1), k1##kk, uu)))));         const float2 eu = fma_(PC(F::E6), k6##kk, fma_(PC(F::E5), k5##kk, fma_(PC(F::E4), k4##kk,                                                                                                fma_(PC(F::E3), k3##kk, mul_(PC(F::E1), k1##kk)))));         const float2 ex = mul_(H, fma_(PC(F::e5), k5##kk, fma_(PC(F::e4), k4##kk, fma_(PC(F::e3), k3##kk,                                                                                          fma_(PC(F::e2), k2##kk, mul_(PC(F::e1), k1##kk))))));         const float2 sx = fma_(rtol, max_(abs_(xx), abs_(add_(xx, dx))), atol);                                            const float2 su = fma_(rtol, max_(abs_(uu), abs_(add_(uu, du))), atol);                                            err2 = max_(err2, max_(mul_(abs_(ex), rcp_(sx)), mul_(abs_(eu), rcp_(su))));                                       o.dx[j0] = dx.x; o.dx[j0 + 1] = dx.y;                                                                              o.du[j0] = du.x; o.du[j0 + 1] = du.y;                                                                          }
+    FIN(p, x01, u01, 0)
+    FIN(q, x23, u23, 2)
+#undef FIN
+#undef PC
+    const float err = fmaxf(err2.x, err2.y);
+    o.err = err;
+    const float hn = mul_(mul_(0.9f, h), pow_(err, -0.2f));
+    o.hn = min_(max_(hn, in.hmin), in.hmax);
+    return o;
+}
+
 // Lane value of slot j (0 = x component, 1 = y) and back.
 PRR_DEV float get(float v, int) { return v; }
 PRR_DEV float get(float2 v, int j) { return j ? v.y : v.x; }

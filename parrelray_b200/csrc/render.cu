@@ -381,30 +381,30 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
     ctx->schedule = PRR_SCHED_PERSISTENT;
     prr_launch_config winner = saved;
     float best_ms = 1e30f;
+    // candidates: CTA size x refill interval x pixel slots per thread, each at the
+    // occupancy limit of its kernel; every candidate is timed three times (minimum kept)
     const int blocks[3] = {64, 128, 256};
-    const int intervals[3] = {1, 4, 16};
+    const int intervals[3] = {8, 16, 32};
     // two pixel slots per thread only where the kernel has them (FP32, register contraction)
     const int nrpt = (plan.precision == PRR_PREC_FP32 && ctx->geod_table != 1) ? 2 : 1;
     for (int rpt = 1; rpt <= nrpt; rpt++)
-    for (int bi = 0; bi < 3; bi++) {
-        int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi], rpt);
-        if (occ < 1) continue;
-        const int bpsms[2] = {occ, std::max(1, occ / 2)};
-        for (int pi = 0; pi < (occ > 1 ? 2 : 1); pi++)
+        for (int bi = 0; bi < 3; bi++) {
+            const int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi], rpt);
+            if (occ < 1) continue;
             for (int ii = 0; ii < 3; ii++) {
                 ctx->cfg.block_size = blocks[bi];
-                ctx->cfg.blocks_per_sm = bpsms[pi];
+                ctx->cfg.blocks_per_sm = occ;
                 ctx->cfg.compaction_interval = intervals[ii];
                 ctx->cfg.rays_per_thread = rpt;
                 float ms = 1e30f;
-                for (int rep = 0; rep < 2; rep++) {
+                for (int rep = 0; rep < 3; rep++) {
                     s = run_plan(ctx, plan, nullptr, nullptr, ctx->stream, true);
                     if (s != PRR_OK) { ctx->cfg = saved; ctx->schedule = saved_sched; return s; }
                     ms = std::min(ms, ctx->last_ms);
                 }
                 if (ms < best_ms) { best_ms = ms; winner = ctx->cfg; }
             }
-    }
+        }
     ctx->cfg = winner;
     ctx->schedule = saved_sched;
     if (best) *best = winner;
