@@ -1,6 +1,6 @@
 // geod_vjp.cuh - reverse-mode derivative (vector-Jacobian product) of the
-// Kerr-Schild geodesic acceleration geod_ks (prr_device.cuh, exact FP64
-// form): given weights w[4] on the outputs G = du/dlambda, returns
+// Kerr-Schild geodesic acceleration geod_ks (prr_device.cuh, the FP64 form
+// of the stepper): given weights w[4] on the outputs G = du/dlambda, returns
 //   gx[k] = sum_r w_r dG_r/dx_k, gu[k] = sum_r w_r dG_r/du_k (k = x, y, z, t),
 //   gM = sum_r w_r dG_r/dM,      ga = sum_r w_r dG_r/da.
 // The adjoint of one stage of the RKF45 step needs exactly this product; one
@@ -18,17 +18,17 @@ namespace prr {
 PRR_DEV void geod_vjp(const V4<double> &p, const V4<double> &u, double M, double a, const double w[4], double gx[4],
                       double gu[4], double &gM, double &ga)
 {
-    // ---- forward (as geod_ks<double, false>) ----
+    // ---- forward (as geod_ks<double, true>, the stepper's form) ----
     const double X = p.x, Y = p.y, Z = p.z;
     const double a2 = a * a;
     const double R2 = X * X + Y * Y + Z * Z;
     const double b = R2 - a2;
     const double S2 = b * b + 4.0 * a2 * Z * Z;
-    const double S = sqrt(S2), iS = 1.0 / S;
+    const double iS = frsqrt<double>(S2), S = S2 * iS;
     const double r2 = 0.5 * (b + S);
-    const double r = sqrt(r2), ir = 1.0 / r;
-    const double q = r2 + a2, iq = 1.0 / q;
-    const double Sig = r2 * r2 + a2 * Z * Z, iSig = 1.0 / Sig;
+    const double ir = frsqrt<double>(r2), r = r2 * ir;
+    const double q = r2 + a2, iq = frcp<double>(q);
+    const double Sig = r2 * r2 + a2 * Z * Z, iSig = frcp<double>(Sig);
     const double rS = r * iS;
     const double drx = X * rS, dry = Y * rS, drz = Z * q * iS * ir;
     const double f = 2.0 * M * r2 * r * iSig;

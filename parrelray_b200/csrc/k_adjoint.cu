@@ -100,7 +100,7 @@ __device__ void initial_state(const FrameParams &fp, const AdjParams &ap, float 
 __device__ void geod_val(const Hot<double> &q, const double z[8], double G[4])
 {
     if (q.metric == PRR_METRIC_FLAT) { G[0] = G[1] = G[2] = G[3] = 0.0; return; }
-    V4<double> g = geod_ks<double, false>({z[0], z[1], z[2], z[3]}, {z[4], z[5], z[6], z[7]}, q.M, q.a);
+    V4<double> g = geod_ks<double, true>({z[0], z[1], z[2], z[3]}, {z[4], z[5], z[6], z[7]}, q.M, q.a);
     G[0] = g.x; G[1] = g.y; G[2] = g.z; G[3] = g.w;
 }
 

@@ -31,11 +31,15 @@ template <class T> struct V4 { T x, y, z, w; };
 // Reciprocal, reciprocal square root and power for the PHYSICAL-mode hot
 // loop.  FP32 uses the SFU approximations (rcp.approx / rsqrt.approx /
 // lg2+ex2: a few ulp, far below the 1e-6 integration tolerance) instead of
-// the IEEE-rounded multi-instruction sequences; FP64 stays exact.
+// the IEEE-rounded multi-instruction sequences.  FP64 uses the correctly
+// rounded reciprocal (no general division) and CUDA's double rsqrt (within
+// an ulp) in place of a square root followed by a division.
 template <class T> PRR_DEV T frcp(T v) { return (T)1 / v; }
 template <> PRR_DEV float frcp<float>(float v) { return __fdividef(1.0f, v); }
+template <> PRR_DEV double frcp<double>(double v) { return __drcp_rn(v); }
 template <class T> PRR_DEV T frsqrt(T v) { return (T)1 / sqrt(v); }
 template <> PRR_DEV float frsqrt<float>(float v) { return rsqrtf(v); }
+template <> PRR_DEV double frsqrt<double>(double v) { return rsqrt(v); }
 template <class T> PRR_DEV T fpow(T b, T e) { return pow(b, e); }
 template <> PRR_DEV float fpow<float>(float b, float e) { return exp2f(e * __log2f(b)); }
 
