@@ -363,8 +363,11 @@ size_t prr_deck_sphere_texture(const prr_deck *d, int sphere, char *buf, size_t 
  * reference does (float(deg * M_PI / 180.0f)).  Texture ids: 0 = the sky
  * (tracer.bimage1), 1, 2, ... = distinct sphere textures in sphere order,
  * -1 = none.  Deck keys the reference lacks, all optional with defaults that
- * reproduce it: spacetime.metric (flat|schwarzschild|kerr; schwarzschild, as
- * main/metric.h:12 selects; no black hole = flat), tracer.mode
+ * reproduce it: spacetime.metric (flat|schwarzschild|kerr, or the path of a
+ * metric plug-in library "*.so", for which the descriptor's metric is
+ * PRR_METRIC_PLUGIN0 until the caller puts the id prr_load_metric_plugin
+ * returned - prr_run_deck does; schwarzschild by default, as main/metric.h:12
+ * selects; no black hole = flat), tracer.mode
  * (reference|physical), tracer.precision (fp32|fp64|split), tracer.rtol and
  * tracer.atol (eps), tracer.maxsteps (10000), tracer.horizon (0.001, as
  * metrics/schwarzschild.cuh:70), tracer.fxaa (0), tracer.bgfilter

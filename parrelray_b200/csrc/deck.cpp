@@ -12,8 +12,9 @@
 //                                              -> prr_run_deck
 //
 // Deck keys the reference does not have (all optional; defaults reproduce
-// the reference): spacetime.metric (flat | schwarzschild | kerr; default
-// schwarzschild, the header main/metric.h:12 selects), tracer.mode
+// the reference): spacetime.metric (flat | schwarzschild | kerr | the path of
+// a metric plug-in library; default schwarzschild, the header main/metric.h:12
+// selects), tracer.mode
 // (reference | physical), tracer.precision (fp32 | fp64 | split),
 // tracer.rtol / tracer.atol (default eps), tracer.maxsteps (10000),
 // tracer.horizon (stop at r <= r_+ + horizon; default 0.001 as
@@ -247,7 +248,9 @@ prr_status prr_deck_frame(const prr_deck *d, int frame, prr_frame_desc *out, cha
     else if (metric.empty() || metric == "schwarzschild") f.metric = PRR_METRIC_SCHWARZSCHILD;
     else if (metric == "kerr") f.metric = PRR_METRIC_KERR;
     else if (metric == "flat") f.metric = PRR_METRIC_FLAT;
-    else { put_err(errbuf, errlen, "unknown spacetime metric '" + metric + "' (flat, schwarzschild, kerr)"); return PRR_ERR_INVALID; }
+    else if (metric.size() > 3 && metric.compare(metric.size() - 3, 3, ".so") == 0)
+        f.metric = PRR_METRIC_PLUGIN0;  // a metric plug-in library: prr_run_deck loads it and sets the id
+    else { put_err(errbuf, errlen, "unknown spacetime metric '" + metric + "' (flat, schwarzschild, kerr, or a plug-in .so)"); return PRR_ERR_INVALID; }
     // ---- tracer (prr.cpp:184-190) ----
     std::string solver = par(d, "tracer", "solver");
     if (solver == "euler") f.solver = PRR_SOLVER_EULER;

@@ -74,6 +74,12 @@ extern "C" prr_status prr_run_deck(prr_ctx *ctx, const char *path, int first, in
         std::string t = deck_str(deck, ("sphere" + std::to_string(k)).c_str(), "tex");
         if ((s = upload_file(ctx, f0.spheres[k].texture_id, t)) != PRR_OK) return s;
     }
+    // a metric plug-in named by the deck (spacetime.metric = <library>.so) replaces main/metric.h's header
+    int plugin_metric = -1;
+    if (f0.metric == PRR_METRIC_PLUGIN0) {
+        const std::string lib = deck_str(deck, "spacetime", "metric");
+        if ((s = prr_load_metric_plugin(ctx, lib.c_str(), &plugin_metric)) != PRR_OK) return s;
+    }
     std::string prefix = out_prefix ? std::string(out_prefix) : deck_str(deck, "tracer", "out");
     prr_stats total;
     memset(&total, 0, sizeof(total));
@@ -85,6 +91,7 @@ extern "C" prr_status prr_run_deck(prr_ctx *ctx, const char *path, int first, in
         size_t npx = 0;
         for (int k = 0; k < nb; k++) {
             if ((s = prr_deck_frame(deck, f + k, &descs[k], err, sizeof(err))) != PRR_OK) return fail(ctx, s, err);
+            if (plugin_metric >= 0) descs[k].metric = plugin_metric;
             npx += (size_t)descs[k].width * (size_t)std::max(descs[k].height, 0);
         }
         rgb.resize(npx * 3);

@@ -183,6 +183,7 @@ def test_deck_options_and_unsupported_choices(built):
         abi.METRIC_KERR, abi.MODE_PHYSICAL, abi.PREC_SPLIT, 500, 1, abi.BG_BILINEAR)
     assert f.spin == np.float32(0.5) and f.rtol == np.float32(1e-7)
     assert frame(bh=0).metric == abi.METRIC_FLAT
+    assert frame(metric="<metric> = </opt/metrics/libmymetric.so>\n").metric == abi.METRIC_PLUGIN0
     assert frame(solver="nonsense").solver == abi.SOLVER_EULER       # Parameters::getSolver fallback
     assert frame(ssaa="nonsense").ssaa == abi.SSAA_REGULAR           # Parameters::getSSAA fallback
     for bad in (dict(solver="rk"), dict(ssaa="jittered")):

@@ -93,3 +93,28 @@ def test_run_deck_reports_missing_textures(gpu, tmp_path):
     with pytest.raises(abi.PrrError) as e:
         gpu.run_deck(bad, prefix=str(DECK_DIR) + "/")
     assert e.value.status == abi.ERR_IO and "sky.png" in str(e.value)
+
+
+def test_deck_names_a_metric_plugin(gpu, small_textures, deck_path):
+    """spacetime.metric = <a plug-in library>: the frames come from the plug-in's hooks (here the
+    reference's own Schwarzschild header compiled unchanged, or the shipped Kerr header at a = 0)."""
+    lib = LIB_PATH.parent / "libprr_metric_schwarzschild.so"
+    if not lib.exists():
+        lib = LIB_PATH.parent / "libprr_metric_kerr.so"
+    # a deck value must not contain '_' (it would open a block, main/io.h:30-36): link the library
+    link = deck_path.parent / "metricplugin.so"
+    if not link.exists():
+        link.symlink_to(lib)
+    text = deck_path.read_text().replace("_spacetime_\n", f"_spacetime_\n<metric> = <{link}>\n")
+    plugdeck = deck_path.parent / "plugin.params"
+    plugdeck.write_text(text)
+    out = deck_path.parent / "outplug"
+    out.mkdir(exist_ok=True)
+    gpu.run_deck(plugdeck, prefix=str(out) + "/", count=1)
+    d = Deck(plugdeck)
+    f = d.frame(0)
+    assert f.metric == abi.METRIC_PLUGIN0
+    mine = load_image(out / "image_0.png")[..., :3]
+    f.metric = abi.METRIC_SCHWARZSCHILD
+    ref = gpu.render(f)[0][0]
+    assert pixel_rule(mine, ref) >= 0.999
