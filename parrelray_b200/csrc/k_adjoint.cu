@@ -158,7 +158,12 @@ struct AdjointArgs {
 
 constexpr int ADJ_K = 64;
 
-__global__ void __launch_bounds__(128) k_adjoint(AdjointArgs A)
+// At least PRR_ADJ_MINB resident CTAs of 128 threads per SM (caps registers).
+#ifndef PRR_ADJ_MINB
+#define PRR_ADJ_MINB 1
+#endif
+
+__global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
 {
     const FrameParams &fp = *A.frame;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -340,5 +345,12 @@ cudaError_t launch_adjoint_order(const int *steps, long long nrays, unsigned *or
 }
 
 size_t adjoint_checkpoint_bytes() { return sizeof(PhysRay<double>); }
+
+int adjoint_blocks_per_sm()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint, 128, 0) != cudaSuccess) { cudaGetLastError(); return 1; }
+    return n > 0 ? n : 1;
+}
 
 }  // namespace prr

@@ -97,6 +97,7 @@ cudaError_t launch_adjoint(const FrameParams *d_fp, const AdjointParamsHost &p, 
 size_t adjoint_order_bytes(long long nrays);
 cudaError_t launch_adjoint_order(const int *steps, long long nrays, unsigned *order, void *scratch, cudaStream_t st);
 size_t adjoint_checkpoint_bytes();
+int adjoint_blocks_per_sm();  // resident 128-thread CTAs of k_adjoint per SM
 constexpr int ADJ_CHECKPOINT_INTERVAL = 64;
 
 // fma_peak.cu

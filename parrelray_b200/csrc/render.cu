@@ -462,7 +462,7 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
         ap.phase = std::atan2((double)S.center[1], (double)S.center[0]);
         ap.sph_z = S.center[2];
     }
-    const int threads = ctx->nsm * 2 * 128;
+    const int threads = ctx->nsm * adjoint_blocks_per_sm() * 128;  // one resident wave
     const int max_ckpt = d.max_steps / ADJ_CHECKPOINT_INTERVAL + 2;
     if ((s = alloc(ctx, ctx->adj_ckpt, (size_t)threads * max_ckpt * adjoint_checkpoint_bytes(), "adjoint checkpoints")) != PRR_OK) return s;
     if ((s = alloc(ctx, ctx->adj_dl, (size_t)npx * 3 * sizeof(float) + 8 * sizeof(double), "adjoint inputs")) != PRR_OK) return s;
