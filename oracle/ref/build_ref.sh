@@ -16,8 +16,9 @@
 #   2. prr.cpp - rewrite each `k<<<grid, block>>>(args);` launch as
 #      `prr_ref_launch(grid, block, [&]{ k(args); });` (host emulation).
 #   3. main/metric.h - the reference's compile-time metric selection point;
-#      replaced by a switch over PRR_REF_METRIC_{SCHW,FLAT,KERR}.  SCHW and
-#      FLAT select the reference's own headers; KERR selects the Kerr-Schild
+#      replaced by a switch over PRR_REF_METRIC_{SCHW,FLAT,CART,KERR}.  SCHW,
+#      FLAT and CART select the reference's own headers (CART: its alternative
+#      "schwarzschild - cart.cuh"); KERR selects the Kerr-Schild
 #      plug-in header shipped by this repository in the reference's plug-in
 #      shape (parrelray_b200/compat/metrics/kerr.cuh), since the reference's
 #      metrics/kerr.cuh is a stub whose hooks do not match the solver.
@@ -66,6 +67,8 @@ cat > "$OUT/src/main/metric.h" <<'EOF'
 #pragma once
 #if defined(PRR_REF_METRIC_FLAT)
 #include "../metrics/flat.cuh"
+#elif defined(PRR_REF_METRIC_CART)
+#include "../metrics/schwarzschild - cart.cuh"
 #elif defined(PRR_REF_METRIC_KERR)
 #include "../compat/kerr_plugin.cuh"
 #else
@@ -88,6 +91,9 @@ build_one() {
 build_one schw PRR_REF_METRIC_SCHW
 build_one flat PRR_REF_METRIC_FLAT
 build_one kerr PRR_REF_METRIC_KERR
+# the reference's alternative Cartesian Schwarzschild header (Christoffel tables;
+# not selected by the shipped main/metric.h)
+build_one cart PRR_REF_METRIC_CART
 echo "built: $(ls "$OUT"/libprr_ref_*.so | tr '\n' ' ')"
 # the patched source copy is only a build intermediate: keep just the libraries
 rm -rf "$OUT/src"

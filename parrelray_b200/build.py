@@ -134,14 +134,14 @@ def build_metric_plugin(header: Path, name: str | None = None, verbose: bool = F
 
 def build_plugins(verbose: bool = False) -> list[Path]:
     """The Kerr plug-in shipped in compat/metrics, and - where the reference
-    tree is mounted - the reference's own Schwarzschild and flat headers,
-    compiled unchanged."""
+    tree is mounted - the reference's own Schwarzschild and flat headers and
+    its alternative Cartesian Schwarzschild header, compiled unchanged."""
     outs = [build_metric_plugin(COMPAT / "metrics" / "kerr.cuh", "kerr", verbose)]
     ref = Path(os.environ.get("PRR_REFERENCE", "/root/reference"))
-    for stem in ("schwarzschild", "flat"):
+    for stem, name in (("schwarzschild", "schwarzschild"), ("flat", "flat"), ("schwarzschild - cart", "schwarzschildcart")):
         h = ref / "metrics" / f"{stem}.cuh"
         if h.exists():
-            outs.append(build_metric_plugin(h, stem, verbose))
+            outs.append(build_metric_plugin(h, name, verbose))
     return outs
 
 
@@ -167,7 +167,7 @@ def build_reference(verbose: bool = False) -> bool:
     if not (ref / "kernels" / "solver.cuh").exists():
         return False
     out = ORACLE_DIR / "_ref"
-    libs = [out / f"libprr_ref_{t}.so" for t in ("schw", "flat", "kerr")]
+    libs = [out / f"libprr_ref_{t}.so" for t in ("schw", "flat", "kerr", "cart")]
     deps = [ORACLE_DIR / "ref" / "build_ref.sh", ORACLE_DIR / "ref" / "ref_driver.cpp",
             PKG / "compat" / "metrics" / "kerr.cuh"] + sorted((ORACLE_DIR / "ref" / "shim").glob("*.h"))
     if all(_newer(l, deps) for l in libs):

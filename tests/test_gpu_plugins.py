@@ -95,3 +95,32 @@ def test_plugin_loading_rules(gpu, small_textures):
     with pytest.raises(abi.PrrError) as e:
         gpu.render(d)
     assert e.value.status == abi.ERR_INVALID
+
+
+def test_reference_alternative_cartesian_header(gpu, small_textures):
+    """The reference's alternative header metrics/"schwarzschild - cart.cuh" (Christoffel tables, not
+    selected by its main/metric.h), compiled unchanged as a plug-in, against the reference's own host
+    build with that header selected, live on the same deck (its rays end in MATH_ERROR at the first
+    step in the reference too: the plug-in reproduces the header as written)."""
+    from pathlib import Path
+
+    from oracles import RefHost, ref_available, write_deck
+    from parrelray_b200 import scenes
+
+    p = plugin_path("schwarzschildcart")
+    if not p.exists() or not ref_available("cart"):
+        pytest.skip("built only where the reference's headers are available")
+    sph = [(*scenes.orbit_point(10.0, 60.0), 1.5, scenes.SPHERE_ID0), (*scenes.orbit_point(12.0, 200.0), 2.0, 2)]
+    d = scenes.make_frame(64, 36, r=30.0, incl_deg=85.0, fov_deg=60.0, metric=abi.METRIC_SCHWARZSCHILD, mass=1.0,
+                          spheres=sph, mode=abi.MODE_REFERENCE, eps=1e-3, horizon_eps=0.001)
+    _, a_deg, b_deg = scenes.camera_pose(30.0, 85.0)
+    deck = write_deck(Path("/tmp/prrcartgpu"), d, small_textures, fov_deg=60.0, a_deg=a_deg, b_deg=b_deg)
+    ref = RefHost("cart")
+    assert ref.load(deck) == 1
+    z = ref.frame(0)
+    gpu.upload_textures(small_textures)
+    d.metric = gpu.load_metric_plugin(p)
+    state, rgb, _ = gpu.trace_rays(d)
+    assert np.mean(state[:, 2] == z["state"][:, 2]) >= 0.995
+    imgs, _, _ = gpu.render(d)
+    assert pixel_rule(imgs[0], quantize(z["image"])) >= 0.999
