@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PRR_ABI_VERSION 1
+#define PRR_ABI_VERSION 2
 #define PRR_MAX_SPHERES 8
 #define PRR_MAX_TEXTURES 32
 
@@ -54,8 +54,28 @@ typedef enum prr_result {
  * Only EULER and RKF45 are integrators in the reference (prr.cpp:295-305). */
 typedef enum prr_solver { PRR_SOLVER_EULER = 0, PRR_SOLVER_RKF45 = 2 } prr_solver;
 
-/* SSAA sample placement; same values as SSAA_DISTR (main/base.h:46-53). */
-typedef enum prr_ssaa { PRR_SSAA_NONE = 0, PRR_SSAA_REGULAR = 1 } prr_ssaa;
+/* SSAA sample placement; same values as SSAA_DISTR (main/base.h:46-53).
+ * NONE and REGULAR are createRays_none/_regular (kernels/ssaa.cuh:92-99,
+ * 36-48).  RANDOM (samples uniform in the pixel) and JITTERED (one sample
+ * uniform in each cell of an n x n grid, samples = n^2) exist in the
+ * reference only as kernels it never launches (ssaa.cuh:55-86, whose random
+ * offsets are not scaled to a pixel); here they are PHYSICAL-mode options
+ * with offsets from a counter-based hash of (ssaa_seed, pixel, sample), so a
+ * frame renders the same on every call. */
+typedef enum prr_ssaa { PRR_SSAA_NONE = 0, PRR_SSAA_REGULAR = 1, PRR_SSAA_RANDOM = 2, PRR_SSAA_JITTERED = 4 } prr_ssaa;
+
+/* Ray-direction model (main/Camera.h:30-42).  SPHERICAL is the one the
+ * reference's initRays uses (rayDir_Spherical); PINHOLE and PANORAMA are
+ * its other two models (rayDir_PinHole, rayDir_Panorama; never called by
+ * the reference), PHYSICAL mode only.  Both use the basis of
+ * Camera::computeVectors (main/Camera.cpp:19-28) evaluated at pitch -b,
+ * because computeVectors takes the pitch with the opposite sign from
+ * rayDir_Spherical: so all three models look the same way for one (a, b),
+ * and the image's left edge is on the same side.  PANORAMA is the
+ * equirectangular model sin(mu) up + cos(mu)(cos(nu) forward + sin(nu) right)
+ * with nu growing to the right; the reference's rayDir_Panorama multiplies
+ * its up term by mu as well and mirrors nu. */
+typedef enum prr_camera { PRR_CAMERA_SPHERICAL = 0, PRR_CAMERA_PINHOLE = 1, PRR_CAMERA_PANORAMA = 2 } prr_camera;
 
 typedef enum prr_metric {
     PRR_METRIC_FLAT = 0,          /* metrics/flat.cuh */
@@ -132,7 +152,9 @@ typedef struct prr_frame_desc {
     float fp64_delta;    /* SPLIT: flag rays with |b - b_c|/b_c < fp64_delta */
     float fp64_rfac;     /* SPLIT: flag rays reaching r < fp64_rfac * r_+ */
     int32_t nspheres;
-    int32_t _pad0;
+    int32_t camera;      /* prr_camera */
+    uint32_t ssaa_seed;  /* RANDOM / JITTERED sample offsets */
+    int32_t _pad1;
     prr_sphere spheres[PRR_MAX_SPHERES];
 } prr_frame_desc;
 
@@ -371,10 +393,12 @@ size_t prr_deck_sphere_texture(const prr_deck *d, int sphere, char *buf, size_t 
  * (reference|physical), tracer.precision (fp32|fp64|split), tracer.rtol and
  * tracer.atol (eps), tracer.maxsteps (10000), tracer.horizon (0.001, as
  * metrics/schwarzschild.cuh:70), tracer.fxaa (0), tracer.bgfilter
- * (rms2x2|bilinear).  Solvers rk/adams/gragg/dormand/taylor and SSAA
- * random/poisson/jittered/rotated have no implementation in the reference's
- * frame loop and return PRR_ERR_UNSUPPORTED; unknown names fall back to
- * euler and regular as Parameters::getSolver/getSSAA do. */
+ * (rms2x2|bilinear), camera.model (spherical|pinhole|panorama), camera.seed
+ * (RANDOM/JITTERED offsets).  SSAA random and jittered map to the PHYSICAL-
+ * mode placements of prr_ssaa.  Solvers rk/adams/gragg/dormand/taylor and
+ * SSAA poisson/rotated have no implementation (in the reference either) and
+ * return PRR_ERR_UNSUPPORTED; unknown names fall back to euler and regular
+ * as Parameters::getSolver/getSSAA do. */
 prr_status prr_deck_frame(const prr_deck *d, int frame, prr_frame_desc *out, char *errbuf, size_t errlen);
 
 /* The reference's main (prr.cpp:345-404): loads the deck at `path`, uploads

@@ -458,7 +458,26 @@ template <class T> struct RayState {
     unsigned long long cells = 0;  // texel cells read for the colour (finite-difference tests)
 };
 
-// createRays_none / createRays_regular
+// The stochastic placements' hash: the PCG output permutation of an LCG
+// step ("pcg_hash", Jarzynski & Olano, JCGT 2020), two 24-bit uniforms per
+// (seed, pixel, sample).
+inline uint32_t pcg_hash(uint32_t v)
+{
+    uint32_t state = v * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+
+inline void sample_offsets(uint32_t seed, long long p, int s, float &r0, float &r1)
+{
+    uint32_t h = pcg_hash(seed ^ pcg_hash((uint32_t)p ^ pcg_hash((uint32_t)(p >> 32) + 0x9e3779b9u * (uint32_t)(s + 1))));
+    uint32_t g = pcg_hash(h);
+    r0 = (float)(h >> 8) * (1.0f / 16777216.0f);
+    r1 = (float)(g >> 8) * (1.0f / 16777216.0f);
+}
+
+// createRays_none / createRays_regular (kernels/ssaa.cuh:92-99, 36-48); RANDOM
+// (uniform in the pixel) and JITTERED (uniform in each cell of an n x n grid).
 inline void ray_uv(const prr_frame_desc *d, long long rid, float &uvx, float &uvy)
 {
     int S = d->samples;
@@ -468,22 +487,70 @@ inline void ray_uv(const prr_frame_desc *d, long long rid, float &uvx, float &uv
     if (d->ssaa == PRR_SSAA_NONE) {
         uvx = (float)x / d->width + (1.0f / d->width) * 0.5f;
         uvy = (float)y / d->height + (1.0f / d->height) * 0.5f;
-    } else {
+    } else if (d->ssaa == PRR_SSAA_REGULAR) {
         int n = (int)roundf(sqrtf((float)S));
         float dux = (1.0f / d->width) / (n + 1.0f), duy = (1.0f / d->height) / (n + 1.0f);
         int i = s % n, j = s / n;
         uvx = (float)x / d->width + (float)(i + 1) * dux;
         uvy = (float)y / d->height + (float)(j + 1) * duy;
+    } else {
+        float r0, r1;
+        sample_offsets(d->ssaa_seed, pix, s, r0, r1);
+        if (d->ssaa == PRR_SSAA_JITTERED) {
+            const int n = (int)roundf(sqrtf((float)S));
+            r0 = ((float)(s % n) + r0) / (float)n;
+            r1 = ((float)(s / n) + r1) / (float)n;
+        }
+        uvx = ((float)x + r0) / (float)d->width;
+        uvy = ((float)y + r1) / (float)d->height;
     }
 }
 
-// Camera::rayDir_Spherical (main/Camera.h:39-42) in FP32.
+// Camera::computeVectors (main/Camera.cpp:19-28) in FP32.
+inline void camera_basis(float a, float b, float fwd[3], float right[3], float up[3])
+{
+    auto nrm = [](float v[3]) {
+        float k = 1.0f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        v[0] = k * v[0]; v[1] = k * v[1]; v[2] = k * v[2];
+    };
+    fwd[0] = cosf(b) * cosf(a); fwd[1] = cosf(b) * sinf(a); fwd[2] = -sinf(b);
+    nrm(fwd);
+    up[0] = cosf(a) * sinf(b); up[1] = sinf(a) * sinf(b); up[2] = cosf(b);
+    nrm(up);
+    right[0] = fwd[1] * up[2] - fwd[2] * up[1];
+    right[1] = fwd[2] * up[0] - fwd[0] * up[2];
+    right[2] = fwd[0] * up[1] - fwd[1] * up[0];
+    nrm(right);
+}
+
+// Camera::rayDir_Spherical (main/Camera.h:39-42) in FP32, rayDir_PinHole
+// (30-33) and the equirectangular panorama (34-37), the last two on the
+// basis oriented like the spherical model (see prr_camera).
 inline V3<float> ray_dir(const prr_frame_desc *d, float uvx, float uvy)
 {
-    float nu = (0.5f - uvy) * d->vfov;
-    float mu = (0.5f - uvx) * (float)d->width / (float)d->height * d->vfov;
-    float cb = cosf(d->cam_beta + nu);
-    V3<float> v = {cb * cosf(d->cam_alpha + mu), cb * sinf(d->cam_alpha + mu), sinf(d->cam_beta + nu)};
+    V3<float> v;
+    if (d->camera == PRR_CAMERA_SPHERICAL) {
+        float nu = (0.5f - uvy) * d->vfov;
+        float mu = (0.5f - uvx) * (float)d->width / (float)d->height * d->vfov;
+        float cb = cosf(d->cam_beta + nu);
+        v = {cb * cosf(d->cam_alpha + mu), cb * sinf(d->cam_alpha + mu), sinf(d->cam_beta + nu)};
+    } else {
+        float f[3], r[3], u[3];
+        camera_basis(d->cam_alpha, -d->cam_beta, f, r, u);  // pitch sign: see the renderer's basis
+        float a, b, c;
+        if (d->camera == PRR_CAMERA_PINHOLE) {
+            const float t = tanf(d->vfov / 2.0f);
+            a = 1.0f;
+            b = (2.0f * uvx - 1.0f) * t * (float)d->width / (float)d->height;
+            c = (1.0f - 2.0f * uvy) * t;
+        } else {
+            const float mu = (0.5f - uvy) * d->vfov;
+            const float nu = (uvx - 0.5f) * (float)d->width / (float)d->height * d->vfov;
+            const float cm = cosf(mu);
+            a = cm * cosf(nu); b = cm * sinf(nu); c = sinf(mu);
+        }
+        v = {a * f[0] + b * r[0] + c * u[0], a * f[1] + b * r[1] + c * u[1], a * f[2] + b * r[2] + c * u[2]};
+    }
     float k = 1.0f / sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
     return {v.x * k, v.y * k, v.z * k};
 }
@@ -877,7 +944,7 @@ int prr_oracle_trace(const prr_frame_desc *d, const uint8_t *const *tex, const i
                      int precision, const long long *ids, long long n, int nthreads, double *state, float *rgb)
 {
     if (!d || n < 0) return 1;
-    if (d->ssaa == PRR_SSAA_REGULAR) {
+    if (d->ssaa == PRR_SSAA_REGULAR || d->ssaa == PRR_SSAA_JITTERED) {
         int q = (int)roundf(sqrtf((float)d->samples));
         if (q * q != d->samples) return 1;
     }

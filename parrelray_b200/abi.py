@@ -23,7 +23,8 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_TIMEOUT, ERR_IO, ERR_UNSUPPORTED, ERR_
 # prr_result (main/base.h:37-43)
 RESULT_SUCCESS, RESULT_MATH_ERROR, RESULT_IO_ERROR, RESULT_INFINITE_GEO, RESULT_INTERSECTION = range(5)
 SOLVER_EULER, SOLVER_RKF45 = 0, 2
-SSAA_NONE, SSAA_REGULAR = 0, 1
+SSAA_NONE, SSAA_REGULAR, SSAA_RANDOM, SSAA_JITTERED = 0, 1, 2, 4
+CAMERA_SPHERICAL, CAMERA_PINHOLE, CAMERA_PANORAMA = 0, 1, 2
 METRIC_FLAT, METRIC_SCHWARZSCHILD, METRIC_KERR = 0, 1, 2
 METRIC_PLUGIN0 = 16
 MODE_REFERENCE, MODE_PHYSICAL = 0, 1
@@ -47,7 +48,7 @@ class FrameDesc(C.Structure):
         ("rtol", C.c_float), ("atol", C.c_float), ("rout", C.c_float), ("horizon_eps", C.c_float),
         ("max_steps", C.c_int32), ("background_id", C.c_int32), ("bg_filter", C.c_int32), ("fxaa", C.c_int32),
         ("fp64_delta", C.c_float), ("fp64_rfac", C.c_float),
-        ("nspheres", C.c_int32), ("_pad0", C.c_int32),
+        ("nspheres", C.c_int32), ("camera", C.c_int32), ("ssaa_seed", C.c_uint32), ("_pad1", C.c_int32),
         ("spheres", Sphere * PRR_MAX_SPHERES),
     ]
 

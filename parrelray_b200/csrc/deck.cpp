@@ -16,6 +16,8 @@
 // a metric plug-in library; default schwarzschild, the header main/metric.h:12
 // selects), tracer.mode
 // (reference | physical), tracer.precision (fp32 | fp64 | split),
+// camera.model (spherical | pinhole | panorama), camera.seed (random /
+// jittered SSAA),
 // tracer.rtol / tracer.atol (default eps), tracer.maxsteps (10000),
 // tracer.horizon (stop at r <= r_+ + horizon; default 0.001 as
 // metrics/schwarzschild.cuh:70), tracer.fxaa (0/1), tracer.bgfilter
@@ -287,10 +289,18 @@ prr_status prr_deck_frame(const prr_deck *d, int frame, prr_frame_desc *out, cha
     std::string ssaa = par(d, "camera", "SSAA");
     if (ssaa == "none") f.ssaa = PRR_SSAA_NONE;
     else if (ssaa == "regular") f.ssaa = PRR_SSAA_REGULAR;
-    else if (ssaa == "random" || ssaa == "poisson" || ssaa == "jittered" || ssaa == "rotated") {
-        put_err(errbuf, errlen, "SSAA distribution '" + ssaa + "' places no rays in the reference (prr.cpp:261-273)");
+    else if (ssaa == "random") f.ssaa = PRR_SSAA_RANDOM;      // PHYSICAL mode (the reference never launches its kernel)
+    else if (ssaa == "jittered") f.ssaa = PRR_SSAA_JITTERED;  // likewise
+    else if (ssaa == "poisson" || ssaa == "rotated") {
+        put_err(errbuf, errlen, "SSAA distribution '" + ssaa + "' has no implementation (none in the reference either)");
         return PRR_ERR_UNSUPPORTED;
     } else f.ssaa = PRR_SSAA_REGULAR;  // Parameters::getSSAA's fallback (main/Parameters.h:24-29)
+    f.ssaa_seed = (uint32_t)pari(d, "camera", "seed");
+    std::string model = par(d, "camera", "model");
+    if (model.empty() || model == "spherical") f.camera = PRR_CAMERA_SPHERICAL;
+    else if (model == "pinhole") f.camera = PRR_CAMERA_PINHOLE;
+    else if (model == "panorama") f.camera = PRR_CAMERA_PANORAMA;
+    else { put_err(errbuf, errlen, "unknown camera model '" + model + "' (spherical, pinhole, panorama)"); return PRR_ERR_INVALID; }
     f.samples = pari(d, "camera", "SSAAsamples");
     f.vfov = deg2rad(parf(d, "camera", "vfov"));
     f.width = pari(d, "camera", "width");

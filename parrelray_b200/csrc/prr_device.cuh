@@ -114,6 +114,10 @@ struct FrameParams {
     DevTex bg;      // bg.p == nullptr: black sky
     float fp64_delta, fp64_rfac;
     int nspheres;
+    int camera;           // prr_camera
+    unsigned ssaa_seed;   // RANDOM / JITTERED offsets
+    float cfwd[3], cright[3], cup[3];  // Camera::computeVectors basis (PINHOLE, PANORAMA)
+    float tan_half;       // tanf(vfov / 2) (PINHOLE)
     DevSphere sph[PRR_MAX_SPHERES];
     long long ray_begin;  // first ray (work) index of this frame in a batch
     long long pix_begin;  // first output pixel of this frame in a batch
@@ -121,28 +125,74 @@ struct FrameParams {
 
 // ------------------------------------------------------------- camera / rays
 
-// Sub-pixel position of ray `s` of pixel (x, y) (createRays_none/regular).
+// Counter-based hash for stochastic sample placement: the PCG output
+// permutation applied to an LCG step of the input ("pcg_hash", Jarzynski &
+// Olano, "Hash Functions for GPU Rendering", JCGT 2020).
+PRR_HD uint32_t pcg_hash(uint32_t v)
+{
+    uint32_t state = v * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+
+// Two uniforms in [0, 1) for sample s of pixel p (24-bit mantissas).
+PRR_HD void sample_offsets(uint32_t seed, long long p, int s, float &r0, float &r1)
+{
+    uint32_t h = pcg_hash(seed ^ pcg_hash((uint32_t)p ^ pcg_hash((uint32_t)(p >> 32) + 0x9e3779b9u * (uint32_t)(s + 1))));
+    uint32_t g = pcg_hash(h);
+    r0 = (float)(h >> 8) * (1.0f / 16777216.0f);
+    r1 = (float)(g >> 8) * (1.0f / 16777216.0f);
+}
+
+// Sub-pixel position of ray `s` of pixel (x, y): createRays_none/regular
+// (kernels/ssaa.cuh:92-99, 36-48), and the RANDOM / JITTERED placements.
 PRR_DEV void ray_uv(const FrameParams &fp, int x, int y, int s, float &uvx, float &uvy)
 {
     if (fp.ssaa == PRR_SSAA_NONE) {
         uvx = (float)x / fp.width + (1.0f / fp.width) * 0.5f;
         uvy = (float)y / fp.height + (1.0f / fp.height) * 0.5f;
-    } else {
+    } else if (fp.ssaa == PRR_SSAA_REGULAR) {
         int n = fp.nsub;
         float dux = (1.0f / fp.width) / (n + 1.0f), duy = (1.0f / fp.height) / (n + 1.0f);
         int i = s % n, j = s / n;
         uvx = (float)x / fp.width + (float)(i + 1) * dux;
         uvy = (float)y / fp.height + (float)(j + 1) * duy;
+    } else {
+        float r0, r1;
+        sample_offsets(fp.ssaa_seed, (long long)y * fp.width + x, s, r0, r1);
+        if (fp.ssaa == PRR_SSAA_JITTERED) {
+            const int n = fp.nsub;
+            r0 = ((float)(s % n) + r0) / (float)n;
+            r1 = ((float)(s / n) + r1) / (float)n;
+        }
+        uvx = ((float)x + r0) / (float)fp.width;
+        uvy = ((float)y + r1) / (float)fp.height;
     }
 }
 
-// Camera::rayDir_Spherical, FP32 as in the reference.
+// Ray direction for the screen position (uvx, uvy): Camera::rayDir_Spherical
+// (main/Camera.h:39-42, FP32 as in the reference), rayDir_PinHole (30-33) and
+// the equirectangular panorama (34-37, see prr_camera).
 PRR_DEV V3<float> ray_dir(const FrameParams &fp, float uvx, float uvy)
 {
-    float nu = (0.5f - uvy) * fp.vfov;
-    float mu = (0.5f - uvx) * (float)fp.width / (float)fp.height * fp.vfov;
-    float cb = cosf(fp.beta + nu);
-    V3<float> v = {cb * cosf(fp.alpha + mu), cb * sinf(fp.alpha + mu), sinf(fp.beta + nu)};
+    V3<float> v;
+    if (fp.camera == PRR_CAMERA_PINHOLE) {
+        const float sx = (2.0f * uvx - 1.0f) * fp.tan_half * (float)fp.width / (float)fp.height;
+        const float sy = (1.0f - 2.0f * uvy) * fp.tan_half;
+        v = {fp.cfwd[0] + sx * fp.cright[0] + sy * fp.cup[0], fp.cfwd[1] + sx * fp.cright[1] + sy * fp.cup[1],
+             fp.cfwd[2] + sx * fp.cright[2] + sy * fp.cup[2]};
+    } else if (fp.camera == PRR_CAMERA_PANORAMA) {
+        const float mu = (0.5f - uvy) * fp.vfov;
+        const float nu = (uvx - 0.5f) * (float)fp.width / (float)fp.height * fp.vfov;
+        const float cm = cosf(mu), a = cm * cosf(nu), b = cm * sinf(nu), c = sinf(mu);
+        v = {a * fp.cfwd[0] + b * fp.cright[0] + c * fp.cup[0], a * fp.cfwd[1] + b * fp.cright[1] + c * fp.cup[1],
+             a * fp.cfwd[2] + b * fp.cright[2] + c * fp.cup[2]};
+    } else {
+        float nu = (0.5f - uvy) * fp.vfov;
+        float mu = (0.5f - uvx) * (float)fp.width / (float)fp.height * fp.vfov;
+        float cb = cosf(fp.beta + nu);
+        v = {cb * cosf(fp.alpha + mu), cb * sinf(fp.alpha + mu), sinf(fp.beta + nu)};
+    }
     float k = 1.0f / sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
     return {v.x * k, v.y * k, v.z * k};
 }

@@ -51,6 +51,24 @@ prr_status alloc(prr_ctx *ctx, DevBuf &b, size_t bytes, const char *what)
     return PRR_OK;
 }
 
+// Camera::computeVectors (main/Camera.cpp:19-28) in FP32: forward, up and
+// right = forward x up, each normalised as cudamaths' normalize does.
+void camera_basis(float a, float b, float fwd[3], float right[3], float up[3])
+{
+    auto nrm = [](float v[3]) {
+        float k = 1.0f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        v[0] = k * v[0]; v[1] = k * v[1]; v[2] = k * v[2];
+    };
+    fwd[0] = cosf(b) * cosf(a); fwd[1] = cosf(b) * sinf(a); fwd[2] = -sinf(b);
+    nrm(fwd);
+    up[0] = cosf(a) * sinf(b); up[1] = sinf(a) * sinf(b); up[2] = cosf(b);
+    nrm(up);
+    right[0] = fwd[1] * up[2] - fwd[2] * up[1];
+    right[1] = fwd[2] * up[0] - fwd[0] * up[2];
+    right[2] = fwd[0] * up[1] - fwd[1] * up[0];
+    nrm(right);
+}
+
 }  // namespace
 
 int resolve_bpsm(prr_ctx *ctx, int precision)
@@ -79,11 +97,17 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
         if (d.ssaa == PRR_SSAA_NONE) {
             if (d.samples != 1) return bad(ctx, f, "SSAA none needs samples == 1");
             p.nsub = 1;
-        } else if (d.ssaa == PRR_SSAA_REGULAR) {
+        } else if (d.ssaa == PRR_SSAA_REGULAR || d.ssaa == PRR_SSAA_JITTERED) {
             int q = (int)std::lround(std::sqrt((double)d.samples));
-            if (q * q != d.samples) return bad(ctx, f, "SSAA regular needs a perfect-square sample count (kernels/ssaa.cuh:41)");
+            if (q * q != d.samples) return bad(ctx, f, "SSAA regular/jittered needs a perfect-square sample count (kernels/ssaa.cuh:41)");
             p.nsub = q;
-        } else return bad(ctx, f, "unknown SSAA distribution (only none and regular are implemented, as in prr.cpp:261-273)");
+        } else if (d.ssaa == PRR_SSAA_RANDOM) {
+            p.nsub = 1;
+        } else return bad(ctx, f, "unknown SSAA distribution (none, regular, random, jittered)");
+        if (d.camera < PRR_CAMERA_SPHERICAL || d.camera > PRR_CAMERA_PANORAMA) return bad(ctx, f, "unknown camera model");
+        if (d.mode == PRR_MODE_REFERENCE &&
+            (d.camera != PRR_CAMERA_SPHERICAL || (d.ssaa != PRR_SSAA_NONE && d.ssaa != PRR_SSAA_REGULAR)))
+            return bad(ctx, f, "REFERENCE mode places rays as the reference does: spherical camera, SSAA none or regular");
         if (!finite_pos(d.vfov) || d.vfov >= 6.3f) return bad(ctx, f, "vfov must be in (0, 2*pi) radians");
         for (int k = 0; k < 3; k++) if (!std::isfinite(d.cam_pos[k])) return bad(ctx, f, "camera position is not finite");
         if (!std::isfinite(d.cam_alpha) || !std::isfinite(d.cam_beta)) return bad(ctx, f, "camera angles are not finite");
@@ -123,6 +147,12 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
         p.width = d.width; p.height = d.height; p.samples = d.samples; p.ssaa = d.ssaa;
         p.vfov = d.vfov; p.cam[0] = d.cam_pos[0]; p.cam[1] = d.cam_pos[1]; p.cam[2] = d.cam_pos[2];
         p.alpha = d.cam_alpha; p.beta = d.cam_beta;
+        p.camera = d.camera;
+        p.ssaa_seed = d.ssaa_seed;
+        // computeVectors takes the pitch with the opposite sign from rayDir_Spherical: evaluate it at -b
+        // so every model's centre ray is the spherical model's
+        camera_basis(d.cam_alpha, -d.cam_beta, p.cfwd, p.cright, p.cup);
+        p.tan_half = tanf(d.vfov / 2.0f);
         p.metric = d.metric; p.M = d.mass; p.a = (d.metric == PRR_METRIC_KERR || plugin) ? d.spin : 0.0f;
         p.rs = 2.0f * d.mass;  // Spacetime::setBhMass (main/Spacetime.h:23)
         float rplus = d.metric == PRR_METRIC_KERR ? kerr_r_plus<float>(d.mass, d.spin) : (d.metric == PRR_METRIC_FLAT ? 0.0f : p.rs);
@@ -423,6 +453,7 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
     if (d.mode != PRR_MODE_PHYSICAL || d.solver != PRR_SOLVER_RKF45) { ctx->err = "prr_adjoint: PHYSICAL mode RKF45 frames only"; return PRR_ERR_INVALID; }
     if (d.fxaa) { ctx->err = "prr_adjoint: FXAA is not differentiated; render the frame without FXAA"; return PRR_ERR_UNSUPPORTED; }
     if (sphere_index < -1 || sphere_index >= d.nspheres) { ctx->err = "prr_adjoint: sphere_index out of range"; return PRR_ERR_INVALID; }
+    if (d.camera != PRR_CAMERA_SPHERICAL) { ctx->err = "prr_adjoint: differentiates the spherical camera model only"; return PRR_ERR_UNSUPPORTED; }
     // orbit camera: position (r sin i, 0, r cos i), yaw pi, pitch i - pi/2
     double px = d.cam_pos[0], py = d.cam_pos[1], pz = d.cam_pos[2];
     double r = std::sqrt(px * px + py * py + pz * pz);

@@ -27,7 +27,7 @@ def test_struct_layouts_match(built):
 
 def test_version_and_status_strings(built):
     lib = abi.load()
-    assert lib.prr_abi_version() == 1
+    assert lib.prr_abi_version() == 2
     assert lib.prr_status_string(abi.OK) == b"ok"
     assert b"device" in lib.prr_status_string(abi.ERR_NO_DEVICE)
 

@@ -186,7 +186,9 @@ def test_deck_options_and_unsupported_choices(built):
     assert frame(metric="<metric> = </opt/metrics/libmymetric.so>\n").metric == abi.METRIC_PLUGIN0
     assert frame(solver="nonsense").solver == abi.SOLVER_EULER       # Parameters::getSolver fallback
     assert frame(ssaa="nonsense").ssaa == abi.SSAA_REGULAR           # Parameters::getSSAA fallback
-    for bad in (dict(solver="rk"), dict(ssaa="jittered")):
+    assert frame(ssaa="jittered").ssaa == abi.SSAA_JITTERED and frame(ssaa="random").ssaa == abi.SSAA_RANDOM
+    assert frame(extra="").camera == abi.CAMERA_SPHERICAL
+    for bad in (dict(solver="rk"), dict(ssaa="poisson")):
         with pytest.raises(PrrError) as e:
             frame(**bad)
         assert e.value.status == abi.ERR_UNSUPPORTED

@@ -169,3 +169,57 @@ def test_kerr_conserved_quantities(oracle, spin):
         assert abs(n0) < 1e-9 * c0[0] ** 2 and abs(n1) < 1e-6 * c0[0] ** 2
         n_checked += 1
     assert n_checked > 50
+
+
+def test_stochastic_placements_and_camera_models(oracle, small_textures):
+    """RANDOM samples fall inside their pixel, JITTERED ones inside their cell of the n x n grid,
+    both change with the seed and repeat with it; the pinhole camera looks along its forward
+    vector at the image centre, and the panorama and spherical models agree there."""
+    W, H = 6, 4
+    for ssaa, S in ((abi.SSAA_RANDOM, 5), (abi.SSAA_JITTERED, 4)):
+        d = scenes.make_frame(W, H, r=30.0, incl_deg=80.0, fov_deg=50.0, metric=abi.METRIC_FLAT, mass=0.0,
+                              samples=S, background=False)
+        d.ssaa, d.ssaa_seed = ssaa, 99
+        st, _ = oracle.trace(d, small_textures, precision=1)
+        uv = st[:, :2].reshape(H, W, S, 2)
+        px = uv[..., 0] * W - np.arange(W)[None, :, None]
+        py = uv[..., 1] * H - np.arange(H)[:, None, None]
+        assert np.all((px >= 0) & (px < 1 + 1e-6) & (py >= 0) & (py < 1 + 1e-6))
+        if ssaa == abi.SSAA_JITTERED:
+            n = 2
+            i = np.arange(S) % n
+            j = np.arange(S) // n
+            assert np.all((np.floor(px * n) == i) | np.isclose(px * n, i + 1))
+            assert np.all((np.floor(py * n) == j) | np.isclose(py * n, j + 1))
+        again, _ = oracle.trace(d, small_textures, precision=1)
+        assert np.array_equal(again[:, :2], st[:, :2])
+        d.ssaa_seed = 100
+        other, _ = oracle.trace(d, small_textures, precision=1)
+        assert not np.array_equal(other[:, :2], st[:, :2])
+    # image centre: pinhole and panorama look along forward = the spherical model's centre ray
+    dirs = {}
+    for cam in (abi.CAMERA_SPHERICAL, abi.CAMERA_PINHOLE, abi.CAMERA_PANORAMA):
+        d = scenes.make_frame(1, 1, r=30.0, incl_deg=80.0, fov_deg=50.0, metric=abi.METRIC_FLAT, mass=0.0,
+                              background=False, rout=1e4)
+        d.camera = cam
+        st, _ = oracle.trace(d, small_textures, precision=1)
+        u = st[0, 7:10]
+        dirs[cam] = u / np.linalg.norm(u)
+    assert np.allclose(dirs[abi.CAMERA_PINHOLE], dirs[abi.CAMERA_SPHERICAL], atol=1e-6)
+    assert np.allclose(dirs[abi.CAMERA_PANORAMA], dirs[abi.CAMERA_SPHERICAL], atol=1e-6)
+
+
+def test_camera_models_share_orientation(oracle, small_textures):
+    """For one (a, b) the three models map every screen position to nearby directions: no model is
+    mirrored or tilted the other way (a mirror would put the corners ~0.8 rad apart at FOV 50)."""
+    dirs = {}
+    for cam in (abi.CAMERA_SPHERICAL, abi.CAMERA_PINHOLE, abi.CAMERA_PANORAMA):
+        d = scenes.make_frame(3, 3, r=30.0, incl_deg=80.0, fov_deg=50.0, metric=abi.METRIC_FLAT, mass=0.0,
+                              background=False, rout=1e4)
+        d.camera = cam
+        st, _ = oracle.trace(d, small_textures, precision=1)
+        u = st[:, 7:10]
+        dirs[cam] = u / np.linalg.norm(u, axis=1, keepdims=True)
+    for cam in (abi.CAMERA_PINHOLE, abi.CAMERA_PANORAMA):
+        ang = np.arccos(np.clip(np.sum(dirs[cam] * dirs[abi.CAMERA_SPHERICAL], axis=1), -1, 1))
+        assert ang.max() < 0.15, (cam, ang)
