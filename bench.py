@@ -316,7 +316,7 @@ def smooth_sky(w: int = 512, h: int = 256) -> np.ndarray:
     return t
 
 
-def bench_adam_fit(ctx, iters: int, size: int, lr: float = 0.02, decay: float = 0.985):
+def bench_adam_fit(ctx, iters: int, size: int, lr: float = 0.01, decay: float = 0.99, sphere: bool = False):
     """The inverse problem of the differentiable-render workload: target rendered at a = 0.7,
     inclination 60 deg (camera r = 20M, sphere phase 30 deg); Adam on (a, inclination) from (0.3,
     45 deg) with the step decaying as lr * decay^t, every gradient from prr_adjoint on the FP64
@@ -326,8 +326,9 @@ def bench_adam_fit(ctx, iters: int, size: int, lr: float = 0.02, decay: float = 
     from parrelray_b200 import abi, scenes
 
     ctx.upload_texture(scenes.SKY_ID, smooth_sky())
-    _, tgt, _ = ctx.render(scenes.kerr_512_adjoint(spin=0.7, incl_deg=60.0, precision=abi.PREC_FP64, size=size),
-                           want_float=True)
+    extra = {} if sphere else {"spheres": []}
+    _, tgt, _ = ctx.render(scenes.kerr_512_adjoint(spin=0.7, incl_deg=60.0, precision=abi.PREC_FP64, size=size,
+                                                   **extra), want_float=True)
     target = tgt[0].astype(np.float64)
     q = np.array([0.3, math.radians(45.0)])
     m = np.zeros(2)
@@ -338,15 +339,16 @@ def bench_adam_fit(ctx, iters: int, size: int, lr: float = 0.02, decay: float = 
     st = abi.Stats()
     t0 = time.perf_counter()
     for it in range(1, iters + 1):
-        d = scenes.kerr_512_adjoint(spin=float(q[0]), incl_deg=math.degrees(q[1]), precision=abi.PREC_FP64, size=size)
+        d = scenes.kerr_512_adjoint(spin=float(q[0]), incl_deg=math.degrees(q[1]), precision=abi.PREC_FP64, size=size,
+                                    **extra)
         _, cur, rs = ctx.render(d, want_float=True)
         diff = cur[0].astype(np.float64) - target
         losses.append(float(np.sum(diff * diff)))
         if losses[-1] < best[0]:
             best = (losses[-1], q.copy())
         dl = np.ascontiguousarray(2.0 * diff, dtype=np.float32)
-        abi.check(abi.load().prr_adjoint(ctx.h, C.byref(d), dl.ctypes.data_as(abi._fp), 0, g.ctypes.data_as(abi._dp),
-                                         C.byref(st)), ctx.h)
+        abi.check(abi.load().prr_adjoint(ctx.h, C.byref(d), dl.ctypes.data_as(abi._fp), 0 if sphere else -1,
+                                         g.ctypes.data_as(abi._dp), C.byref(st)), ctx.h)
         dev_ms += rs.kernel_ms + st.kernel_ms + st.trace_ms
         grad = np.array([g[0], g[2]])
         m = b1 * m + (1 - b1) * grad
@@ -355,7 +357,8 @@ def bench_adam_fit(ctx, iters: int, size: int, lr: float = 0.02, decay: float = 
         q[0] = min(max(q[0], 0.0), 0.99)
     wall = time.perf_counter() - t0
     ctx.upload_textures(scenes.standard_textures())
-    return {"workload": f"Adam on (a, i) from (0.3, 45 deg) towards (0.7, 60 deg), {size}x{size}, FP64, smooth sky",
+    return {"workload": f"Adam on (a, i) from (0.3, 45 deg) towards (0.7, 60 deg), {size}x{size}, FP64, smooth sky"
+                        + ("" if sphere else ", no sphere"),
             "iterations": iters, "lr": lr, "lr_decay": decay, "loss_first": losses[0], "loss_last": losses[-1],
             "loss_min": best[0], "a_best": float(best[1][0]), "incl_best_deg": math.degrees(best[1][1]),
             "a_final": float(q[0]), "incl_final_deg": math.degrees(q[1]),
@@ -421,6 +424,10 @@ def main():
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--adjoint-size", type=int, default=512, help="side of the square differentiable-render frame")
     ap.add_argument("--adam", type=int, default=0, help="also run an N-iteration Adam fit of (a, i) (0: off)")
+    ap.add_argument("--adam-lr", type=float, default=0.01)
+    ap.add_argument("--adam-decay", type=float, default=0.99)
+    ap.add_argument("--adam-sphere", action="store_true",
+                    help="keep the workload's sphere in the fit (its edges make the loss rougher)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--launch", default=None,
                     help="block,blocks_per_sm,compaction_interval,rays_per_thread for the persistent renderer "
@@ -572,7 +579,8 @@ def main():
                                             "d(L2 to the a=0.7 render)/d(a, M, i, r, phase)",
                                 "grad": g.tolist(), "accepted_steps": ast.accepted}
         if args.adam > 0 and ws == 1:
-            extra["adam_fit"] = bench_adam_fit(ctx, args.adam, args.adjoint_size)
+            extra["adam_fit"] = bench_adam_fit(ctx, args.adam, args.adjoint_size, args.adam_lr, args.adam_decay,
+                                               args.adam_sphere)
         if not args.no_trajectory and ws == 1:
             extra["trajectory"] = bench_trajectory(ctx, torch, stream)
         if not args.no_uneven and ws == 1:
