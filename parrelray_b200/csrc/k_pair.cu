@@ -8,6 +8,12 @@
 // paired instructions may round subnormal intermediates differently, so a
 // ray's result can differ between RPT = 1 and 2 in the last bits (it never
 // depends on the block shape or the refill interval).
+//
+// SPLIT (RPT = 1 only): the FP32 pass of a split-precision render.
+// Per-sample colours go to sample_rgb (the per-pixel combine runs after the
+// FP64 pass), and rays near a photon orbit (near_critical, tested before
+// the first attempt) or that dip below fp64_rfac * r_+ are queued for
+// k_fp64_requeue (k_persistent.cu).
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -42,22 +48,64 @@ struct Slot {
     int frame, px, py, s, S;
     float acc0, acc1, acc2;
     bool busy, need;
+    float flag_r;  // split precision: queue the ray for FP64 below this radius
     PhysRay<float> R;
     Hot<float> q;
 };
 
 struct Counts {
-    unsigned long long att = 0, acc = 0, rays = 0, esc = 0, cap = 0, hit = 0, inf = 0, nan = 0;
+    unsigned long long att = 0, acc = 0, rays = 0, esc = 0, cap = 0, hit = 0, inf = 0, nan = 0, f64 = 0;
 };
+
+// Split precision: the next sample of slot `sl`, or true when its pixel is
+// complete (the pixel itself is written by the combine after the FP64 pass).
+__device__ __forceinline__ bool next_sample_split(const FrameParams &fp, Slot &sl)
+{
+    sl.s += 1;
+    if (sl.s < sl.S) {
+        phys_init<float>(fp, sl.px, sl.py, sl.s, sl.R);
+        return false;
+    }
+    return true;
+}
+
+// Split precision: a ray queued for the FP64 pass.  Its colour slot is zeroed
+// here and overwritten by k_fp64_requeue; it is counted as a ray there.
+__device__ __forceinline__ bool flag_ray(const PersistentArgs &a, Slot &sl, Counts &c)
+{
+    const FrameParams &fp = a.frames[sl.frame];
+    c.att += (unsigned)sl.R.i;
+    c.acc += (unsigned)sl.R.accepted;
+    c.f64++;
+    const long long rid = ((long long)sl.py * fp.width + sl.px) * sl.S + sl.s;
+    const unsigned long long slot = atomicAdd(&a.counters[C_FP64_QUEUED], 1ull);
+    if ((long long)slot < a.fp64_capacity) a.fp64_queue[slot] = ((unsigned long long)sl.frame << 40) | (unsigned long long)rid;
+    float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
+    o[0] = o[1] = o[2] = 0.f;
+    return next_sample_split(fp, sl);
+}
 
 // A finished ray of slot `sl`: counters, SSAA accumulation, next sample or
 // pixel output.  Returns true when the slot's pixel is complete.
+template <bool SPLIT>
 __device__ __forceinline__ bool finish_ray(const PersistentArgs &a, Slot &sl, int result, V3<float> col, Counts &c)
 {
     const FrameParams &fp = a.frames[sl.frame];
     c.att += (unsigned)sl.R.i;
     c.acc += (unsigned)sl.R.accepted;
     c.rays++;
+    if constexpr (SPLIT) {
+        const long long rid = ((long long)sl.py * fp.width + sl.px) * sl.S + sl.s;
+        float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
+        o[0] = col.x; o[1] = col.y; o[2] = col.z;
+        if (result == PRR_RESULT_SUCCESS) {
+            if (col.x + col.y + col.z >= 0.f && metric_radius<float>(fp, sl.R.x.x, sl.R.x.y, sl.R.x.z) >= sl.q.rout) c.esc++;
+            else c.cap++;
+        } else if (result == PRR_RESULT_INTERSECTION) c.hit++;
+        else if (result == PRR_RESULT_INFINITE_GEO) c.inf++;
+        else c.nan++;
+        return next_sample_split(fp, sl);
+    }
     if (a.ray_state || a.sample_rgb) {  // per-ray outputs (single-frame parity runs)
         const long long rid = ((long long)sl.py * fp.width + sl.px) * sl.S + sl.s;
         if (a.ray_state) {
@@ -99,6 +147,7 @@ __device__ __forceinline__ bool finish_ray(const PersistentArgs &a, Slot &sl, in
     return true;
 }
 
+template <bool SPLIT>
 __device__ __forceinline__ void start_pixel(const PersistentArgs &a, Slot &sl, long long it)
 {
     sl.frame = find_frame2(a.frame_pix_begin, a.nframes, it);
@@ -110,6 +159,7 @@ __device__ __forceinline__ void start_pixel(const PersistentArgs &a, Slot &sl, l
     sl.s = 0;
     sl.acc0 = sl.acc1 = sl.acc2 = 0.f;
     sl.q = make_hot<float>(fp);
+    sl.flag_r = SPLIT ? fp.fp64_rfac * kerr_r_plus<float>(sl.q.M, sl.q.a) : -1.f;
     phys_init<float>(fp, sl.px, sl.py, 0, sl.R);
     sl.busy = true;
 }
@@ -151,9 +201,10 @@ template <> __device__ __forceinline__ void load_in<float2>(pv::StageIn<float2> 
 // least) cap the registers per thread.  One-slot threads in CTAs of up to 64
 // threads use the instantiation capped at 127 registers (8 CTAs = 16 warps
 // per SM, no spills; 4 % faster than 141 registers and 12 warps).
-template <int RPT, int MAXT, int MINB>
+template <int RPT, int MAXT, int MINB, bool SPLIT>
 __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
 {
+    static_assert(!SPLIT || RPT == 1, "split precision runs one ray per thread");
     using V = typename std::conditional<RPT == 2, float2, float>::type;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -161,7 +212,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
     Counts cnt;
 #pragma unroll
     for (int j = 0; j < RPT; j++) {
-        sl[j].busy = false; sl[j].need = true;
+        sl[j].busy = false; sl[j].need = true; sl[j].flag_r = -1.f;
         sl[j].frame = 0; sl[j].px = sl[j].py = sl[j].s = 0; sl[j].S = 1;
         sl[j].acc0 = sl[j].acc1 = sl[j].acc2 = 0.f;
         sl[j].R.x = {30.f, 0.f, 0.f, 0.f}; sl[j].R.u = {-1.f, 0.f, 0.f, 1.f};
@@ -195,7 +246,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
                     if (sl[j].need) {
                         const long long it = (long long)base + off + __popc(m[j] & lt);
                         sl[j].need = false;
-                        if (it < a.total_pixels) start_pixel(a, sl[j], it);
+                        if (it < a.total_pixels) start_pixel<SPLIT>(a, sl[j], it);
                         else sl[j].busy = false;
                     }
                     off += __popc(m[j]);
@@ -229,8 +280,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
             if (!sl[j].busy) continue;
             int result = 0;
             V3<float> col;
-            if (phys_precheck<float>(sl[j].R, result, col) == STEP_DONE) {
-                if (finish_ray(a, sl[j], result, col, cnt)) { sl[j].busy = false; sl[j].need = true; }
+            if (SPLIT && sl[j].R.i == 0 && near_critical<float>(a.frames[sl[j].frame], sl[j].R)) {
+                if (flag_ray(a, sl[j], cnt)) { sl[j].busy = false; sl[j].need = true; }
+            } else if (phys_precheck<float>(sl[j].R, result, col) == STEP_DONE) {
+                if (finish_ray<SPLIT>(a, sl[j], result, col, cnt)) { sl[j].busy = false; sl[j].need = true; }
             } else {
                 go[j] = true;
             }
@@ -261,9 +314,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
             int result = 0;
             V3<float> col;
             const int st = phys_accept<float>(fp, sl[j].q, sl[j].R, dxv, duv, pv::get(out.err, j), pv::get(out.hn, j),
-                                              result, col, -1.0f, nullptr);
+                                              result, col, SPLIT ? sl[j].flag_r : -1.0f, nullptr);
             if (st == STEP_CONTINUE) continue;
-            if (finish_ray(a, sl[j], result, col, cnt)) { sl[j].busy = false; sl[j].need = true; }
+            const bool done = (SPLIT && st == STEP_FLAG64) ? flag_ray(a, sl[j], cnt) : finish_ray<SPLIT>(a, sl[j], result, col, cnt);
+            if (done) { sl[j].busy = false; sl[j].need = true; }
         }
     }
     warp_sum_add(&a.counters[C_ATTEMPTS], cnt.att);
@@ -274,26 +328,33 @@ __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
     warp_sum_add(&a.counters[C_INTERSECTION], cnt.hit);
     warp_sum_add(&a.counters[C_INFINITE], cnt.inf);
     warp_sum_add(&a.counters[C_MATH_ERROR], cnt.nan);
+    if (SPLIT) warp_sum_add(&a.counters[C_FP64], cnt.f64);
 }
 
-cudaError_t launch_pair(const PersistentArgs &a, int rpt, int block, int blocks_per_sm, int nsm, cudaStream_t st)
+cudaError_t launch_pair(const PersistentArgs &a, int rpt, bool split, int block, int blocks_per_sm, int nsm, cudaStream_t st)
 {
     if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
+    if (split && (rpt != 1 || !a.sample_rgb || !a.fp64_queue)) return cudaErrorInvalidValue;
     int grid = nsm * blocks_per_sm;
     if (grid < 1) grid = 1;
-    if (rpt == 2) k_pair<2, 256, 1><<<grid, block, 0, st>>>(a);
-    else if (rpt == 1 && block <= 64) k_pair<1, 64, 8><<<grid, block, 0, st>>>(a);
-    else if (rpt == 1) k_pair<1, 256, 1><<<grid, block, 0, st>>>(a);
+    if (split && block <= 64) k_pair<1, 64, 8, true><<<grid, block, 0, st>>>(a);
+    else if (split) k_pair<1, 256, 1, true><<<grid, block, 0, st>>>(a);
+    else if (rpt == 2) k_pair<2, 256, 1, false><<<grid, block, 0, st>>>(a);
+    else if (rpt == 1 && block <= 64) k_pair<1, 64, 8, false><<<grid, block, 0, st>>>(a);
+    else if (rpt == 1) k_pair<1, 256, 1, false><<<grid, block, 0, st>>>(a);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
-int pair_occupancy(int rpt, int block)
+int pair_occupancy(int rpt, bool split, int block)
 {
     int n = 0;
-    cudaError_t e = rpt == 2     ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<2, 256, 1>, block, 0)
-                    : block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8>, block, 0)
-                                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1>, block, 0);
+    cudaError_t e;
+    if (split) e = block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, true>, block, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, true>, block, 0);
+    else if (rpt == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<2, 256, 1, false>, block, 0);
+    else e = block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, false>, block, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, false>, block, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
 }

@@ -11,8 +11,9 @@
 // of any size (the frame of a work item is found by binary search in the
 // per-frame pixel prefix).  Nothing of a ray's state touches HBM.
 //
-// Split precision: the FP32 pass writes per-sample colours and queues rays
-// near a photon orbit (or that dip below fp64_rfac*r_+) for an FP64 pass.
+// The FP64 and Christoffel-table renders run here; the FP32 pass of a
+// split-precision render runs in k_pair.cu, and its FP64 pass (the rays
+// queued near a photon orbit or below fp64_rfac*r_+) in k_fp64_requeue below.
 #include "kernels.cuh"
 #include "phys_stepper.cuh"
 
@@ -76,7 +77,7 @@ __device__ __forceinline__ void write_state(O *st, long long rid, const PhysRay<
 #define PRR_PERSISTENT_MINB 1
 #endif
 
-template <class T, int GEOD, bool SPLIT>
+template <class T, int GEOD>
 __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_persistent(PersistentArgs a)
 {
     const int lane = threadIdx.x & 31;
@@ -86,7 +87,6 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
     bool busy = false, need = true;
     PhysRay<T> R;
     Hot<T> q;
-    T flag_r = (T)-1;
     LaneCounts cnt;
     const long long t0 = clock64();
     unsigned iter = 0;
@@ -118,7 +118,6 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
                     S = fp.samples; s = 0;
                     acc0 = acc1 = acc2 = 0.f;
                     q = make_hot<T>(fp);
-                    flag_r = SPLIT ? (T)fp.fp64_rfac * kerr_r_plus<T>(q.M, q.a) : (T)-1;
                     phys_init<T>(fp, px, py, 0, R, uv);
                     busy = true;
                 } else {
@@ -144,55 +143,36 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
         const FrameParams &fp = a.frames[frame];
         int result = 0;
         V3<float> col;
-        int st = STEP_CONTINUE;
-        if (SPLIT && R.i == 0 && near_critical<T>(fp, R)) st = STEP_FLAG64;
-        else st = phys_attempt<T, GEOD>(fp, q, R, result, col, flag_r);
+        const int st = phys_attempt<T, GEOD>(fp, q, R, result, col, (T)-1);
         if (st == STEP_CONTINUE) continue;
 
         cnt.att += (unsigned)R.i;
         cnt.acc += (unsigned)R.accepted;
         const long long rid = ((long long)py * fp.width + px) * S + s;
-        if (SPLIT) {
+        cnt.add(result, result == PRR_RESULT_SUCCESS && metric_radius<T>(fp, R.x.x, R.x.y, R.x.z) >= q.rout);
+        if (a.ray_steps) a.ray_steps[fp.ray_begin + rid] = R.accepted;
+        if (a.ray_state) write_state<T, float>(a.ray_state, rid, R, result, uv);
+        if (a.ray_state64) write_state<T, double>(a.ray_state64, rid, R, result, uv);
+        if (a.sample_rgb) {
             float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
-            if (st == STEP_FLAG64) {
-                unsigned long long slot = atomicAdd(&a.counters[C_FP64_QUEUED], 1ull);
-                if ((long long)slot < a.fp64_capacity) a.fp64_queue[slot] = ((unsigned long long)frame << 40) | (unsigned long long)rid;
-                cnt.f64++;
-                o[0] = o[1] = o[2] = 0.f;
-            } else {
-                o[0] = col.x; o[1] = col.y; o[2] = col.z;
-                cnt.add(result, result == PRR_RESULT_SUCCESS && col.x + col.y + col.z >= 0.f &&
-                                    metric_radius<T>(fp, R.x.x, R.x.y, R.x.z) >= q.rout);
-            }
+            o[0] = col.x; o[1] = col.y; o[2] = col.z;
+        }
+        if (S == 1) {
+            acc0 = fminf(fmaxf(col.x, 0.f), 1.f); acc1 = fminf(fmaxf(col.y, 0.f), 1.f); acc2 = fminf(fmaxf(col.z, 0.f), 1.f);
         } else {
-            if (st == STEP_FLAG64) { result = PRR_RESULT_INFINITE_GEO; col = {0.f, 0.f, 0.f}; }
-            cnt.add(result, result == PRR_RESULT_SUCCESS && metric_radius<T>(fp, R.x.x, R.x.y, R.x.z) >= q.rout);
-            if (a.ray_steps) a.ray_steps[fp.ray_begin + rid] = R.accepted;
-            if (a.ray_state) write_state<T, float>(a.ray_state, rid, R, result, uv);
-            if (a.ray_state64) write_state<T, double>(a.ray_state64, rid, R, result, uv);
-            if (a.sample_rgb) {
-                float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
-                o[0] = col.x; o[1] = col.y; o[2] = col.z;
-            }
-            if (S == 1) {
-                acc0 = fminf(fmaxf(col.x, 0.f), 1.f); acc1 = fminf(fmaxf(col.y, 0.f), 1.f); acc2 = fminf(fmaxf(col.z, 0.f), 1.f);
-            } else {
-                acc0 += fminf(fmaxf(col.x * col.x, 0.f), 1.f);
-                acc1 += fminf(fmaxf(col.y * col.y, 0.f), 1.f);
-                acc2 += fminf(fmaxf(col.z * col.z, 0.f), 1.f);
-            }
+            acc0 += fminf(fmaxf(col.x * col.x, 0.f), 1.f);
+            acc1 += fminf(fmaxf(col.y * col.y, 0.f), 1.f);
+            acc2 += fminf(fmaxf(col.z * col.z, 0.f), 1.f);
         }
         s += 1;
         if (s < S) {
             phys_init<T>(fp, px, py, s, R, uv);
             continue;
         }
-        if (!SPLIT) {
-            if (S > 1) { acc0 = sqrtf(acc0 / (float)S); acc1 = sqrtf(acc1 / (float)S); acc2 = sqrtf(acc2 / (float)S); }
-            long long op = fp.pix_begin + (long long)py * fp.width + px;
-            if (a.image) { a.image[3 * op] = acc0; a.image[3 * op + 1] = acc1; a.image[3 * op + 2] = acc2; }
-            if (a.rgb8 && !fp.fxaa) { a.rgb8[3 * op] = quant8(acc0); a.rgb8[3 * op + 1] = quant8(acc1); a.rgb8[3 * op + 2] = quant8(acc2); }
-        }
+        if (S > 1) { acc0 = sqrtf(acc0 / (float)S); acc1 = sqrtf(acc1 / (float)S); acc2 = sqrtf(acc2 / (float)S); }
+        const long long op = fp.pix_begin + (long long)py * fp.width + px;
+        if (a.image) { a.image[3 * op] = acc0; a.image[3 * op + 1] = acc1; a.image[3 * op + 2] = acc2; }
+        if (a.rgb8 && !fp.fxaa) { a.rgb8[3 * op] = quant8(acc0); a.rgb8[3 * op + 1] = quant8(acc1); a.rgb8[3 * op + 2] = quant8(acc2); }
         busy = false;
         need = true;
     }
@@ -253,32 +233,32 @@ __global__ void __launch_bounds__(128) k_fp64_requeue(PersistentArgs a)
     cnt.flush(a.counters);
 }
 
-template <class T, int GEOD, bool SPLIT>
+template <class T, int GEOD>
 static cudaError_t launch_one(const PersistentArgs &a, int block, int blocks_per_sm, int nsm, cudaStream_t st)
 {
     int grid = nsm * blocks_per_sm;
     if (grid < 1) grid = 1;
-    k_persistent<T, GEOD, SPLIT><<<grid, block, 0, st>>>(a);
+    k_persistent<T, GEOD><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st)
 {
     if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
-    if (precision == PRR_PREC_FP64) return launch_one<double, 0, false>(a, block, blocks_per_sm, nsm, st);
-    if (precision == PRR_PREC_SPLIT) return launch_one<float, 0, true>(a, block, blocks_per_sm, nsm, st);
-    if (a.geod_table) return launch_one<float, 1, false>(a, block, blocks_per_sm, nsm, st);
-    return launch_pair(a, a.rays_per_thread == 2 ? 2 : 1, block, blocks_per_sm, nsm, st);
+    if (precision == PRR_PREC_FP64) return launch_one<double, 0>(a, block, blocks_per_sm, nsm, st);
+    if (precision == PRR_PREC_SPLIT) return launch_pair(a, 1, true, block, blocks_per_sm, nsm, st);
+    if (a.geod_table) return launch_one<float, 1>(a, block, blocks_per_sm, nsm, st);
+    return launch_pair(a, a.rays_per_thread == 2 ? 2 : 1, false, block, blocks_per_sm, nsm, st);
 }
 
 int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread)
 {
     int n = 0;
     cudaError_t e;
-    if (precision == PRR_PREC_FP64) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<double, 0, false>, block, 0);
-    else if (precision == PRR_PREC_SPLIT) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 0, true>, block, 0);
-    else if (geod_table) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 1, false>, block, 0);
-    else return pair_occupancy(rays_per_thread == 2 ? 2 : 1, block);
+    if (precision == PRR_PREC_FP64) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<double, 0>, block, 0);
+    else if (precision == PRR_PREC_SPLIT) return pair_occupancy(1, true, block);
+    else if (geod_table) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 1>, block, 0);
+    else return pair_occupancy(rays_per_thread == 2 ? 2 : 1, false, block);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
 }

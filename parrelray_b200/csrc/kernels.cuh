@@ -59,16 +59,19 @@ struct PersistentArgs {
     int *ray_steps;              // optional: accepted steps per ray (FP64/table/split kernels, single frame)
 };
 // Dispatches to the kernel of the precision: FP32 with the register
-// contraction -> k_pair (k_pair.cu, rays_per_thread slots per thread);
-// FP64, SPLIT and the Christoffel-table variant -> k_persistent.
+// contraction and the FP32 pass of SPLIT -> k_pair (k_pair.cu,
+// rays_per_thread slots per thread); FP64 and the Christoffel-table
+// variant -> k_persistent.
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st);
 
 // k_persistent.cu: resident CTAs per SM of the kernel launch_persistent picks.
 int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread = 1);
 
-// k_pair.cu: the FP32 renderer with `rpt` pixel slots per thread.
-cudaError_t launch_pair(const PersistentArgs &a, int rpt, int block, int blocks_per_sm, int nsm, cudaStream_t st);
-int pair_occupancy(int rpt, int block);
+// k_pair.cu: the FP32 renderer with `rpt` pixel slots per thread; `split`:
+// the FP32 pass of a split-precision render (rpt 1; needs sample_rgb and
+// fp64_queue).
+cudaError_t launch_pair(const PersistentArgs &a, int rpt, bool split, int block, int blocks_per_sm, int nsm, cudaStream_t st);
+int pair_occupancy(int rpt, bool split, int block);
 
 // k_persistent.cu: FP64 re-integration of the queued rays of a split render.
 cudaError_t launch_fp64_requeue(const PersistentArgs &a, int block, int nsm, cudaStream_t st);
