@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PRR_ABI_VERSION 2
+#define PRR_ABI_VERSION 3
 #define PRR_MAX_SPHERES 8
 #define PRR_MAX_TEXTURES 32
 
@@ -113,6 +113,74 @@ typedef enum prr_schedule { PRR_SCHED_PLAIN = 0, PRR_SCHED_PERSISTENT = 1 } prr_
  * used for gradients. */
 typedef enum prr_bg_filter { PRR_BG_RMS2X2 = 0, PRR_BG_BILINEAR = 1 } prr_bg_filter;
 
+/* Emission from plasma around the hole (PHYSICAL mode, FP32 or FP64).  The
+ * reference declares the fields (main/Spacetime.h:50-51: density, pressure,
+ * temperature, velocity, magnetic field on a grid of dataDim cells) and a
+ * per-ray luminosity integrated along the path (Ray::I, main/base.h:175),
+ * and uses neither; this is the model that fills them in.
+ *
+ * Along each ray, at every accepted step of affine length h, with n the
+ * plasma density, u_e the plasma 4-velocity, k the ray's 4-momentum and
+ * g = (k.u_cam)/(k.u_e) the frequency ratio (u_cam: a static observer at the
+ * camera):
+ *     I   += trans * g^(2 + spectral_index) * j * nu_cam * h,  j = n * Theta^temp_power
+ *     trans *= exp(-absorb * n * nu_cam * h / g)
+ * (nu_cam = -k.u_cam scales h to the affine length of a ray whose camera
+ * frequency is 1; this is the invariant transfer equation d(I_nu/nu^3)/dl =
+ * j_nu/nu^2 for a spectrum j_nu ~ nu^-spectral_index, with grey absorption.)
+ * Points where the flow is not timelike or k.u_e >= 0 emit nothing.  The
+ * pixel colour is trans * (the colour without emission) + map(gain * I).
+ *
+ * Rays are traced forward from the camera (as every mode here and the
+ * reference do), so the received picture is the time reverse of the traced
+ * scene: in Kerr the hole of spin -a; every flow velocity reversed.  g is
+ * invariant under that reversal, so the formula above is exact for it.
+ *
+ * DISK: n = (r / r_in)^(-index) * exp(-cos^2(theta) / (2 height^2)) for
+ *   r_in <= r <= r_out (Kerr-Schild r, cos theta = z / r), 0 elsewhere;
+ *   Theta = 1; u_e on circular orbits of angular velocity
+ *   Omega = sense sqrt(M) / (r^1.5 + sense a sqrt(M)) about the z axis
+ *   (the equatorial Keplerian value at the point's r; sense +1 co-rotates
+ *   with the hole).
+ * GRID: n, Theta and (optionally) the coordinate velocity dx^i/dt from the
+ *   plasma grid of prr_upload_plasma, trilinear between its nodes, 0
+ *   outside its box and outside [r_in, r_out]; without a velocity field the
+ *   flow is the DISK's. */
+typedef enum prr_emission { PRR_EMISSION_NONE = 0, PRR_EMISSION_DISK = 1, PRR_EMISSION_GRID = 2 } prr_emission;
+
+/* map(x) of the emission colour: AFMHOT (clamp(2x), clamp(2x - 1/2),
+ * clamp(2x - 1)) or GREY (clamp(x) in all three channels). */
+typedef enum prr_colormap { PRR_CMAP_AFMHOT = 0, PRR_CMAP_GREY = 1 } prr_colormap;
+
+typedef struct prr_emission_desc {
+    float index;          /* DISK: radial density power law */
+    float height;         /* DISK: Gaussian width in cos(theta) (> 0) */
+    float r_in, r_out;    /* emitting shell, Kerr-Schild r */
+    float spectral_index; /* j_nu ~ nu^-spectral_index */
+    float absorb;         /* grey absorption per unit density (>= 0) */
+    float gain;           /* colour scale of I */
+    int32_t sense;        /* +1 co-rotating, -1 counter-rotating (Keplerian flow) */
+    float temp_power;     /* GRID: j = n * Theta^temp_power */
+    int32_t colormap;     /* prr_colormap */
+    int32_t _pad[2];
+} prr_emission_desc;
+
+/* A plasma grid (the reference's density/temperature/velocity fields,
+ * main/Spacetime.h:50-51, with its dataDim = (nx, ny, nz)).  Nodes sit at
+ * lo + (hi - lo) * (i, j, k) / (n - 1) in Kerr-Schild (x, y, z); arrays are
+ * x-fastest (index i + nx * (j + ny * k)).  density is required (>= 0);
+ * temperature (NULL: 1 everywhere) and velocity (3 floats per node, the
+ * coordinate velocity dx/dt, dy/dt, dz/dt; NULL: the DISK flow) are
+ * optional.  The reference's pressure and magnetic field are not used by the
+ * emission model. */
+typedef struct prr_plasma_desc {
+    int32_t nx, ny, nz;   /* >= 2 each */
+    float lo[3], hi[3];   /* box corners, lo < hi */
+    const float *density;
+    const float *temperature;
+    const float *velocity;
+} prr_plasma_desc;
+
 /* A textured sphere (scene/sphere.h:19-65). */
 typedef struct prr_sphere {
     float center[3];
@@ -154,8 +222,9 @@ typedef struct prr_frame_desc {
     int32_t nspheres;
     int32_t camera;      /* prr_camera */
     uint32_t ssaa_seed;  /* RANDOM / JITTERED sample offsets */
-    int32_t _pad1;
+    int32_t emission;    /* prr_emission (PHYSICAL mode, FP32/FP64, persistent schedule) */
     prr_sphere spheres[PRR_MAX_SPHERES];
+    prr_emission_desc emis; /* used when emission != NONE */
 } prr_frame_desc;
 
 /* Counters of one render call (summed over frames). */
@@ -198,6 +267,13 @@ const char *prr_last_error(const prr_ctx *ctx);
  * reference loads with stbi_ldr_to_hdr_gamma(1), cudamaths/image.cu:15).
  * Alpha is ignored.  Re-uploading an id replaces it. */
 prr_status prr_upload_texture(prr_ctx *ctx, int id, const uint8_t *rgba8, int w, int h);
+
+/* ---- plasma (the grid behind the reference's Spacetime::setDataDimensions
+ * and its density/temperature/velocity pointers, main/Spacetime.h:28,50-51;
+ * the reference never fills them) ----
+ * Copies the grid to the device; replaces the previous one.  Frames with
+ * emission = GRID sample the grid present when they are rendered. */
+prr_status prr_upload_plasma(prr_ctx *ctx, const prr_plasma_desc *plasma);
 
 /* ---- rendering (replaces prr.cpp:renderframe 237-341 and the frame loop
  *      382-386) ----
@@ -429,7 +505,8 @@ prr_status prr_make_texture(int kind, uint32_t seed, int w, int h, uint8_t *out_
 /* Fills `d` with the defaults used where a deck is silent. */
 void prr_frame_desc_defaults(prr_frame_desc *d);
 /* sizeof of the ABI structs, for binding checks: 0 prr_frame_desc,
- * 1 prr_stats, 2 prr_launch_config, 3 prr_sphere; 0 for other values. */
+ * 1 prr_stats, 2 prr_launch_config, 3 prr_sphere, 4 prr_emission_desc,
+ * 5 prr_plasma_desc; 0 for other values. */
 size_t prr_sizeof(int which);
 
 #ifdef __cplusplus

@@ -26,10 +26,16 @@
 //   texture sampling     cudamaths/tex2d.cuh:112-131
 //   background           main/base.h:119-162 (getColorDefault2), cudamaths/f3.cuh:101-103
 //   SSAA combine / FXAA  kernels/ssaa.cuh:109-131, 141-181
+//   plasma emission      the model of prr_emission (include/prr.h) for the
+//                        fields main/Spacetime.h:50-51 and Ray::I
+//                        (main/base.h:175), which the reference declares
+//                        and never uses; restated here with the full 4x4
+//                        metric
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "prr.h"
@@ -162,9 +168,19 @@ template <class T> inline V3<T> tex_bilinear(const Tex &t, T u, T v)
 template <class T> inline T fmaxT(T a, T b) { return fmax(a, b); }
 template <class T> inline T fminT(T a, T b) { return fmin(a, b); }
 
+// Host copy of a plasma grid (prr_oracle_set_plasma).
+struct Plasma {
+    bool present = false;
+    int nx = 0, ny = 0, nz = 0;
+    float lo[3] = {0, 0, 0}, inv[3] = {0, 0, 0};  // inv = (n - 1) / (hi - lo), in float as the library computes it
+    std::vector<float> n, theta, vel;             // theta, vel empty when absent
+};
+Plasma g_plasma;
+
 struct Scene {
     const prr_frame_desc *d;
     Tex tex[PRR_MAX_TEXTURES];
+    const Plasma *plasma = nullptr;
 };
 
 // ---------------------------------------------------------------- metrics
@@ -456,6 +472,7 @@ template <class T> struct RayState {
     V3<float> rgb;
     V3<T> rgbT;  // the same colour in T (gradient path)
     unsigned long long cells = 0;  // texel cells read for the colour (finite-difference tests)
+    T I = T(0.0), trans = T(1.0), nu_cam = T(0.0);  // plasma emission (intensity, transmittance, camera frequency)
 };
 
 // The stochastic placements' hash: the PCG output permutation of an LCG
@@ -573,6 +590,44 @@ template <class T> inline T max4abs(const V4<T> &a, const V4<T> &b)
     return fmaxT<T>(fmaxT<T>(fmaxT<T>(fabs(a.x - b.x), fabs(a.y - b.y)), fabs(a.z - b.z)), fabs(a.w - b.w));
 }
 
+// ---------------------------------------------------------------- emission
+
+template <class T> inline T gdot(const T g[16], const T A[4], const T B[4])
+{
+    T s = 0;
+    for (int m = 0; m < 4; m++)
+        for (int n = 0; n < 4; n++) s += g[4 * m + n] * A[m] * B[n];
+    return s;
+}
+
+// Trilinear interpolation of the grid's nodes around (x, y, z); false
+// outside the box.
+template <class T> bool plasma_at(const Plasma &P, T x, T y, T z, T &n, T &theta, T v[3])
+{
+    const T p[3] = {x, y, z};
+    const int dim[3] = {P.nx, P.ny, P.nz};
+    int i[3];
+    T t[3];
+    for (int k = 0; k < 3; k++) {
+        T s = (p[k] - (T)P.lo[k]) * (T)P.inv[k];
+        if (!(s >= (T)0 && s <= (T)(dim[k] - 1))) return false;
+        i[k] = std::min((int)s, dim[k] - 2);
+        t[k] = s - (T)i[k];
+    }
+    n = 0; theta = P.theta.empty() ? (T)1 : (T)0;
+    v[0] = v[1] = v[2] = 0;
+    for (int c = 0; c < 8; c++) {
+        const int bx = c & 1, by = (c >> 1) & 1, bz = c >> 2;
+        const T w = (bx ? t[0] : (T)1 - t[0]) * (by ? t[1] : (T)1 - t[1]) * (bz ? t[2] : (T)1 - t[2]);
+        const size_t id = (size_t)(i[0] + bx) + (size_t)P.nx * ((size_t)(i[1] + by) + (size_t)P.ny * (size_t)(i[2] + bz));
+        n += w * (T)P.n[id];
+        if (!P.theta.empty()) theta += w * (T)P.theta[id];
+        if (!P.vel.empty())
+            for (int k = 0; k < 3; k++) v[k] += w * (T)P.vel[3 * id + k];
+    }
+    return true;
+}
+
 template <class T> class Tracer {
 public:
     Tracer(const Scene &sc) : sc_(sc), d_(sc.d)
@@ -652,6 +707,58 @@ private:
         if (ref_) u = scl(u0, u);  // whole 4-vector scaled (solver.cuh:54)
         else u.w = u0;            // null: u^t solves g(u,u) = 0
         R.u = u;
+        if constexpr (std::is_floating_point<T>::value) emis_init(R);
+    }
+
+    // Frequency of the ray measured by a static observer at the camera:
+    // nu_cam = -k_t / sqrt(-g_tt).
+    void emis_init(RayState<T> &R) const
+    {
+        if (d_->emission == PRR_EMISSION_NONE) return;
+        T g[16];
+        mt_.metric(R.r, g, false);
+        const T k[4] = {R.u.x, R.u.y, R.u.z, R.u.w};
+        const T kt = g[12] * k[0] + g[13] * k[1] + g[14] * k[2] + g[15] * k[3];
+        R.nu_cam = -kt / sqrt(-g[15]);
+        R.I = 0;
+        R.trans = 1;
+    }
+
+    // Emission of one accepted step of affine length h ending at (R.r, R.u).
+    void emis_step(RayState<T> &R, T h) const
+    {
+        if (d_->emission == PRR_EMISSION_NONE) return;
+        const prr_emission_desc &e = d_->emis;
+        const T M = d_->metric == PRR_METRIC_FLAT ? (T)0 : mt_.M, a = d_->metric == PRR_METRIC_KERR ? mt_.a : (T)0;
+        const T r = ks_r<T>(R.r.x, R.r.y, R.r.z, a);
+        if (!(r >= (T)e.r_in && r <= (T)e.r_out)) return;
+        T n, theta = 1, v[3];
+        bool flow = false;
+        if (d_->emission == PRR_EMISSION_DISK) {
+            const T c = R.r.z / r;
+            n = pow(r / (T)e.r_in, -(T)e.index) * std::exp(-c * c / ((T)2 * (T)e.height * (T)e.height));
+        } else {
+            if (!sc_.plasma || !plasma_at<T>(*sc_.plasma, R.r.x, R.r.y, R.r.z, n, theta, v)) return;
+            flow = !sc_.plasma->vel.empty();
+        }
+        if (!(n > (T)0)) return;
+        if (!flow) {  // equatorial Keplerian angular velocity at r, about the z axis
+            const T s = (T)e.sense, om = s * sqrt(M) / (r * sqrt(r) + s * a * sqrt(M));
+            v[0] = -om * R.r.y; v[1] = om * R.r.x; v[2] = 0;
+        }
+        T g[16];
+        mt_.metric(R.r, g, false);
+        const T xi[4] = {v[0], v[1], v[2], (T)1}, k[4] = {R.u.x, R.u.y, R.u.z, R.u.w};
+        const T N = gdot<T>(g, xi, xi);
+        if (!(N < (T)0)) return;
+        const T nu_e = -gdot<T>(g, k, xi) / sqrt(-N);
+        if (!(nu_e > (T)0)) return;
+        const T gr = R.nu_cam / nu_e, dl = R.nu_cam * h;
+        T j = n;
+        if (d_->emission == PRR_EMISSION_GRID && e.temp_power != 0.0f) j *= pow(theta, (T)e.temp_power);
+        const T w = e.spectral_index == 0.0f ? gr * gr : pow(gr, (T)2 + (T)e.spectral_index);
+        R.I += R.trans * w * j * dl;
+        if (e.absorb > 0.0f) R.trans *= std::exp(-(T)e.absorb * n * dl / gr);
     }
 
     bool user_update(RayState<T> &R, T h) const
@@ -773,12 +880,14 @@ private:
             R.r = _x; R.u = _u;
             accepted++;
             R.accepted = accepted;
+            const T h_step = h;
             if (user_update(R, h)) {
                 if (!intersect) h = _h;
                 x = _x; u = _u; R.r = x; R.u = u; trace_h = h;
             } else if (R.result == PRR_RESULT_INTERSECTION && !intersect) {
                 intersect = true; h = hmin; continue;
             }
+            if constexpr (std::is_floating_point<T>::value) emis_step(R, h_step);
             if (!user_endloop(R, trace_h)) return;
             x = R.r; u = R.u;
             l += h;
@@ -810,6 +919,14 @@ private:
         if (set_black) c = {black[0], black[1], black[2]};
         R.rgb = {(float)c.x, (float)c.y, (float)c.z};
         R.rgbT = c;
+        if (d_->emission != PRR_EMISSION_NONE) {  // trans * colour + map(gain * I)
+            const float x = (float)((T)d_->emis.gain * R.I), tr = (float)R.trans;
+            auto cl = [](float v) { return std::fmin(std::fmax(v, 0.0f), 1.0f); };
+            float m[3];
+            if (d_->emis.colormap == PRR_CMAP_GREY) m[0] = m[1] = m[2] = cl(x);
+            else { m[0] = cl(2.0f * x); m[1] = cl(2.0f * x - 0.5f); m[2] = cl(2.0f * x - 1.0f); }
+            R.rgb = {tr * R.rgb.x + m[0], tr * R.rgb.y + m[1], tr * R.rgb.z + m[2]};
+        }
     }
 };
 
@@ -909,11 +1026,13 @@ Scene make_scene(const prr_frame_desc *d, const uint8_t *const *tex, const int *
     for (int i = 0; i < PRR_MAX_TEXTURES; i++) {
         if (tex && tex[i]) { sc.tex[i].p = tex[i]; sc.tex[i].w = tw[i]; sc.tex[i].h = th[i]; }
     }
+    if (g_plasma.present) sc.plasma = &g_plasma;
     return sc;
 }
 
 template <class T>
-void trace_list(const Scene &sc, const long long *ids, long long n, int nthreads, double *state, float *rgb)
+void trace_list(const Scene &sc, const long long *ids, long long n, int nthreads, double *state, float *rgb,
+                double *emis = nullptr)
 {
     Tracer<T> tr(sc);
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1)
@@ -927,6 +1046,7 @@ void trace_list(const Scene &sc, const long long *ids, long long n, int nthreads
             s[11] = (double)R.accepted; s[12] = (double)R.attempts;
         }
         if (rgb) { rgb[3 * k] = R.rgb.x; rgb[3 * k + 1] = R.rgb.y; rgb[3 * k + 2] = R.rgb.z; }
+        if (emis) { emis[3 * k] = (double)R.I; emis[3 * k + 1] = (double)R.trans; emis[3 * k + 2] = (double)R.nu_cam; }
     }
 }
 
@@ -955,6 +1075,40 @@ int prr_oracle_trace(const prr_frame_desc *d, const uint8_t *const *tex, const i
     return 0;
 }
 
+// Plasma emission per ray: emis[3] = I, transmittance, nu_cam (the camera
+// frequency); otherwise as prr_oracle_trace.
+int prr_oracle_trace_emission(const prr_frame_desc *d, const uint8_t *const *tex, const int *tw, const int *th,
+                              int precision, const long long *ids, long long n, int nthreads, double *emis)
+{
+    if (!d || n < 0 || d->mode != PRR_MODE_PHYSICAL) return 1;
+    Scene sc = make_scene(d, tex, tw, th);
+    if (precision == 1) trace_list<double>(sc, ids, n, nthreads, nullptr, nullptr, emis);
+    else trace_list<float>(sc, ids, n, nthreads, nullptr, nullptr, emis);
+    return 0;
+}
+
+// The plasma grid of GRID emission (as prr_upload_plasma takes it); NULL
+// clears it.  Returns 1 on a bad descriptor.
+int prr_oracle_set_plasma(const prr_plasma_desc *p)
+{
+    g_plasma = Plasma();
+    if (!p) return 0;
+    if (!p->density || p->nx < 2 || p->ny < 2 || p->nz < 2) return 1;
+    const size_t nn = (size_t)p->nx * p->ny * p->nz;
+    g_plasma.nx = p->nx; g_plasma.ny = p->ny; g_plasma.nz = p->nz;
+    const int dim[3] = {p->nx, p->ny, p->nz};
+    for (int k = 0; k < 3; k++) {
+        if (!(p->hi[k] > p->lo[k])) return 1;
+        g_plasma.lo[k] = p->lo[k];
+        g_plasma.inv[k] = (float)(dim[k] - 1) / (p->hi[k] - p->lo[k]);
+    }
+    g_plasma.n.assign(p->density, p->density + nn);
+    if (p->temperature) g_plasma.theta.assign(p->temperature, p->temperature + nn);
+    if (p->velocity) g_plasma.vel.assign(p->velocity, p->velocity + 3 * nn);
+    g_plasma.present = true;
+    return 0;
+}
+
 // SSAA combine and optional FXAA of per-sample colours (rgb: W*H*S*3).
 // FP64 host gradient of sum(dL_dimage * image) with respect to (spin, mass,
 // camera inclination, camera distance, orbital phase of sphere
@@ -974,7 +1128,7 @@ int prr_oracle_grad(const prr_frame_desc *d, const uint8_t *const *tex, const in
                     const double *params, double *loss_out, long long *sig_out)
 {
     typedef HD<5> D;
-    if (!d || !dL_dimage || !grads || d->mode != PRR_MODE_PHYSICAL || d->fxaa) return 1;
+    if (!d || !dL_dimage || !grads || d->mode != PRR_MODE_PHYSICAL || d->fxaa || d->emission != PRR_EMISSION_NONE) return 1;
     Scene sc = make_scene(d, tex, tw, th);
     double px = d->cam_pos[0], py = d->cam_pos[1], pz = d->cam_pos[2];
     double r = std::sqrt(px * px + py * py + pz * pz);

@@ -67,6 +67,28 @@ class Context:
         for k, v in textures.items():
             self.upload_texture(k, v)
 
+    def upload_plasma(self, density: np.ndarray, lo, hi, temperature: np.ndarray | None = None,
+                      velocity: np.ndarray | None = None) -> None:
+        """The plasma grid of GRID emission (prr_upload_plasma): density and temperature as (nz, ny, nx)
+        arrays, velocity as (nz, ny, nx, 3) (coordinate velocity dx/dt), on nodes spanning the box lo..hi."""
+        n = np.ascontiguousarray(density, dtype=np.float32)
+        if n.ndim != 3:
+            raise ValueError("density must be an (nz, ny, nx) array")
+        t = None if temperature is None else np.ascontiguousarray(temperature, dtype=np.float32)
+        v = None if velocity is None else np.ascontiguousarray(velocity, dtype=np.float32)
+        if t is not None and t.shape != n.shape:
+            raise ValueError("temperature must have the density's shape")
+        if v is not None and v.shape != n.shape + (3,):
+            raise ValueError("velocity must be an (nz, ny, nx, 3) array")
+        d = abi.PlasmaDesc()
+        d.nz, d.ny, d.nx = n.shape
+        d.lo[:] = [float(x) for x in lo]
+        d.hi[:] = [float(x) for x in hi]
+        d.density = n.ctypes.data_as(abi._fp)
+        d.temperature = t.ctypes.data_as(abi._fp) if t is not None else None
+        d.velocity = v.ctypes.data_as(abi._fp) if v is not None else None
+        self._check(self.lib.prr_upload_plasma(self.h, C.byref(d)))
+
     def set_schedule(self, schedule: int, cfg: LaunchConfig | None = None) -> None:
         self._check(self.lib.prr_set_schedule(self.h, schedule, C.byref(cfg) if cfg else None))
 

@@ -32,10 +32,27 @@ PREC_FP32, PREC_FP64, PREC_SPLIT = 0, 1, 2
 SCHED_PLAIN, SCHED_PERSISTENT = 0, 1
 BG_RMS2X2, BG_BILINEAR = 0, 1
 OPT_GEOD_TABLE, OPT_WATCHDOG_CYCLES = 1, 2
+EMISSION_NONE, EMISSION_DISK, EMISSION_GRID = 0, 1, 2
+CMAP_AFMHOT, CMAP_GREY = 0, 1
 
 
 class Sphere(C.Structure):
     _fields_ = [("center", C.c_float * 3), ("radius", C.c_float), ("texture_id", C.c_int32), ("_pad", C.c_int32 * 3)]
+
+
+class EmissionDesc(C.Structure):
+    _fields_ = [
+        ("index", C.c_float), ("height", C.c_float), ("r_in", C.c_float), ("r_out", C.c_float),
+        ("spectral_index", C.c_float), ("absorb", C.c_float), ("gain", C.c_float), ("sense", C.c_int32),
+        ("temp_power", C.c_float), ("colormap", C.c_int32), ("_pad", C.c_int32 * 2),
+    ]
+
+
+class PlasmaDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("lo", C.c_float * 3), ("hi", C.c_float * 3),
+        ("density", C.POINTER(C.c_float)), ("temperature", C.POINTER(C.c_float)), ("velocity", C.POINTER(C.c_float)),
+    ]
 
 
 class FrameDesc(C.Structure):
@@ -48,8 +65,9 @@ class FrameDesc(C.Structure):
         ("rtol", C.c_float), ("atol", C.c_float), ("rout", C.c_float), ("horizon_eps", C.c_float),
         ("max_steps", C.c_int32), ("background_id", C.c_int32), ("bg_filter", C.c_int32), ("fxaa", C.c_int32),
         ("fp64_delta", C.c_float), ("fp64_rfac", C.c_float),
-        ("nspheres", C.c_int32), ("camera", C.c_int32), ("ssaa_seed", C.c_uint32), ("_pad1", C.c_int32),
+        ("nspheres", C.c_int32), ("camera", C.c_int32), ("ssaa_seed", C.c_uint32), ("emission", C.c_int32),
         ("spheres", Sphere * PRR_MAX_SPHERES),
+        ("emis", EmissionDesc),
     ]
 
     @property
@@ -87,6 +105,7 @@ SIGNATURES = {
     "prr_destroy": (None, [_P]),
     "prr_last_error": (C.c_char_p, [_P]),
     "prr_upload_texture": (C.c_int, [_P, C.c_int, _u8p, C.c_int, C.c_int]),
+    "prr_upload_plasma": (C.c_int, [_P, C.POINTER(PlasmaDesc)]),
     "prr_render": (C.c_int, [_P, C.POINTER(FrameDesc), C.c_int, _u8p, _fp, C.POINTER(Stats)]),
     "prr_render_device": (C.c_int, [_P, C.POINTER(FrameDesc), C.c_int, _P, _P, _P]),
     "prr_trace_rays": (C.c_int, [_P, C.POINTER(FrameDesc), _fp, _fp, C.POINTER(Stats)]),

@@ -63,6 +63,8 @@ size_t prr_sizeof(int which)
     case 1: return sizeof(prr_stats);
     case 2: return sizeof(prr_launch_config);
     case 3: return sizeof(prr_sphere);
+    case 4: return sizeof(prr_emission_desc);
+    case 5: return sizeof(prr_plasma_desc);
     }
     return 0;
 }
@@ -106,6 +108,10 @@ void prr_frame_desc_defaults(prr_frame_desc *d)
     d->fp64_rfac = 1.05f;
     d->nspheres = 0;
     for (int i = 0; i < PRR_MAX_SPHERES; i++) d->spheres[i].texture_id = -1;
+    d->emission = PRR_EMISSION_NONE;
+    d->emis.index = 2.0f; d->emis.height = 0.3f; d->emis.r_in = 2.0f; d->emis.r_out = 30.0f;
+    d->emis.spectral_index = 0.0f; d->emis.absorb = 0.0f; d->emis.gain = 1.0f; d->emis.sense = 1;
+    d->emis.temp_power = 0.0f; d->emis.colormap = PRR_CMAP_AFMHOT;
 }
 
 prr_status prr_create(int device, prr_ctx **out)
@@ -203,6 +209,62 @@ prr_status prr_upload_texture(prr_ctx *ctx, int id, const uint8_t *rgba8, int w,
     PRR_CK(ctx, cudaMemcpyAsync(t.buf.p, rgba8, bytes, cudaMemcpyHostToDevice, ctx->stream));
     PRR_CK(ctx, cudaStreamSynchronize(ctx->stream));
     t.w = w; t.h = h;
+    return PRR_OK;
+}
+
+prr_status prr_upload_plasma(prr_ctx *ctx, const prr_plasma_desc *pd)
+{
+    if (!ctx) return PRR_ERR_INVALID;
+    if (!pd || !pd->density || pd->nx < 2 || pd->ny < 2 || pd->nz < 2) {
+        fail(ctx, "prr_upload_plasma: need a density array and nx, ny, nz >= 2");
+        return PRR_ERR_INVALID;
+    }
+    const long long nn = (long long)pd->nx * pd->ny * pd->nz;
+    if (nn > (1LL << 28)) { fail(ctx, "prr_upload_plasma: more than 2^28 nodes"); return PRR_ERR_INVALID; }
+    for (int k = 0; k < 3; k++)
+        if (!std::isfinite(pd->lo[k]) || !std::isfinite(pd->hi[k]) || !(pd->hi[k] > pd->lo[k])) {
+            fail(ctx, "prr_upload_plasma: need finite box corners with lo < hi on every axis");
+            return PRR_ERR_INVALID;
+        }
+    for (long long i = 0; i < nn; i++) {
+        if (!(pd->density[i] >= 0.0f) || !std::isfinite(pd->density[i])) {
+            fail(ctx, "prr_upload_plasma: density must be finite and >= 0 (node " + std::to_string(i) + ")");
+            return PRR_ERR_INVALID;
+        }
+        if (pd->temperature && (!(pd->temperature[i] >= 0.0f) || !std::isfinite(pd->temperature[i]))) {
+            fail(ctx, "prr_upload_plasma: temperature must be finite and >= 0 (node " + std::to_string(i) + ")");
+            return PRR_ERR_INVALID;
+        }
+        if (pd->velocity && !(std::isfinite(pd->velocity[3 * i]) && std::isfinite(pd->velocity[3 * i + 1]) &&
+                              std::isfinite(pd->velocity[3 * i + 2]))) {
+            fail(ctx, "prr_upload_plasma: velocity must be finite (node " + std::to_string(i) + ")");
+            return PRR_ERR_INVALID;
+        }
+    }
+    PRR_CK(ctx, cudaSetDevice(ctx->device));
+    PlasmaGrid &G = ctx->plasma;
+    G.present = false;
+    const size_t fb = (size_t)nn * sizeof(float);
+    if (G.n.ensure(fb) != PRR_OK || (pd->temperature && G.theta.ensure(fb) != PRR_OK) ||
+        (pd->velocity && G.vel.ensure((size_t)nn * sizeof(float4)) != PRR_OK)) {
+        fail(ctx, "prr_upload_plasma: out of device memory");
+        return PRR_ERR_NOMEM;
+    }
+    PRR_CK(ctx, cudaMemcpyAsync(G.n.p, pd->density, fb, cudaMemcpyHostToDevice, ctx->stream));
+    if (pd->temperature) PRR_CK(ctx, cudaMemcpyAsync(G.theta.p, pd->temperature, fb, cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<float4> v4;
+    if (pd->velocity) {  // one aligned 16-byte load per node on the device
+        v4.resize((size_t)nn);
+        for (long long i = 0; i < nn; i++)
+            v4[i] = make_float4(pd->velocity[3 * i], pd->velocity[3 * i + 1], pd->velocity[3 * i + 2], 0.0f);
+        PRR_CK(ctx, cudaMemcpyAsync(G.vel.p, v4.data(), (size_t)nn * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    PRR_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    G.nx = pd->nx; G.ny = pd->ny; G.nz = pd->nz;
+    for (int k = 0; k < 3; k++) { G.lo[k] = pd->lo[k]; G.hi[k] = pd->hi[k]; }
+    G.has_theta = pd->temperature != nullptr;
+    G.has_vel = pd->velocity != nullptr;
+    G.present = true;
     return PRR_OK;
 }
 

@@ -253,6 +253,27 @@ prr_status prr_deck_frame(const prr_deck *d, int frame, prr_frame_desc *out, cha
     else if (metric.size() > 3 && metric.compare(metric.size() - 3, 3, ".so") == 0)
         f.metric = PRR_METRIC_PLUGIN0;  // a metric plug-in library: prr_run_deck loads it and sets the id
     else { put_err(errbuf, errlen, "unknown spacetime metric '" + metric + "' (flat, schwarzschild, kerr, or a plug-in .so)"); return PRR_ERR_INVALID; }
+    // ---- plasma emission (the plasma fields main/Spacetime.h:50-51 declares;
+    //      keys of this library, PHYSICAL mode, prr_emission_desc) ----
+    std::string emis = par(d, "spacetime", "emission");
+    if (emis.empty() || emis == "none") f.emission = PRR_EMISSION_NONE;
+    else if (emis == "disk") f.emission = PRR_EMISSION_DISK;
+    else if (emis == "grid") {
+        put_err(errbuf, errlen, "grid emission takes its plasma from prr_upload_plasma, not from a deck");
+        return PRR_ERR_UNSUPPORTED;
+    } else { put_err(errbuf, errlen, "unknown spacetime emission '" + emis + "' (none, disk)"); return PRR_ERR_INVALID; }
+    f.emis.index = parf(d, "spacetime", "emisIndex", f.emis.index);
+    f.emis.height = parf(d, "spacetime", "emisHeight", f.emis.height);
+    f.emis.r_in = parf(d, "spacetime", "emisRin", f.emis.r_in);
+    f.emis.r_out = parf(d, "spacetime", "emisRout", f.emis.r_out);
+    f.emis.spectral_index = parf(d, "spacetime", "emisAlpha", f.emis.spectral_index);
+    f.emis.absorb = parf(d, "spacetime", "emisAbsorb", f.emis.absorb);
+    f.emis.gain = parf(d, "spacetime", "emisGain", f.emis.gain);
+    if (has_key(d, "spacetime", "emisSense")) f.emis.sense = pari(d, "spacetime", "emisSense");
+    std::string cmap = par(d, "spacetime", "emisMap");
+    if (cmap.empty() || cmap == "afmhot") f.emis.colormap = PRR_CMAP_AFMHOT;
+    else if (cmap == "grey") f.emis.colormap = PRR_CMAP_GREY;
+    else { put_err(errbuf, errlen, "unknown emission colour map '" + cmap + "' (afmhot, grey)"); return PRR_ERR_INVALID; }
     // ---- tracer (prr.cpp:184-190) ----
     std::string solver = par(d, "tracer", "solver");
     if (solver == "euler") f.solver = PRR_SOLVER_EULER;

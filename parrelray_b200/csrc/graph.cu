@@ -88,6 +88,7 @@ prr_status record(prr_graph *g, cudaStream_t st)
     a.compaction_interval = g->cfg.compaction_interval;
     a.watchdog_cycles = ctx->watchdog_cycles;
     a.rays_per_thread = g->cfg.rays_per_thread;
+    a.emission = plan.any_emission;
     a.image = (float *)g->image.p;
     float *image = (float *)g->image.p;
     if (plan.precision == PRR_PREC_SPLIT) {
@@ -157,7 +158,7 @@ extern "C" prr_status prr_graph_create(prr_ctx *ctx, const prr_frame_desc *frame
     g->d_rgb8 = d_rgb8;
     g->d_rgbf = d_rgbf;
     g->cfg = ctx->cfg;
-    g->bpsm = resolve_bpsm(ctx, plan.precision);
+    g->bpsm = resolve_bpsm(ctx, plan.precision, plan.any_emission);
     if ((s = galloc(g, g->frames, nf * sizeof(FrameParams), "frame parameters")) != PRR_OK ||
         (s = galloc(g, g->frame_begin, (nf + 1) * sizeof(long long), "frame table")) != PRR_OK ||
         (s = galloc(g, g->counters, C_COUNT * sizeof(unsigned long long), "counters")) != PRR_OK ||

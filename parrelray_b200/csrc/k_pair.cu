@@ -14,6 +14,9 @@
 // FP64 pass), and rays near a photon orbit (near_critical, tested before
 // the first attempt) or that dip below fp64_rfac * r_+ are queued for
 // k_fp64_requeue (k_persistent.cu).
+//
+// EMIS (RPT = 1, not SPLIT): plasma emission (emission.cuh) accumulated at
+// every accepted step of frames that have it, composited into the colour.
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -51,6 +54,7 @@ struct Slot {
     float flag_r;  // split precision: queue the ray for FP64 below this radius
     PhysRay<float> R;
     Hot<float> q;
+    EmisRay<float> E;  // emission kernels only
 };
 
 struct Counts {
@@ -87,10 +91,11 @@ __device__ __forceinline__ bool flag_ray(const PersistentArgs &a, Slot &sl, Coun
 
 // A finished ray of slot `sl`: counters, SSAA accumulation, next sample or
 // pixel output.  Returns true when the slot's pixel is complete.
-template <bool SPLIT>
+template <bool SPLIT, bool EMIS>
 __device__ __forceinline__ bool finish_ray(const PersistentArgs &a, Slot &sl, int result, V3<float> col, Counts &c)
 {
     const FrameParams &fp = a.frames[sl.frame];
+    if constexpr (EMIS) col = emis_colour<float>(fp, sl.E, col);
     c.att += (unsigned)sl.R.i;
     c.acc += (unsigned)sl.R.accepted;
     c.rays++;
@@ -137,6 +142,7 @@ __device__ __forceinline__ bool finish_ray(const PersistentArgs &a, Slot &sl, in
     sl.s += 1;
     if (sl.s < sl.S) {
         phys_init<float>(fp, sl.px, sl.py, sl.s, sl.R);
+        if constexpr (EMIS) emis_init<float>(fp, sl.R.x, sl.R.u, sl.E);
         return false;
     }
     float o0 = sl.acc0, o1 = sl.acc1, o2 = sl.acc2;
@@ -147,7 +153,7 @@ __device__ __forceinline__ bool finish_ray(const PersistentArgs &a, Slot &sl, in
     return true;
 }
 
-template <bool SPLIT>
+template <bool SPLIT, bool EMIS>
 __device__ __forceinline__ void start_pixel(const PersistentArgs &a, Slot &sl, long long it)
 {
     sl.frame = find_frame2(a.frame_pix_begin, a.nframes, it);
@@ -161,6 +167,7 @@ __device__ __forceinline__ void start_pixel(const PersistentArgs &a, Slot &sl, l
     sl.q = make_hot<float>(fp);
     sl.flag_r = SPLIT ? fp.fp64_rfac * kerr_r_plus<float>(sl.q.M, sl.q.a) : -1.f;
     phys_init<float>(fp, sl.px, sl.py, 0, sl.R);
+    if constexpr (EMIS) emis_init<float>(fp, sl.R.x, sl.R.u, sl.E);
     sl.busy = true;
 }
 
@@ -201,10 +208,11 @@ template <> __device__ __forceinline__ void load_in<float2>(pv::StageIn<float2> 
 // least) cap the registers per thread.  One-slot threads in CTAs of up to 64
 // threads use the instantiation capped at 127 registers (8 CTAs = 16 warps
 // per SM, no spills; 4 % faster than 141 registers and 12 warps).
-template <int RPT, int MAXT, int MINB, bool SPLIT>
+template <int RPT, int MAXT, int MINB, bool SPLIT, bool EMIS>
 __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
 {
     static_assert(!SPLIT || RPT == 1, "split precision runs one ray per thread");
+    static_assert(!EMIS || (RPT == 1 && !SPLIT), "emission runs one FP32 ray per thread");
     using V = typename std::conditional<RPT == 2, float2, float>::type;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -246,7 +254,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
                     if (sl[j].need) {
                         const long long it = (long long)base + off + __popc(m[j] & lt);
                         sl[j].need = false;
-                        if (it < a.total_pixels) start_pixel<SPLIT>(a, sl[j], it);
+                        if (it < a.total_pixels) start_pixel<SPLIT, EMIS>(a, sl[j], it);
                         else sl[j].busy = false;
                     }
                     off += __popc(m[j]);
@@ -283,7 +291,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
             if (SPLIT && sl[j].R.i == 0 && near_critical<float>(a.frames[sl[j].frame], sl[j].R)) {
                 if (flag_ray(a, sl[j], cnt)) { sl[j].busy = false; sl[j].need = true; }
             } else if (phys_precheck<float>(sl[j].R, result, col) == STEP_DONE) {
-                if (finish_ray<SPLIT>(a, sl[j], result, col, cnt)) { sl[j].busy = false; sl[j].need = true; }
+                if (finish_ray<SPLIT, EMIS>(a, sl[j], result, col, cnt)) { sl[j].busy = false; sl[j].need = true; }
             } else {
                 go[j] = true;
             }
@@ -314,9 +322,9 @@ __global__ void __launch_bounds__(MAXT, MINB) k_pair(PersistentArgs a)
             int result = 0;
             V3<float> col;
             const int st = phys_accept<float>(fp, sl[j].q, sl[j].R, dxv, duv, pv::get(out.err, j), pv::get(out.hn, j),
-                                              result, col, SPLIT ? sl[j].flag_r : -1.0f, nullptr);
+                                              result, col, SPLIT ? sl[j].flag_r : -1.0f, nullptr, EMIS ? &sl[j].E : nullptr);
             if (st == STEP_CONTINUE) continue;
-            const bool done = (SPLIT && st == STEP_FLAG64) ? flag_ray(a, sl[j], cnt) : finish_ray<SPLIT>(a, sl[j], result, col, cnt);
+            const bool done = (SPLIT && st == STEP_FLAG64) ? flag_ray(a, sl[j], cnt) : finish_ray<SPLIT, EMIS>(a, sl[j], result, col, cnt);
             if (done) { sl[j].busy = false; sl[j].need = true; }
         }
     }
@@ -335,26 +343,39 @@ cudaError_t launch_pair(const PersistentArgs &a, int rpt, bool split, int block,
 {
     if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
     if (split && (rpt != 1 || !a.sample_rgb || !a.fp64_queue)) return cudaErrorInvalidValue;
+    if (a.emission && split) return cudaErrorInvalidValue;
     int grid = nsm * blocks_per_sm;
     if (grid < 1) grid = 1;
-    if (split && block <= 64) k_pair<1, 64, 8, true><<<grid, block, 0, st>>>(a);
-    else if (split) k_pair<1, 256, 1, true><<<grid, block, 0, st>>>(a);
-    else if (rpt == 2) k_pair<2, 256, 1, false><<<grid, block, 0, st>>>(a);
-    else if (rpt == 1 && block <= 64) k_pair<1, 64, 8, false><<<grid, block, 0, st>>>(a);
-    else if (rpt == 1) k_pair<1, 256, 1, false><<<grid, block, 0, st>>>(a);
-    else return cudaErrorInvalidValue;
+    const bool small = block <= 64;
+    if (a.emission) {
+        if (small) k_pair<1, 64, 8, false, true><<<grid, block, 0, st>>>(a);
+        else k_pair<1, 256, 1, false, true><<<grid, block, 0, st>>>(a);
+    } else if (split) {
+        if (small) k_pair<1, 64, 8, true, false><<<grid, block, 0, st>>>(a);
+        else k_pair<1, 256, 1, true, false><<<grid, block, 0, st>>>(a);
+    } else if (rpt == 2) {
+        k_pair<2, 256, 1, false, false><<<grid, block, 0, st>>>(a);
+    } else if (rpt == 1) {
+        if (small) k_pair<1, 64, 8, false, false><<<grid, block, 0, st>>>(a);
+        else k_pair<1, 256, 1, false, false><<<grid, block, 0, st>>>(a);
+    } else {
+        return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
-int pair_occupancy(int rpt, bool split, int block)
+int pair_occupancy(int rpt, bool split, int block, bool emission)
 {
     int n = 0;
+    const bool small = block <= 64;
     cudaError_t e;
-    if (split) e = block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, true>, block, 0)
-                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, true>, block, 0);
-    else if (rpt == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<2, 256, 1, false>, block, 0);
-    else e = block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, false>, block, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, false>, block, 0);
+    if (emission) e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, false, true>, block, 0)
+                            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, false, true>, block, 0);
+    else if (split) e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, true, false>, block, 0)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, true, false>, block, 0);
+    else if (rpt == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<2, 256, 1, false, false>, block, 0);
+    else e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, false, false>, block, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, false, false>, block, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
 }

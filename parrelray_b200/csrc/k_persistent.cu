@@ -77,7 +77,9 @@ __device__ __forceinline__ void write_state(O *st, long long rid, const PhysRay<
 #define PRR_PERSISTENT_MINB 1
 #endif
 
-template <class T, int GEOD>
+// EMIS: plasma emission (emission.cuh) accumulated at every accepted step of
+// frames that have it, composited into the colour.
+template <class T, int GEOD, bool EMIS>
 __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_persistent(PersistentArgs a)
 {
     const int lane = threadIdx.x & 31;
@@ -87,6 +89,7 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
     bool busy = false, need = true;
     PhysRay<T> R;
     Hot<T> q;
+    EmisRay<T> E;
     LaneCounts cnt;
     const long long t0 = clock64();
     unsigned iter = 0;
@@ -119,6 +122,7 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
                     acc0 = acc1 = acc2 = 0.f;
                     q = make_hot<T>(fp);
                     phys_init<T>(fp, px, py, 0, R, uv);
+                    if (EMIS) emis_init<T>(fp, R.x, R.u, E);
                     busy = true;
                 } else {
                     busy = false;
@@ -143,8 +147,9 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
         const FrameParams &fp = a.frames[frame];
         int result = 0;
         V3<float> col;
-        const int st = phys_attempt<T, GEOD>(fp, q, R, result, col, (T)-1);
+        const int st = phys_attempt<T, GEOD>(fp, q, R, result, col, (T)-1, nullptr, EMIS ? &E : nullptr);
         if (st == STEP_CONTINUE) continue;
+        if (EMIS) col = emis_colour<T>(fp, E, col);
 
         cnt.att += (unsigned)R.i;
         cnt.acc += (unsigned)R.accepted;
@@ -167,6 +172,7 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
         s += 1;
         if (s < S) {
             phys_init<T>(fp, px, py, s, R, uv);
+            if (EMIS) emis_init<T>(fp, R.x, R.u, E);
             continue;
         }
         if (S > 1) { acc0 = sqrtf(acc0 / (float)S); acc1 = sqrtf(acc1 / (float)S); acc2 = sqrtf(acc2 / (float)S); }
@@ -233,32 +239,40 @@ __global__ void __launch_bounds__(128) k_fp64_requeue(PersistentArgs a)
     cnt.flush(a.counters);
 }
 
-template <class T, int GEOD>
+template <class T, int GEOD, bool EMIS>
 static cudaError_t launch_one(const PersistentArgs &a, int block, int blocks_per_sm, int nsm, cudaStream_t st)
 {
     int grid = nsm * blocks_per_sm;
     if (grid < 1) grid = 1;
-    k_persistent<T, GEOD><<<grid, block, 0, st>>>(a);
+    k_persistent<T, GEOD, EMIS><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st)
 {
     if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
-    if (precision == PRR_PREC_FP64) return launch_one<double, 0>(a, block, blocks_per_sm, nsm, st);
+    if (precision == PRR_PREC_FP64) {
+        if (a.emission) return launch_one<double, 0, true>(a, block, blocks_per_sm, nsm, st);
+        return launch_one<double, 0, false>(a, block, blocks_per_sm, nsm, st);
+    }
     if (precision == PRR_PREC_SPLIT) return launch_pair(a, 1, true, block, blocks_per_sm, nsm, st);
-    if (a.geod_table) return launch_one<float, 1>(a, block, blocks_per_sm, nsm, st);
+    if (a.geod_table) {
+        if (a.emission) return cudaErrorInvalidValue;  // emission runs with the register contraction
+        return launch_one<float, 1, false>(a, block, blocks_per_sm, nsm, st);
+    }
     return launch_pair(a, a.rays_per_thread == 2 ? 2 : 1, false, block, blocks_per_sm, nsm, st);
 }
 
-int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread)
+int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread, int emission)
 {
     int n = 0;
     cudaError_t e;
-    if (precision == PRR_PREC_FP64) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<double, 0>, block, 0);
+    if (precision == PRR_PREC_FP64)
+        e = emission ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<double, 0, true>, block, 0)
+                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<double, 0, false>, block, 0);
     else if (precision == PRR_PREC_SPLIT) return pair_occupancy(1, true, block);
-    else if (geod_table) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 1>, block, 0);
-    else return pair_occupancy(rays_per_thread == 2 ? 2 : 1, false, block);
+    else if (geod_table) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 1, false>, block, 0);
+    else return pair_occupancy(rays_per_thread == 2 ? 2 : 1, false, block, emission != 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
 }

@@ -57,6 +57,7 @@ struct PersistentArgs {
     long long watchdog_cycles;   // 0 = off
     int rays_per_thread;         // FP32: pixel slots in flight per thread (1 or 2; 0 = 1)
     int *ray_steps;              // optional: accepted steps per ray (FP64/table/split kernels, single frame)
+    int emission;                // 1 = some frame has plasma emission (the kernels with emission.cuh)
 };
 // Dispatches to the kernel of the precision: FP32 with the register
 // contraction and the FP32 pass of SPLIT -> k_pair (k_pair.cu,
@@ -65,13 +66,13 @@ struct PersistentArgs {
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st);
 
 // k_persistent.cu: resident CTAs per SM of the kernel launch_persistent picks.
-int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread = 1);
+int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread = 1, int emission = 0);
 
 // k_pair.cu: the FP32 renderer with `rpt` pixel slots per thread; `split`:
 // the FP32 pass of a split-precision render (rpt 1; needs sample_rgb and
-// fp64_queue).
+// fp64_queue); a.emission: the instantiation with plasma emission (rpt 1).
 cudaError_t launch_pair(const PersistentArgs &a, int rpt, bool split, int block, int blocks_per_sm, int nsm, cudaStream_t st);
-int pair_occupancy(int rpt, bool split, int block);
+int pair_occupancy(int rpt, bool split, int block, bool emission = false);
 
 // k_persistent.cu: FP64 re-integration of the queued rays of a split render.
 cudaError_t launch_fp64_requeue(const PersistentArgs &a, int block, int nsm, cudaStream_t st);

@@ -142,8 +142,9 @@ extern "C" prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, co
     a.rgb8 = d_rgb8;
     a.counters = counters;
     a.compaction_interval = 1;
+    a.emission = plan.any_emission;
     const int block = 128;
-    int bpsm = persistent_occupancy(plan.precision, 0, block);
+    int bpsm = persistent_occupancy(plan.precision, 0, block, 1, plan.any_emission);
     if (e == cudaSuccess) e = launch_persistent(a, plan.precision, block, bpsm > 0 ? bpsm : 1, nsm, st);
     for (int f = 0; f < n && e == cudaSuccess; f++) {
         const FrameParams &p = plan.fp[f];

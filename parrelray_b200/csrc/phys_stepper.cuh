@@ -22,6 +22,7 @@
 // compensation.  The two sphere tests of an accepted step (User_UPDATE with
 // the step h, User_ENDLOOP with the next step) share one geometry pass.
 #pragma once
+#include "emission.cuh"
 #include "geod_table.cuh"
 #include "prr_device.cuh"
 
@@ -185,6 +186,8 @@ enum StepStatus { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_FLAG64 = 2 };
 // hit_sphere: when non-null, an INTERSECTION stores the hit sphere's index
 // there and leaves the final state in R (otherwise R.u receives the colour,
 // as User_ENDLOOP does).
+// em: when non-null, every accepted step adds its plasma emission
+// (emission.cuh) before the termination tests.
 // An attempt is split in three parts so the FP32 path can evaluate the
 // stages of two rays at once (phys_pair.cuh): phys_precheck (caps before
 // the attempt), the stages (increments dxv/duv, scaled error err and next
@@ -201,11 +204,11 @@ template <class T> PRR_DEV int phys_precheck(PhysRay<T> &R, int &result, V3<floa
 
 template <class T>
 PRR_DEV int phys_accept(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, const T dxv[4], const T duv[4], T err,
-                        T hn, int &result, V3<float> &colour, T flag_r, int *hit_sphere);
+                        T hn, int &result, V3<float> &colour, T flag_r, int *hit_sphere, EmisRay<T> *em = nullptr);
 
 template <class T, int GEOD>
 PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, int &result, V3<float> &colour,
-                         T flag_r, int *hit_sphere = nullptr)
+                         T flag_r, int *hit_sphere = nullptr, EmisRay<T> *em = nullptr)
 {
     using F = Fehlberg;
     if (phys_precheck<T>(R, result, colour) == STEP_DONE) return STEP_DONE;
@@ -280,12 +283,12 @@ PRR_DEV int phys_attempt(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, 
 #undef PRR_FIN
     T hn = (T)0.9 * h * fpow<T>(err, (T)-0.2);
     hn = fmin(fmax(hn, q.hmin), q.hmax);
-    return phys_accept<T>(fp, q, R, dxv, duv, err, hn, result, colour, flag_r, hit_sphere);
+    return phys_accept<T>(fp, q, R, dxv, duv, err, hn, result, colour, flag_r, hit_sphere, em);
 }
 
 template <class T>
 PRR_DEV int phys_accept(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, const T dxv[4], const T duv[4], T err,
-                        T hn, int &result, V3<float> &colour, T flag_r, int *hit_sphere)
+                        T hn, int &result, V3<float> &colour, T flag_r, int *hit_sphere, EmisRay<T> *em)
 {
     const T h = R.h;
     if (R.intersect && R.i > 10000) R.intersect = 0;
@@ -327,6 +330,7 @@ PRR_DEV int phys_accept(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, c
     }
     R.x = xn; R.u = un; R.cx = cxn; R.cu = cun;
     R.accepted += 1;
+    if (em) emis_step<T>(fp, q.M, q.a, xn, un, h, *em);
     int candE;
     T dE;
     if (!hitU) {

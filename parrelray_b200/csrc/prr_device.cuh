@@ -100,6 +100,23 @@ struct DevSphere {
 
 // Everything a kernel needs about one frame, prepared on the host from a
 // prr_frame_desc.
+// The plasma grid of prr_upload_plasma on the device (nodes x-fastest).
+struct DevPlasma {
+    const float *n;       // density
+    const float *theta;   // temperature (nullptr: 1)
+    const float4 *vel;    // coordinate velocity (vx, vy, vz, 0) (nullptr: the DISK flow)
+    int nx, ny, nz;
+    float lo[3], inv[3];  // box corner and (n - 1) / (hi - lo) per axis
+};
+
+// prr_emission_desc plus the grid, for one frame.
+struct EmisParams {
+    int kind;             // prr_emission
+    int sense, cmap;
+    float index, height, r_in, r_out, spectral, absorb, gain, temp_power;
+    DevPlasma grid;
+};
+
 struct FrameParams {
     int width, height, samples, ssaa, nsub;
     float vfov, cam[3], alpha, beta;
@@ -118,6 +135,7 @@ struct FrameParams {
     unsigned ssaa_seed;   // RANDOM / JITTERED offsets
     float cfwd[3], cright[3], cup[3];  // Camera::computeVectors basis (PINHOLE, PANORAMA)
     float tan_half;       // tanf(vfov / 2) (PINHOLE)
+    EmisParams em;        // em.kind == PRR_EMISSION_NONE: no plasma
     DevSphere sph[PRR_MAX_SPHERES];
     long long ray_begin;  // first ray (work) index of this frame in a batch
     long long pix_begin;  // first output pixel of this frame in a batch

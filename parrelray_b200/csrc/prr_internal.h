@@ -21,6 +21,15 @@ struct TexSlot {
     int w = 0, h = 0;
 };
 
+// The plasma grid of prr_upload_plasma (density, temperature and velocity as
+// float4 per node, each on the device; the last two optional).
+struct PlasmaGrid {
+    DevBuf n, theta, vel;
+    bool present = false, has_theta = false, has_vel = false;
+    int nx = 0, ny = 0, nz = 0;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+};
+
 // A loaded metric plug-in library (compat/prr_plugin.cuh).
 struct MetricPlugin {
     std::string path, name;
@@ -38,6 +47,7 @@ struct prr_ctx {
     cudaEvent_t e0 = nullptr, e1 = nullptr, t0 = nullptr, t1 = nullptr;
     std::string err;
     TexSlot tex[PRR_MAX_TEXTURES];
+    PlasmaGrid plasma;
     int schedule = PRR_SCHED_PERSISTENT;
     prr_launch_config cfg{};
     int geod_table = -1;  // -1: per schedule (PERSISTENT contraction, PLAIN table); 0: contraction; 1: table
@@ -53,7 +63,7 @@ struct prr_ctx {
     std::vector<DevBuf *> all_buffers()
     {
         return {&frames, &frame_begin, &counters, &image, &sample_rgb, &rays, &queue, &state, &out_u8, &out_f, &scratch,
-                &adj_ckpt, &adj_dl, &adj_sort};
+                &adj_ckpt, &adj_dl, &adj_sort, &plasma.n, &plasma.theta, &plasma.vel};
     }
 };
 
@@ -67,6 +77,7 @@ struct RenderPlan {
     int mode = PRR_MODE_PHYSICAL;
     int precision = PRR_PREC_FP32;
     bool any_fxaa = false;
+    bool any_emission = false;  // some frame has plasma emission
 };
 
 // The plug-in of a frame's metric id, or null for a built-in metric.
@@ -86,4 +97,4 @@ prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, doub
 prr_status collect_stats(prr_ctx *ctx, const RenderPlan &plan, prr_stats *stats);
 // Resident CTAs per SM of the persistent kernel under the context's launch
 // configuration (its blocks_per_sm, or the occupancy limit when that is 0).
-int resolve_bpsm(prr_ctx *ctx, int precision);
+int resolve_bpsm(prr_ctx *ctx, int precision, bool emission = false);

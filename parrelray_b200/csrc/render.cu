@@ -69,12 +69,59 @@ void camera_basis(float a, float b, float fwd[3], float right[3], float up[3])
     nrm(right);
 }
 
+// Validates a frame's emission block and fills its device parameters
+// (prr_emission_desc in include/prr.h).
+prr_status emission_params(prr_ctx *ctx, int f, const prr_frame_desc &d, EmisParams &em)
+{
+    memset(&em, 0, sizeof(em));
+    em.kind = PRR_EMISSION_NONE;
+    if (d.emission == PRR_EMISSION_NONE) return PRR_OK;
+    if (d.emission != PRR_EMISSION_DISK && d.emission != PRR_EMISSION_GRID) return bad(ctx, f, "unknown emission model (none, disk, grid)");
+    if (d.mode != PRR_MODE_PHYSICAL) return bad(ctx, f, "emission renders in PHYSICAL mode");
+    if (d.precision != PRR_PREC_FP32 && d.precision != PRR_PREC_FP64) return bad(ctx, f, "emission renders in FP32 or FP64");
+    const prr_emission_desc &e = d.emis;
+    if (!(e.r_in >= 0.0f) || !(e.r_out > e.r_in) || !std::isfinite(e.r_out)) return bad(ctx, f, "emission needs 0 <= r_in < r_out (finite)");
+    if (d.emission == PRR_EMISSION_DISK && (!(e.r_in > 0.0f) || !finite_pos(e.height) || !std::isfinite(e.index)))
+        return bad(ctx, f, "disk emission needs r_in > 0, height > 0 and a finite index");
+    if (!std::isfinite(e.spectral_index) || !std::isfinite(e.temp_power)) return bad(ctx, f, "emission exponents must be finite");
+    if (!(e.absorb >= 0.0f) || !std::isfinite(e.absorb) || !(e.gain >= 0.0f) || !std::isfinite(e.gain))
+        return bad(ctx, f, "emission needs finite absorb >= 0 and gain >= 0");
+    if (e.sense != 1 && e.sense != -1) return bad(ctx, f, "emission sense must be +1 (co-rotating) or -1");
+    if (e.colormap != PRR_CMAP_AFMHOT && e.colormap != PRR_CMAP_GREY) return bad(ctx, f, "unknown emission colour map");
+    if (d.emission == PRR_EMISSION_GRID && !ctx->plasma.present) return bad(ctx, f, "grid emission needs a plasma grid (prr_upload_plasma)");
+    // nu_cam is measured by a static observer at the camera: g_tt = f - 1 < 0 there
+    const double M = d.metric == PRR_METRIC_FLAT ? 0.0 : d.mass, a = d.metric == PRR_METRIC_KERR ? d.spin : 0.0;
+    const double x = d.cam_pos[0], y = d.cam_pos[1], z = d.cam_pos[2];
+    const double b = x * x + y * y + z * z - a * a;
+    const double r = std::sqrt(0.5 * (b + std::sqrt(b * b + 4.0 * a * a * z * z)));
+    const double fc = M > 0.0 ? 2.0 * M * r * r * r / (r * r * r * r + a * a * z * z) : 0.0;
+    if (!(fc < 1.0)) return bad(ctx, f, "emission needs the camera outside the ergoregion (a static observer there)");
+    em.kind = d.emission;
+    em.sense = e.sense;
+    em.cmap = e.colormap;
+    em.index = e.index; em.height = e.height; em.r_in = e.r_in; em.r_out = e.r_out;
+    em.spectral = e.spectral_index; em.absorb = e.absorb; em.gain = e.gain; em.temp_power = e.temp_power;
+    if (d.emission == PRR_EMISSION_GRID) {
+        const PlasmaGrid &G = ctx->plasma;
+        em.grid.n = (const float *)G.n.p;
+        em.grid.theta = G.has_theta ? (const float *)G.theta.p : nullptr;
+        em.grid.vel = G.has_vel ? (const float4 *)G.vel.p : nullptr;
+        em.grid.nx = G.nx; em.grid.ny = G.ny; em.grid.nz = G.nz;
+        const int nn[3] = {G.nx, G.ny, G.nz};
+        for (int k = 0; k < 3; k++) {
+            em.grid.lo[k] = G.lo[k];
+            em.grid.inv[k] = (float)(nn[k] - 1) / (G.hi[k] - G.lo[k]);
+        }
+    }
+    return PRR_OK;
+}
+
 }  // namespace
 
-int resolve_bpsm(prr_ctx *ctx, int precision)
+int resolve_bpsm(prr_ctx *ctx, int precision, bool emission)
 {
     if (ctx->cfg.blocks_per_sm > 0) return ctx->cfg.blocks_per_sm;
-    int b = persistent_occupancy(precision, ctx->geod_table == 1, ctx->cfg.block_size, ctx->cfg.rays_per_thread);
+    int b = persistent_occupancy(precision, ctx->geod_table == 1, ctx->cfg.block_size, ctx->cfg.rays_per_thread, emission);
     return b > 0 ? b : 1;
 }
 
@@ -87,6 +134,7 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
     plan.mode = frames[0].mode;
     plan.precision = frames[0].precision;
     plan.any_fxaa = false;
+    plan.any_emission = false;
     for (int f = 0; f < n; f++) {
         const prr_frame_desc &d = frames[f];
         FrameParams &p = plan.fp[f];
@@ -166,6 +214,9 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
         p.fp64_delta = d.precision == PRR_PREC_SPLIT ? d.fp64_delta : 0.0f;
         p.fp64_rfac = d.precision == PRR_PREC_SPLIT ? d.fp64_rfac : 0.0f;
         p.nspheres = d.nspheres;
+        prr_status es = emission_params(ctx, f, d, p.em);
+        if (es != PRR_OK) return es;
+        if (p.em.kind != PRR_EMISSION_NONE) plan.any_emission = true;
         long long npx = (long long)d.width * d.height;
         p.pix_begin = plan.pix_begin[f];
         p.ray_begin = plan.ray_begin[f];
@@ -208,12 +259,26 @@ static PersistentArgs persistent_args(prr_ctx *ctx, const RenderPlan &plan)
     a.watchdog_cycles = ctx->watchdog_cycles;
     a.rays_per_thread = ctx->cfg.rays_per_thread;
     a.ray_steps = ctx->ray_steps_out;
+    a.emission = plan.any_emission;
     return a;
+}
+
+// Emission runs on the persistent kernels with the register contraction.
+static prr_status check_emission_schedule(prr_ctx *ctx, const RenderPlan &plan)
+{
+    if (!plan.any_emission) return PRR_OK;
+    if (ctx->schedule == PRR_SCHED_PLAIN || ctx->geod_table == 1) {
+        ctx->err = "emission renders on the persistent schedule with the register contraction";
+        return PRR_ERR_UNSUPPORTED;
+    }
+    return PRR_OK;
 }
 
 prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float *d_rgbf, cudaStream_t st, bool timed)
 {
-    prr_status s = upload_plan(ctx, plan, st);
+    prr_status s = check_emission_schedule(ctx, plan);
+    if (s != PRR_OK) return s;
+    s = upload_plan(ctx, plan, st);
     if (s != PRR_OK) return s;
     const int n = (int)plan.fp.size();
     unsigned long long *counters = (unsigned long long *)ctx->counters.p;
@@ -267,7 +332,7 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
         trace_timed = timed;
         PersistentArgs a = persistent_args(ctx, plan);
         a.image = image;
-        const int bpsm = resolve_bpsm(ctx, plan.precision);
+        const int bpsm = resolve_bpsm(ctx, plan.precision, plan.any_emission);
         if (plan.precision == PRR_PREC_SPLIT) {
             if ((s = alloc(ctx, ctx->sample_rgb, (size_t)plan.total_rays * 3 * sizeof(float), "per-sample colours")) != PRR_OK) return s;
             if ((s = alloc(ctx, ctx->queue, (size_t)plan.total_rays * sizeof(unsigned long long), "FP64 queue")) != PRR_OK) return s;
@@ -315,7 +380,9 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
 prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, double *h_state64, float *h_rgb)
 {
     cudaStream_t st = ctx->stream;
-    prr_status s = upload_plan(ctx, plan, st);
+    prr_status s = check_emission_schedule(ctx, plan);
+    if (s != PRR_OK) return s;
+    s = upload_plan(ctx, plan, st);
     if (s != PRR_OK) return s;
     const FrameParams &p = plan.fp[0];
     const long long nr = (long long)p.width * p.height * p.samples;
@@ -347,7 +414,7 @@ prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, doub
         if (h_state64) a.ray_state64 = (double *)ctx->state.p;
         else a.ray_state = (float *)ctx->state.p;
         int prec = plan.precision == PRR_PREC_FP64 ? PRR_PREC_FP64 : PRR_PREC_FP32;
-        PRR_CK(ctx, launch_persistent(a, prec, ctx->cfg.block_size, resolve_bpsm(ctx, prec), ctx->nsm, st));
+        PRR_CK(ctx, launch_persistent(a, prec, ctx->cfg.block_size, resolve_bpsm(ctx, prec, plan.any_emission), ctx->nsm, st));
         ctx->last_launches = 1;
     }
     PRR_CK(ctx, cudaEventRecord(ctx->e1, st));
@@ -416,10 +483,10 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
     const int blocks[3] = {64, 128, 256};
     const int intervals[3] = {8, 16, 32};
     // two pixel slots per thread only where the kernel has them (FP32, register contraction)
-    const int nrpt = (plan.precision == PRR_PREC_FP32 && ctx->geod_table != 1) ? 2 : 1;
+    const int nrpt = (plan.precision == PRR_PREC_FP32 && ctx->geod_table != 1 && !plan.any_emission) ? 2 : 1;
     for (int rpt = 1; rpt <= nrpt; rpt++)
         for (int bi = 0; bi < 3; bi++) {
-            const int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi], rpt);
+            const int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi], rpt, plan.any_emission);
             if (occ < 1) continue;
             for (int ii = 0; ii < 3; ii++) {
                 ctx->cfg.block_size = blocks[bi];
@@ -454,6 +521,7 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
     if (d.fxaa) { ctx->err = "prr_adjoint: FXAA is not differentiated; render the frame without FXAA"; return PRR_ERR_UNSUPPORTED; }
     if (sphere_index < -1 || sphere_index >= d.nspheres) { ctx->err = "prr_adjoint: sphere_index out of range"; return PRR_ERR_INVALID; }
     if (d.camera != PRR_CAMERA_SPHERICAL) { ctx->err = "prr_adjoint: differentiates the spherical camera model only"; return PRR_ERR_UNSUPPORTED; }
+    if (d.emission != PRR_EMISSION_NONE) { ctx->err = "prr_adjoint: differentiates frames without plasma emission only"; return PRR_ERR_UNSUPPORTED; }
     // orbit camera: position (r sin i, 0, r cos i), yaw pi, pitch i - pi/2
     double px = d.cam_pos[0], py = d.cam_pos[1], pz = d.cam_pos[2];
     double r = std::sqrt(px * px + py * py + pz * pz);

@@ -18,6 +18,10 @@ Workloads (all synthetic; the reference ships no textures):
   uneven_64           64 requests: log-uniform resolutions 256^2..2048x1024,
                       a ~ U[0, 0.998], r ~ U[8, 40], i ~ U[10, 89], tol 1e-7
   kerr_512_adjoint    Kerr 512x512, one sphere R=1 at orbit radius 9
+  eht_disk            Kerr a=0.94, r=50, i=17, FOV 27, pinhole, square frame, black
+                      sky, emission from a thick co-rotating disk (density
+                      ~ r^-3, Gaussian width 0.4 in cos theta, r_+ .. 20M,
+                      spectral index 0, gain 2) - an image like the EHT's M87*
 """
 from __future__ import annotations
 
@@ -86,6 +90,30 @@ def make_frame(width: int, height: int, *, r: float, incl_deg: float, fov_deg: f
         s.radius = rad
         s.texture_id = tex
     return d
+
+
+def set_emission(d: abi.FrameDesc, kind: int = abi.EMISSION_DISK, *, index: float = 2.0, height: float = 0.4,
+                 r_in: float = 2.0, r_out: float = 20.0, spectral_index: float = 0.0, absorb: float = 0.0,
+                 gain: float = 1.0, sense: int = 1, temp_power: float = 0.0,
+                 colormap: int = abi.CMAP_AFMHOT) -> abi.FrameDesc:
+    """Fills the frame's emission block (prr_emission_desc)."""
+    d.emission = kind
+    e = d.emis
+    e.index, e.height, e.r_in, e.r_out = index, height, r_in, r_out
+    e.spectral_index, e.absorb, e.gain, e.sense = spectral_index, absorb, gain, sense
+    e.temp_power, e.colormap = temp_power, colormap
+    return d
+
+
+def eht_disk(size: int = 1024, spin: float = 0.94, incl_deg: float = 17.0, r: float = 50.0, fov_deg: float = 27.0,
+             precision: int = abi.PREC_FP32, samples: int = 1, gain: float = 2.0, index: float = 3.0,
+             height: float = 0.4, **kw) -> abi.FrameDesc:
+    """Emission from a thick disk around a Kerr hole, seen almost face-on."""
+    d = make_frame(size, size, r=r, incl_deg=incl_deg, fov_deg=fov_deg, metric=abi.METRIC_KERR, spin=spin,
+                   precision=precision, samples=samples, background=False)
+    d.camera = abi.CAMERA_PINHOLE  # the spherical model compresses yaw by cos(pitch): near face-on it squashes the ring
+    rp = 1.0 + math.sqrt(1.0 - spin * spin)
+    return set_emission(d, abi.EMISSION_DISK, r_in=f32(rp), r_out=20.0, index=index, height=height, gain=gain, **kw)
 
 
 def orbit_point(radius: float, phase_deg: float) -> tuple[float, float, float]:

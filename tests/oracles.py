@@ -63,7 +63,49 @@ class Oracle:
                                         C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         lib.prr_oracle_metric.restype = None
         lib.prr_oracle_metric.argtypes = [C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.prr_oracle_trace_emission.restype = C.c_int
+        lib.prr_oracle_trace_emission.argtypes = [C.POINTER(abi.FrameDesc), _u8pp, _ip, _ip, C.c_int,
+                                                  C.POINTER(C.c_longlong), C.c_longlong, C.c_int, C.POINTER(C.c_double)]
+        lib.prr_oracle_set_plasma.restype = C.c_int
+        lib.prr_oracle_set_plasma.argtypes = [C.POINTER(abi.PlasmaDesc)]
         self.lib = lib
+        self._plasma_keep = None
+
+    def set_plasma(self, density=None, lo=None, hi=None, temperature=None, velocity=None) -> None:
+        """The plasma grid of GRID emission, as Context.upload_plasma takes it; no density clears it."""
+        if density is None:
+            self.lib.prr_oracle_set_plasma(None)
+            self._plasma_keep = None
+            return
+        n = np.ascontiguousarray(density, dtype=np.float32)
+        t = None if temperature is None else np.ascontiguousarray(temperature, dtype=np.float32)
+        v = None if velocity is None else np.ascontiguousarray(velocity, dtype=np.float32)
+        d = abi.PlasmaDesc()
+        d.nz, d.ny, d.nx = n.shape
+        d.lo[:] = [float(x) for x in lo]
+        d.hi[:] = [float(x) for x in hi]
+        fp = C.POINTER(C.c_float)
+        d.density = n.ctypes.data_as(fp)
+        d.temperature = t.ctypes.data_as(fp) if t is not None else None
+        d.velocity = v.ctypes.data_as(fp) if v is not None else None
+        if self.lib.prr_oracle_set_plasma(C.byref(d)):
+            raise ValueError("oracle rejected the plasma grid")
+        self._plasma_keep = (n, t, v)
+
+    def trace_emission(self, d: abi.FrameDesc, textures, precision: int = 0, ids=None, nthreads: int | None = None):
+        """(n, 3) float64 per ray: emission intensity I, transmittance, camera frequency nu_cam."""
+        tt = TexTable(textures)
+        if ids is None:
+            n, idp = d.nrays, None
+        else:
+            ids = np.ascontiguousarray(ids, dtype=np.int64)
+            n, idp = len(ids), ids.ctypes.data_as(C.POINTER(C.c_longlong))
+        out = np.zeros((n, 3), dtype=np.float64)
+        rc = self.lib.prr_oracle_trace_emission(C.byref(d), tt.ptrs, tt.w, tt.h, precision, idp, n,
+                                                nthreads or os.cpu_count(), out.ctypes.data_as(C.POINTER(C.c_double)))
+        if rc:
+            raise ValueError("oracle rejected the frame")
+        return out
 
     def trace(self, d: abi.FrameDesc, textures: dict[int, np.ndarray], precision: int = 0, ids=None,
               nthreads: int | None = None):

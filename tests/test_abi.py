@@ -22,12 +22,14 @@ def test_struct_layouts_match(built):
     assert lib.prr_sizeof(1) == C.sizeof(abi.Stats)
     assert lib.prr_sizeof(2) == C.sizeof(abi.LaunchConfig)
     assert lib.prr_sizeof(3) == C.sizeof(abi.Sphere)
+    assert lib.prr_sizeof(4) == C.sizeof(abi.EmissionDesc)
+    assert lib.prr_sizeof(5) == C.sizeof(abi.PlasmaDesc)
     assert lib.prr_sizeof(99) == 0
 
 
 def test_version_and_status_strings(built):
     lib = abi.load()
-    assert lib.prr_abi_version() == 2
+    assert lib.prr_abi_version() == 3
     assert lib.prr_status_string(abi.OK) == b"ok"
     assert b"device" in lib.prr_status_string(abi.ERR_NO_DEVICE)
 

@@ -197,6 +197,34 @@ def test_deck_options_and_unsupported_choices(built):
     assert e.value.status == abi.ERR_INVALID
 
 
+def test_deck_emission_keys(built):
+    """spacetime.emission (none, disk) and the emis* keys fill prr_emission_desc; grid takes its plasma from
+    prr_upload_plasma, so a deck asking for it is unsupported."""
+    base = ("_tracer_\n<solver> = <rkf>\n<mode> = <physical>\n<rout1> = <100>\n<h> = <0.01>\n<hmin> = <1e-4>\n"
+            "<hmax> = <0.1>\n<eps> = <1e-6>\n_spacetime_\n<hasBlackHole> = <1>\n<mass> = <1>\n<metric> = <kerr>\n"
+            "<spin> = <0.9>\n{emis}_camera_\n<vfov> = <30>\n<width> = <8>\n<height> = <8>\n<SSAA> = <none>\n"
+            "<SSAAsamples> = <1>\n_frame0_\n<x> = <50>\n<y> = <0>\n<z> = <0>\n<a> = <180>\n<b> = <0>\n")
+    f = Deck(text=base.format(emis="")).frame(0)
+    assert f.emission == abi.EMISSION_NONE
+    f = Deck(text=base.format(emis="<emission> = <disk>\n<emisIndex> = <3>\n<emisHeight> = <0.25>\n"
+                                   "<emisRin> = <1.5>\n<emisRout> = <25>\n<emisAlpha> = <0.7>\n<emisAbsorb> = <0.1>\n"
+                                   "<emisGain> = <4>\n<emisSense> = <-1>\n<emisMap> = <grey>\n")).frame(0)
+    e = f.emis
+    assert f.emission == abi.EMISSION_DISK
+    assert (e.index, e.height, e.r_in, e.r_out) == (3.0, np.float32(0.25), 1.5, 25.0)
+    assert (e.spectral_index, e.absorb, e.gain, e.sense, e.colormap) == (
+        np.float32(0.7), np.float32(0.1), 4.0, -1, abi.CMAP_GREY)
+    f = Deck(text=base.format(emis="<emission> = <disk>\n")).frame(0)  # defaults of prr_frame_desc_defaults
+    assert (f.emis.index, f.emis.sense, f.emis.colormap, f.emis.gain) == (2.0, 1, abi.CMAP_AFMHOT, 1.0)
+    with pytest.raises(PrrError) as e:
+        Deck(text=base.format(emis="<emission> = <grid>\n")).frame(0)
+    assert e.value.status == abi.ERR_UNSUPPORTED
+    for bad in ("<emission> = <plasma>\n", "<emission> = <disk>\n<emisMap> = <viridis>\n"):
+        with pytest.raises(PrrError) as e:
+            Deck(text=base.format(emis=bad)).frame(0)
+        assert e.value.status == abi.ERR_INVALID
+
+
 def test_missing_deck_file_is_an_io_error(built, tmp_path):
     with pytest.raises(PrrError) as e:
         Deck(tmp_path / "nope.params")
