@@ -9,7 +9,7 @@ from pathlib import Path
 
 import pytest
 
-from parrelray_b200 import build
+from parrelray_b200 import abi, build
 
 USER_HEADER = r"""
 #pragma once
@@ -61,7 +61,7 @@ def test_user_header_builds_unchanged(built, tmp_path):
     lib = _exports(out)
     assert lib.prr_plugin_name() == b"testflat"
     assert lib.prr_plugin_ray_bytes() == 48  # the reference's Ray layout (main/base.h:172-176)
-    assert lib.prr_plugin_abi_version() == 2
+    assert lib.prr_plugin_abi_version() == abi.load().prr_abi_version()  # plug-ins embed the frame layout
     assert h.read_text() == USER_HEADER  # the header itself is not touched
     assert not (build.BUILD / "plugins" / "testflat").exists()  # staging copy removed
 
