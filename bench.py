@@ -234,6 +234,40 @@ def bench_trajectory(ctx, torch, stream, plain_stride: int = 10):
     return res
 
 
+def bench_emission(ctx, torch, stream, size: int = 1024, reps: int = 3):
+    """Plasma emission: the EHT-like frame (Kerr a = 0.94, i = 17 deg, pinhole
+    camera, thick co-rotating disk, r_+ .. 20M) at size x size with 2x2 SSAA,
+    FP32, tolerance 1e-6, timed with CUDA events around `reps` renders; the
+    same frame with emission off (the cost of the emission hook); FP32 vs FP64
+    at 256x256 (pixels within 1/255)."""
+    from parrelray_b200 import abi, scenes
+
+    f = scenes.eht_disk(size, samples=4)
+    off = scenes.eht_disk(size, samples=4)
+    off.emission = abi.EMISSION_NONE
+    out8 = torch.empty(size * size * 3, dtype=torch.uint8, device="cuda")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = {"workload": f"eht_disk: Kerr a=0.94, i=17 deg, r=50M, pinhole FOV 27 deg, {size}x{size}, 2x2 SSAA, "
+                       "thick disk n ~ r^-3, FP32, tol 1e-6", "rays": f.nrays}
+    for name, fr in (("emission", f), ("no_emission", off)):
+        ctx.render_device(fr, out8.data_ptr(), stream=stream.cuda_stream)  # warm-up
+        ev0.record(stream)
+        for _ in range(reps):
+            ctx.render_device(fr, out8.data_ptr(), stream=stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / reps
+        res[name] = {"ms": ms, "mrays_s": fr.nrays / (ms * 1e-3) / 1e6}
+    st = ctx.render(f)[2]
+    res["emission"]["accepted_steps"] = int(st.accepted)
+    res["emission_overhead"] = res["emission"]["ms"] / res["no_emission"]["ms"]
+    a = ctx.render(scenes.eht_disk(256, samples=4))[0][0].astype(np.int32)
+    b = ctx.render(scenes.eht_disk(256, samples=4, precision=abi.PREC_FP64))[0][0].astype(np.int32)
+    d = np.abs(a - b).max(axis=-1)
+    res["fp32_vs_fp64_256"] = {"pixels_within_1_255": float(np.mean(d <= 1)), "max_abs_diff_255": int(d.max())}
+    return res
+
+
 def bench_uneven(ctx, torch, stream, textures, oracle_rays_per_request: int = 64, oracle_seconds: float = 10.0):
     """The 64-request workload (log-uniform 256x256..2048x1024, a ~ U[0, 0.998],
     r ~ U[8M, 40M], i ~ U[10, 89] deg, tolerance 1e-7) in one batched render
@@ -422,6 +456,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-trajectory", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--no-emission", action="store_true")
     ap.add_argument("--adjoint-size", type=int, default=512, help="side of the square differentiable-render frame")
     ap.add_argument("--adam", type=int, default=0, help="also run an N-iteration Adam fit of (a, i) (0: off)")
     ap.add_argument("--adam-lr", type=float, default=0.01)
@@ -585,6 +620,8 @@ def main():
             extra["trajectory"] = bench_trajectory(ctx, torch, stream)
         if not args.no_uneven and ws == 1:
             extra["uneven"] = bench_uneven(ctx, torch, stream, tex)
+        if not args.no_emission and ws == 1:
+            extra["emission"] = bench_emission(ctx, torch, stream)
         if not args.no_accuracy:
             f64 = build_frames(rank, ws, args.width, args.height)
             f64.precision = abi.PREC_FP64
