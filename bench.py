@@ -53,6 +53,25 @@ FLOPS_GEOD_KERR = 168
 F_ATTEMPT = 6 * FLOPS_GEOD_KERR + FLOPS_STAGES
 
 
+def reserve_stdout():
+    """Points file descriptor 1 at stderr for the rest of the run and returns
+    a stream on the original stdout: the result line is then the only line on
+    stdout, whatever the reference host build (whose solver prints with printf)
+    or a library writes."""
+    sys.stdout.flush()
+    fd = os.dup(1)
+    os.dup2(2, 1)
+    sys.stdout = sys.stderr
+    return os.fdopen(fd, "w", buffering=1)
+
+
+RESULT_OUT = sys.stdout
+
+
+def emit(line: dict) -> None:
+    print(json.dumps(line), file=RESULT_OUT, flush=True)
+
+
 def pair_kernel_name(cfg) -> str:
     """The FP32 renderer instantiation a launch shape selects (k_pair.cu: launch_pair)."""
     if cfg.rays_per_thread == 2:
@@ -414,7 +433,7 @@ def run_reference_arm(args):
     for it in range(args.warmup + args.steps):
         r = cpu_reference_sample(frame, tex, budget if it >= args.warmup else 2.0, nthreads)
         if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "reference host build (oracle/_ref) not built"}))
+            emit({"impl": "reference", "unavailable": "reference host build (oracle/_ref) not built"})
             return 0
         if it >= args.warmup:
             vals.append(r)
@@ -438,7 +457,7 @@ def run_reference_arm(args):
                                                  "not the workload's 1e-6"} if loose else None},
         "e2e": {"value": mr, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
 
 
@@ -469,6 +488,8 @@ def main():
                          "(default: prr_autotune on a quarter-size copy of the frame, outside the timed region)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global RESULT_OUT
+    RESULT_OUT = reserve_stdout()
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -652,7 +673,7 @@ def main():
             "e2e": e2e, "clocks": clocks, "gpu_launches": int(st.kernel_launches) * args.steps,
         }
         line.update(extra)
-        print(json.dumps(line), flush=True)
+        emit(line)
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
