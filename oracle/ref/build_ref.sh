@@ -16,12 +16,17 @@
 #   2. prr.cpp - rewrite each `k<<<grid, block>>>(args);` launch as
 #      `prr_ref_launch(grid, block, [&]{ k(args); });` (host emulation).
 #   3. main/metric.h - the reference's compile-time metric selection point;
-#      replaced by a switch over PRR_REF_METRIC_{SCHW,FLAT,CART,KERR}.  SCHW,
-#      FLAT and CART select the reference's own headers (CART: its alternative
-#      "schwarzschild - cart.cuh"); KERR selects the Kerr-Schild
-#      plug-in header shipped by this repository in the reference's plug-in
-#      shape (parrelray_b200/compat/metrics/kerr.cuh), since the reference's
-#      metrics/kerr.cuh is a stub whose hooks do not match the solver.
+#      replaced by a switch over PRR_REF_METRIC_{SCHW,FLAT,CART,SPH,KERR}.
+#      SCHW, FLAT, CART and SPH select the reference's own headers (CART: its
+#      alternative "schwarzschild - cart.cuh"; SPH: its spherical-coordinate
+#      "schwarzschild - sph.cuh", built with SPHERICAL defined); KERR selects
+#      the Kerr-Schild plug-in header shipped by this repository in the
+#      reference's plug-in shape (parrelray_b200/compat/metrics/kerr.cuh),
+#      since the reference's metrics/kerr.cuh is a stub whose hooks do not
+#      match the solver.
+#   4. kernels/solver.cuh:35 - the SPHERICAL branch of initRays assigns `u`
+#      without declaring it (declared only in the #else branch); the
+#      assignment becomes a declaration.  Without SPHERICAL nothing changes.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REPO="$(cd "$HERE/../.." && pwd)"
@@ -60,6 +65,16 @@ assert n == 7, f"prr.cpp: expected 7 kernel launches, rewrote {n}"
 open(p, "w", encoding="utf-8").write(s2)
 PY
 
+# 4. declare `u` in the SPHERICAL branch of initRays
+python3 - "$OUT/src/kernels/solver.cuh" <<'PY'
+import sys
+p = sys.argv[1]
+s = open(p, encoding="utf-8-sig").read()
+old = "#ifdef SPHERICAL\n\tu = f4(vel_cartTOspher("
+assert s.count(old) == 1, "solver.cuh: SPHERICAL initRays branch not found"
+open(p, "w", encoding="utf-8").write(s.replace(old, "#ifdef SPHERICAL\n\tf4 u = f4(vel_cartTOspher("))
+PY
+
 # 3. metric selection
 mkdir -p "$OUT/src/compat"
 cp "$REPO/parrelray_b200/compat/metrics/kerr.cuh" "$OUT/src/compat/kerr_plugin.cuh"
@@ -69,6 +84,8 @@ cat > "$OUT/src/main/metric.h" <<'EOF'
 #include "../metrics/flat.cuh"
 #elif defined(PRR_REF_METRIC_CART)
 #include "../metrics/schwarzschild - cart.cuh"
+#elif defined(PRR_REF_METRIC_SPH)
+#include "../metrics/schwarzschild - sph.cuh"
 #elif defined(PRR_REF_METRIC_KERR)
 #include "../compat/kerr_plugin.cuh"
 #else
@@ -80,8 +97,8 @@ EOF
 CXX="${PRR_ORACLE_CXX:-g++}"
 CXXFLAGS=(-O2 -std=c++17 -fopenmp -fPIC -ffp-contract=off -w -I "$HERE/shim" -I "$OUT/src")
 build_one() {
-    local tag="$1" def="$2"
-    "$CXX" "${CXXFLAGS[@]}" -D"$def" -shared -o "$OUT/libprr_ref_${tag}.so" \
+    local tag="$1" def="$2" extra="${3:-}"
+    "$CXX" "${CXXFLAGS[@]}" -D"$def" ${extra} -shared -o "$OUT/libprr_ref_${tag}.so" \
         -x c++ "$HERE/ref_driver.cpp" \
         -x c++ "$OUT/src/main/Spacetime.cpp" \
         -x c++ "$OUT/src/main/Camera.cpp" \
@@ -94,6 +111,10 @@ build_one kerr PRR_REF_METRIC_KERR
 # the reference's alternative Cartesian Schwarzschild header (Christoffel tables;
 # not selected by the shipped main/metric.h)
 build_one cart PRR_REF_METRIC_CART
+# the reference's spherical-coordinate Schwarzschild header, with the
+# reference's SPHERICAL switch (kernels/solver.cuh:34-41, prr.cpp:250-252,
+# main/base.h:71-83,121-124)
+build_one sph PRR_REF_METRIC_SPH -DSPHERICAL
 echo "built: $(ls "$OUT"/libprr_ref_*.so | tr '\n' ' ')"
 # the patched source copy is only a build intermediate: keep just the libraries
 rm -rf "$OUT/src"

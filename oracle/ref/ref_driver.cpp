@@ -118,12 +118,15 @@ double prr_ref_frame(int frame, int nthreads, int rows_stride,
     int samples = camera.getAAsamples();
     std::string header = "frame" + to_string(frame);
 
-    // prr.cpp:245-253
+    // prr.cpp:245-253 (with SPHERICAL, 250-252 too)
     camera.pos = f3(parf(header, "x"), parf(header, "y"), parf(header, "z"));
     camera.a = parf(header, "a") * M_PI / 180.0f;
     camera.b = parf(header, "b") * M_PI / 180.0f;
     camera.computeVectors();
     spacetime.updateScene(frame);
+#ifdef SPHERICAL
+    camera.spos = pos_cartTOspher(camera.pos);
+#endif
     spacetime.setBhMass(parf(header, "mass", spacetime.getBhMass()));
 
     // prr.cpp:258-276
@@ -215,6 +218,9 @@ int prr_ref_prepare(int frame, int nthreads)
     camera.b = parf(header, "b") * M_PI / 180.0f;
     camera.computeVectors();
     spacetime.updateScene(frame);
+#ifdef SPHERICAL
+    camera.spos = pos_cartTOspher(camera.pos);
+#endif
     spacetime.setBhMass(parf(header, "mass", spacetime.getBhMass()));
     dim3 blocks(res.x / 8 + 1, res.y / 8 + 1), threads(8, 8);
     if (camera.getSSAADistr() == SSAA_DISTR::NONE) prr_ref_launch(blocks, threads, [&] { createRays_none(rays, res); });

@@ -100,13 +100,15 @@ COMPAT = PKG / "compat"
 
 
 def build_metric_plugin(header: Path, name: str | None = None, verbose: bool = False,
-                        lib_dir: Path | None = None) -> Path:
+                        lib_dir: Path | None = None, spherical: bool = False) -> Path:
     """Compiles an unchanged ParRelRay metric plug-in header (the files the
     reference's main/metric.h selects, e.g. metrics/schwarzschild.cuh) into
     libprr_metric_<name>.so for prr_load_metric_plugin.  The header is copied
     into a staging tree whose main/, cudamaths/ and scene/ are this package's
     compatibility headers, so its "../main/base.h"-style includes resolve to
-    them; the staging copy is deleted after the build."""
+    them; the staging copy is deleted after the build.  `spherical` defines
+    SPHERICAL, the reference's compile-time switch for headers whose states
+    are (r, theta, phi, t) (e.g. metrics/"schwarzschild - sph.cuh")."""
     header = Path(header)
     name = name or header.stem.replace(" ", "").replace("-", "")
     out = Path(lib_dir or LIBDIR) / f"libprr_metric_{name}.so"
@@ -125,7 +127,8 @@ def build_metric_plugin(header: Path, name: str | None = None, verbose: bool = F
     out.parent.mkdir(parents=True, exist_ok=True)
     try:
         _run([nvcc(), "-fmad=false", *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-              "--expt-relaxed-constexpr", "-w", f'-DPRR_PLUGIN_NAME="{name}"', "-I", str(stage), "-I", str(COMPAT),
+              "--expt-relaxed-constexpr", "-w", f'-DPRR_PLUGIN_NAME="{name}"', *(["-DSPHERICAL"] if spherical else []),
+              "-I", str(stage), "-I", str(COMPAT),
               "-I", str(CSRC), "-I", str(INCLUDE), str(tu), "-o", str(out)], verbose)
     finally:
         shutil.rmtree(stage, ignore_errors=True)
@@ -134,14 +137,17 @@ def build_metric_plugin(header: Path, name: str | None = None, verbose: bool = F
 
 def build_plugins(verbose: bool = False) -> list[Path]:
     """The Kerr plug-in shipped in compat/metrics, and - where the reference
-    tree is mounted - the reference's own Schwarzschild and flat headers and
-    its alternative Cartesian Schwarzschild header, compiled unchanged."""
+    tree is mounted - the reference's own Schwarzschild and flat headers, its
+    alternative Cartesian Schwarzschild header and its spherical-coordinate
+    Schwarzschild header (with SPHERICAL), compiled unchanged."""
     outs = [build_metric_plugin(COMPAT / "metrics" / "kerr.cuh", "kerr", verbose)]
     ref = Path(os.environ.get("PRR_REFERENCE", "/root/reference"))
-    for stem, name in (("schwarzschild", "schwarzschild"), ("flat", "flat"), ("schwarzschild - cart", "schwarzschildcart")):
+    for stem, name, sph in (("schwarzschild", "schwarzschild", False), ("flat", "flat", False),
+                            ("schwarzschild - cart", "schwarzschildcart", False),
+                            ("schwarzschild - sph", "schwarzschildsph", True)):
         h = ref / "metrics" / f"{stem}.cuh"
         if h.exists():
-            outs.append(build_metric_plugin(h, name, verbose))
+            outs.append(build_metric_plugin(h, name, verbose, spherical=sph))
     return outs
 
 
@@ -167,7 +173,7 @@ def build_reference(verbose: bool = False) -> bool:
     if not (ref / "kernels" / "solver.cuh").exists():
         return False
     out = ORACLE_DIR / "_ref"
-    libs = [out / f"libprr_ref_{t}.so" for t in ("schw", "flat", "kerr", "cart")]
+    libs = [out / f"libprr_ref_{t}.so" for t in ("schw", "flat", "kerr", "cart", "sph")]
     deps = [ORACLE_DIR / "ref" / "build_ref.sh", ORACLE_DIR / "ref" / "ref_driver.cpp",
             PKG / "compat" / "metrics" / "kerr.cuh"] + sorted((ORACLE_DIR / "ref" / "shim").glob("*.h"))
     if all(_newer(l, deps) for l in libs):

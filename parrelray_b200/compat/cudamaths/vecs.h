@@ -242,3 +242,6 @@ PRR_VHD f4 f4_zero() { return f4(0, 0, 0, 0); }
 PRR_VHD f3 f3_id() { return f3(1, 1, 1); }
 PRR_VHD f4 f4_id() { return f4(1, 1, 1, 1); }
 PRR_VHD i2 i2_zero() { return i2(0, 0); }
+
+// Cartesian <-> spherical conversions (the reference's vecs.h includes them)
+#include "transform.cuh"

@@ -50,19 +50,33 @@ struct OutSphere {
         return sqavg(tex[pi], tex[pi + i2(0, 1)], tex[pi + i2(1, 0)], tex[pi + i2(1, 1)]);
     }
 
-    // background at the POSITION p (main/base.h:68-117)
+    // background at the POSITION p (main/base.h:68-117); with SPHERICAL, p
+    // is (r, theta, phi, t) and the sky is mirrored in phi (base.h:76-83)
     __device__ f3 getColorDefault(f4 p)
     {
         if (!tex.dt.p) return f3(0.0f, 0.0f, 0.0f);
+#ifdef SPHERICAL
+        float theta = p.y, phi = p.z;
+        phi = -phi;
+        phi += 2.0f * PI;  // in double, as the reference's PI is a double literal
+        if (phi == 2.0f * PI) phi = 0;
+        if (theta == PI) theta = 0;
+#else
         float theta = acosf(p.z / p.xyz().norm()), phi = atan2f(p.y, p.x);
         phi = (phi >= 0 ? phi : phi + 2.0f * PI);
+#endif
         return cell_rms(theta, phi);
     }
 
     // background in the DIRECTION u (main/base.h:119-162); the library's
-    // own lookup, which reproduces the reference's arithmetic
+    // own lookup, which reproduces the reference's arithmetic.  With
+    // SPHERICAL the reference has no direction lookup and returns green
+    // (base.h:121-124; its diagnostic printf is not repeated here).
     __device__ f3 getColorDefault2(f4 u)
     {
+#ifdef SPHERICAL
+        return f3(0.0f, 1.0f, 0.0f);
+#endif
         if (!tex.dt.p) return f3(0.0f, 0.0f, 0.0f);
         prr::V3<float> c = prr::background_rms<float>(tex.dt, u.x, u.y, u.z);
         return f3(c.x, c.y, c.z);

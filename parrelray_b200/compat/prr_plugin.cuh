@@ -45,6 +45,9 @@ __host__ __device__ inline Camera make_camera(const FrameParams &fp)
     Camera c(f3(fp.cam[0], fp.cam[1], fp.cam[2]), fp.alpha, fp.beta, fp.vfov, i2(fp.width, fp.height),
              fp.ssaa == 0 ? SSAA_DISTR::NONE : SSAA_DISTR::REGULAR, fp.samples);
     c.computeVectors();
+#ifdef SPHERICAL
+    c.spos = pos_cartTOspher(c.pos);  // prr.cpp:250-252
+#endif
     return c;
 }
 
@@ -85,11 +88,28 @@ __device__ inline void from_ray(const Ray &T, RefRay &R)
     R.u = {T.u.x, T.u.y, T.u.z, T.u.w};
 }
 
-// The header's functions as the solver's hook set (ref_stepper.cuh).
+// The header's functions as the solver's hook set (ref_stepper.cuh).  A
+// header written for SPHERICAL states (r, theta, phi, t) is compiled with
+// SPHERICAL defined, as the reference compiles it: its rays then start at
+// the camera's spherical position with the spherical rates of the pin-hole
+// direction (kernels/solver.cuh:34-37).
 struct PluginHooks {
+#ifdef SPHERICAL
+    static constexpr bool kSpherical = true;
+#else
+    static constexpr bool kSpherical = false;
+#endif
     Camera cam;
     Spacetime space;
     Tracer trace;
+
+    __device__ void spherical_start(RefRay &R, V4<float> &u) const
+    {
+        Camera c = cam;
+        f3 v = vel_cartTOspher(c.pos, c.rayDir_PinHole(f2(R.uvx, R.uvy)));
+        u = {v.x, v.y, v.z, 1.0f};
+        R.r = {c.spos.x, c.spos.y, c.spos.z, 0.0f};
+    }
 
     __device__ void metric(const RefRay &R, float g[16]) const
     {
@@ -183,7 +203,11 @@ __global__ void k_plugin_collect(const Ray *__restrict__ rays, long long nrays, 
     if (counters) {
         int cls;
         switch (T.result) {
+#ifdef SPHERICAL
+        case RESULT::SUCCESS: cls = T.r.x >= rout ? prr::C_ESCAPED : prr::C_CAPTURED; break;
+#else
         case RESULT::SUCCESS: cls = T.r.xyz().norm() >= rout ? prr::C_ESCAPED : prr::C_CAPTURED; break;
+#endif
         case RESULT::INTERSECTION: cls = prr::C_INTERSECTION; break;
         case RESULT::INFINITE_GEO: cls = prr::C_INFINITE; break;
         default: cls = prr::C_MATH_ERROR;

@@ -55,11 +55,18 @@ PRR_DEV bool isnan4(const V4<float> &a) { return isnan(a.x) || isnan(a.y) || isn
 template <class H> PRR_DEV void ref_init_h(const FrameParams &fp, const H &hk, int x, int y, int s, RefRay &R)
 {
     ray_uv(fp, x, y, s, R.uvx, R.uvy);
-    V3<float> dir = ray_dir(fp, R.uvx, R.uvy);
-    R.r = {fp.cam[0], fp.cam[1], fp.cam[2], 0.0f};
+    V4<float> u;
+    if constexpr (H::kSpherical) {
+        // a hook set in spherical coordinates places the ray itself
+        // (kernels/solver.cuh:34-37)
+        hk.spherical_start(R, u);
+    } else {
+        V3<float> dir = ray_dir(fp, R.uvx, R.uvy);
+        R.r = {fp.cam[0], fp.cam[1], fp.cam[2], 0.0f};
+        u = {dir.x, dir.y, dir.z, 1.0f};
+    }
     R.u = {0.0f, 0.0f, 0.0f, 0.0f};
     R.result = PRR_RESULT_SUCCESS;
-    V4<float> u = {dir.x, dir.y, dir.z, 1.0f};
     float g[16];
     hk.metric(R, g);
     float a = g[15];
@@ -99,6 +106,7 @@ PRR_DEV bool ref_endloop(const FrameParams &fp, RefRay &R, float th)
 }
 
 struct BuiltinHooks {
+    static constexpr bool kSpherical = false;  // Cartesian (x, y, z, t) states
     const FrameParams &fp;
     PRR_DEV void metric(const RefRay &R, float g[16]) const { ref_metric(fp, R, g); }
     PRR_DEV V4<float> geod(const V4<float> &x, const V4<float> &u) const { return ref_geod(fp, x, u); }

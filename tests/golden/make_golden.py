@@ -39,6 +39,16 @@ CASES = {
                       [(9.0, 40.0, 1.0, 1)]),
 }
 
+# Metric plug-in headers of the reference run through its own frame pipeline
+# (files named plugin_*): the reference's spherical-coordinate Schwarzschild
+# header metrics/"schwarzschild - sph.cuh", built with SPHERICAL.  It ignores
+# the scene's spheres, so these frames have none.
+PLUGIN_CASES = {
+    "plugin_sph_64x36_s1": ("sph", abi.METRIC_SCHWARZSCHILD, 64, 36, 1, 0.0, 30.0, 85.0, 60.0, 1e-3, []),
+    "plugin_sph_32x18_s4": ("sph", abi.METRIC_SCHWARZSCHILD, 32, 18, 4, 0.0, 20.0, 88.0, 50.0, 1e-4, []),
+}
+ALL_CASES = {**CASES, **PLUGIN_CASES}
+
 SKY = (256, 128)
 SPH = (128, 64)
 
@@ -74,7 +84,7 @@ def main() -> int:
         return 2
     tex = textures()
     digest = texture_digest(tex)
-    for name, spec in CASES.items():
+    for name, spec in ALL_CASES.items():
         d, meta = case_frame(spec)
         _, a_deg, b_deg = scenes.camera_pose(spec[6], spec[7])
         deck = write_deck(Path("/tmp/prrgolden"), d, tex, fov_deg=spec[8], a_deg=a_deg, b_deg=b_deg)

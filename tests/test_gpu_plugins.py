@@ -10,6 +10,10 @@ with prr_load_metric_plugin renders what the reference renders with it.
   >= 99.5% of rays, image within 1/255 on >= 99.9% of pixels).
 * A plug-in and the built-in REFERENCE path for the same metric agree ray for
   ray.
+* The reference's spherical-coordinate header metrics/"schwarzschild - sph.cuh"
+  (states (r, theta, phi, t), built with SPHERICAL) against the reference's
+  own frame pipeline built with the same header and switch
+  (tests/golden/plugin_sph_*.npz).
 """
 import numpy as np
 import pytest
@@ -124,3 +128,33 @@ def test_reference_alternative_cartesian_header(gpu, small_textures):
     assert np.mean(state[:, 2] == z["state"][:, 2]) >= 0.995
     imgs, _, _ = gpu.render(d)
     assert pixel_rule(imgs[0], quantize(z["image"])) >= 0.999
+
+
+@pytest.mark.parametrize("case", ["plugin_sph_64x36_s1", "plugin_sph_32x18_s4"])
+def test_reference_spherical_header(gpu, case):
+    """metrics/"schwarzschild - sph.cuh" compiled unchanged with SPHERICAL: rays start at the camera's
+    spherical position with the spherical rates of the pin-hole direction (kernels/solver.cuh:34-37),
+    the header's pole flip and angle wrapping run in User_ENDLOOP, and its rayToRGB looks the sky up
+    at the final (theta, phi) (main/base.h:68-117).  Bars: the REFERENCE-mode ones; escape angles
+    within 1e-3 rad for >= 99% of the rays that escape in both."""
+    p = plugin_path("schwarzschildsph")
+    if not p.exists():
+        pytest.skip(f"{p.name} is built only where the reference's headers are available")
+    d, tex, z = load_case(case)
+    gpu.upload_textures(tex)
+    d.metric = gpu.load_metric_plugin(p)
+    state, rgb, stats = gpu.trace_rays(d)
+    ref = z["state"]
+    assert stats.rays == d.nrays and stats.attempts > 0
+    assert np.mean(state[:, 2] == ref[:, 2]) >= 0.995
+    esc = (ref[:, 2] == abi.RESULT_SUCCESS) & (ref[:, 3] >= 100.0) & (state[:, 3] >= 100.0)
+    assert esc.sum() > 0.3 * d.nrays
+    dth = np.abs(state[esc, 4] - ref[esc, 4])
+    dph = np.abs(np.angle(np.exp(1j * (state[esc, 5].astype(np.float64) - ref[esc, 5]))))
+    assert np.mean((dth <= 1e-3) & (dph <= 1e-3)) >= 0.99, (dth.max(), dph.max())
+    cap = (ref[:, 2] == abi.RESULT_SUCCESS) & (ref[:, 3] < 3.0)
+    assert np.mean(state[cap, 3] < 3.0) >= 0.99
+    assert np.mean(np.abs(rgb - z["rgb"]).max(axis=1) <= 1 / 255) >= 0.99
+    imgs, _, _ = gpu.render(d)
+    npx = d.width * d.height
+    assert pixel_rule(imgs[0], quantize(z["image"])) >= min(0.999, 1 - 1.0 / npx - 1e-12)

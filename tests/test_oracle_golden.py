@@ -15,11 +15,13 @@ import pytest
 from parrelray_b200 import abi, scenes
 
 GOLDEN = Path(__file__).parent / "golden"
-CASES = sorted(p.stem for p in GOLDEN.glob("*.npz"))
+# the built-in metrics; plugin_* fixtures hold a reference metric header's own
+# outputs (tests/test_gpu_plugins.py) and have no restatement here
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("plugin_"))
 
 
 def load_case(name):
-    from golden.make_golden import CASES as SPECS, case_frame, textures
+    from golden.make_golden import ALL_CASES as SPECS, case_frame, textures
 
     z = np.load(GOLDEN / f"{name}.npz")
     d, meta = case_frame(SPECS[name])
@@ -87,3 +89,31 @@ def test_oracle_matches_live_reference(oracle, small_textures, seed, metric_tag,
     assert np.array_equal(st[:, :11].astype(np.float32), out["state"], equal_nan=True)
     assert np.array_equal(rgb, out["rgb"], equal_nan=True)
     assert np.array_equal(oracle.post(rgb, d.width, d.height, S, False), out["image"])
+
+
+@pytest.mark.parametrize("name", ["plugin_sph_64x36_s1", "plugin_sph_32x18_s4"])
+def test_plugin_fixture_is_the_reference_output(name):
+    """The spherical-header fixtures are what the reference's own frame pipeline, built with
+    metrics/"schwarzschild - sph.cuh" and SPHERICAL, renders from the deck (bit for bit, live,
+    where the reference tree is mounted); every ray ends with SUCCESS, at the horizon or at rout."""
+    from pathlib import Path
+
+    from golden.make_golden import ALL_CASES
+    from oracles import RefHost, ref_available, write_deck
+
+    d, tex, z = load_case(name)
+    st = z["state"]
+    assert np.all(st[:, 2] == abi.RESULT_SUCCESS)
+    r = st[:, 3]
+    assert np.all((r >= 100.0) | (r <= 2.0 + 0.001 + 1e-6))
+    assert 0 < np.mean(r >= 100.0) < 1
+    if not ref_available("sph"):
+        pytest.skip("reference host build with the spherical header not built here")
+    spec = ALL_CASES[name]
+    _, a_deg, b_deg = scenes.camera_pose(spec[6], spec[7])
+    deck = write_deck(Path("/tmp/prrsphgolden"), d, tex, fov_deg=spec[8], a_deg=a_deg, b_deg=b_deg)
+    ref = RefHost("sph")
+    assert ref.load(deck) == 1
+    out = ref.frame(0, fxaa=True)
+    assert np.array_equal(out["state"], st, equal_nan=True)
+    assert np.array_equal(out["image"], z["image"])
