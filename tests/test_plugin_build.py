@@ -73,4 +73,55 @@ def test_shipped_plugins_are_built(built):
     for p in outs:
         assert _exports(p).prr_plugin_frame_params_size() > 0
     if Path("/root/reference/metrics/schwarzschild.cuh").exists():
-        assert {"libprr_metric_schwarzschild.so", "libprr_metric_flat.so"} <= names
+        assert {"libprr_metric_schwarzschild.so", "libprr_metric_flat.so", "libprr_metric_schwarzschildcart.so",
+                "libprr_metric_schwarzschildsph.so"} <= names
+
+
+SPHERICAL_HEADER = r"""
+#pragma once
+#include "../main/base.h"
+#include "../main/Camera.h"
+#include "../main/Spacetime.h"
+#include "../cudamaths/mats.h"
+
+__device__ bool User_LOOP(ray *iray, Camera cam, Spacetime space) { return true; }
+__device__ bool User_UPDATE(ray *iray, Camera cam, Spacetime space, float h) { return true; }
+__device__ bool User_ENDLOOP(ray *iray, Camera cam, Spacetime space, tracer trace)
+{
+    if (iray->r.x >= trace.sph1.rout) { iray->result = RESULT::SUCCESS; return false; }
+    return true;
+}
+__device__ f4 getGeod(f4 p, f4 u, Spacetime space)
+{
+    // flat space in (r, theta, phi, t)
+    float r = p.x, st = sinf(p.y), ct = cosf(p.y);
+    return f4(r * (u.y * u.y + st * st * u.z * u.z), -2.0f / r * u.x * u.y + st * ct * u.z * u.z,
+              -2.0f / r * u.x * u.z - 2.0f * ct / st * u.y * u.z, 0.0f);
+}
+__device__ mat4 getMetric(ray *R, Spacetime space)
+{
+    mat4 g; float r = R->r.x, st = sinf(R->r.y);
+    g[0] = 1.0f; g[5] = r * r; g[10] = r * r * st * st; g[15] = -1.0f;
+    return g;
+}
+__global__ void rayToRGB(ray *rays, Camera cam, Spacetime space, tracer trace, int samples)
+{
+    i2 ij = i2(blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+    if ((ij.x >= cam.getRes().x * samples) || (ij.y >= cam.getRes().y)) return;
+    int pid = ij.y * cam.getRes().x * samples + ij.x;
+    f3 back = pos_spherTOcart(pos_cartTOspher(f3(1.0f, 2.0f, 3.0f)));  // the conversions are there
+    rays[pid].u = f4(trace.sph1.getColorDefault(rays[pid].r) + 0.0f * back, 0.0f);
+}
+"""
+
+
+def test_spherical_header_builds_with_the_switch(built, tmp_path):
+    """A header written for the reference's SPHERICAL build (states (r, theta, phi, t); the sky looked
+    up at the final angles; the Cartesian <-> spherical conversions of cudamaths/transform.cuh) builds
+    unchanged with spherical=True."""
+    h = tmp_path / "flatsph.cuh"
+    h.write_text(SPHERICAL_HEADER)
+    out = build.build_metric_plugin(h, "testflatsph", lib_dir=tmp_path / "lib", spherical=True)
+    lib = _exports(out)
+    assert lib.prr_plugin_name() == b"testflatsph"
+    assert lib.prr_plugin_ray_bytes() == 48
