@@ -17,6 +17,12 @@
 #pragma once
 #include "phys_stepper.cuh"
 
+// One-ray stages (stages_xy) evaluate the geodesic with its x/y twins paired
+// (geod_xy) unless built with PRR_GEOD_XY=0 (the all-scalar geod).
+#ifndef PRR_GEOD_XY
+#define PRR_GEOD_XY 1
+#endif
+
 namespace prr {
 namespace pv {
 
@@ -105,6 +111,71 @@ template <class V> PRR_DEV Vec4<V> geod(const Vec4<V> &p, const Vec4<V> &u, V Ma
     const V Lam = fma_(lx, Gx, fma_(ly, Gy, fma_(lz, Gz, neg_(A))));
     const V fLam = mul_(f, Lam);
     return {fma_(fLam, lx, neg_(Gx)), fma_(fLam, ly, neg_(Gy)), fma_(fLam, lz, neg_(Gz)), fma_(m1, fLam, A)};
+}
+
+PRR_DEV float2 f2(float a, float b) { return make_float2(a, b); }
+PRR_DEV float2 sp(float a) { return make_float2(a, a); }
+
+// geod<float> with the x and y components of one ray paired: P = (X, Y) and
+// U = (u^x, u^y) in, (du^x, du^y) in gxy and du^z, du^t in gz, gt out.  The
+// operations are geod's, one for one and in its order; where geod applies
+// the same operation to an x and a y quantity (gradients, l, D l, the
+// lowered contraction, the raise) one paired instruction does both, and the
+// rest (scalars and dot products) stays scalar.
+PRR_DEV void geod_xy(float2 P, float Z, float2 U, float uz, float ut, float Mass, float a, float2 &gxy, float &gz,
+                     float &gt)
+{
+    const float X = P.x, Y = P.y, ux = U.x, uy = U.y;
+    const float a2 = mul_(a, a), Z2 = mul_(Z, Z);
+    const float R2 = fma_(X, X, fma_(Y, Y, Z2));
+    const float b = fma_(-1.0f, a2, R2);
+    const float S2 = fma_(b, b, mul_(mul_(4.0f, a2), Z2));
+    const float iS = rsq_(S2);
+    const float S = mul_(S2, iS);
+    const float r2 = mul_(0.5f, add_(b, S));
+    const float ir = rsq_(r2);
+    const float r = mul_(r2, ir);
+    const float q = add_(r2, a2), iq = rcp_(q);
+    const float Sig = fma_(r2, r2, mul_(a2, Z2)), iSig = rcp_(Sig);
+    const float2 r_ = sp(r), iq_ = sp(iq);
+    // radius gradient
+    const float rS = mul_(r, iS);
+    const float2 dr = mul_(P, sp(rS));
+    const float drz = mul_(mul_(Z, q), mul_(iS, ir));
+    // f and its gradient
+    const float r3 = mul_(r2, r);
+    const float f = mul_(mul_(mul_(2.0f, Mass), r3), iSig);
+    const float c1 = mul_(f, fma_(mul_(-4.0f, r3), iSig, mul_(3.0f, ir)));
+    const float2 df = mul_(sp(c1), dr);
+    const float dfz = fma_(c1, drz, mul_(mul_(-2.0f, f), mul_(a2, mul_(Z, iSig))));
+    // null vector l (l_t = 1)
+    const float2 l = mul_(fma_(r_, P, f2(mul_(a, Y), neg_(mul_(a, X)))), iq_);
+    const float lz = mul_(Z, ir);
+    // directional derivatives along the spatial velocity
+    const float Dr = fma_(ux, dr.x, fma_(uy, dr.y, mul_(uz, drz)));
+    const float nDq = mul_(mul_(-2.0f, r), Dr);
+    const float2 w = mul_(l, sp(nDq));
+    const float2 Dl = mul_(fma_(sp(Dr), P, fma_(r_, U, f2(fma_(a, uy, w.x), fma_(neg_(a), ux, w.y)))), iq_);
+    const float Dlz = mul_(fma_(neg_(lz), Dr, uz), ir);
+    const float Df = fma_(ux, df.x, fma_(uy, df.y, mul_(uz, dfz)));
+    const float L = fma_(l.x, ux, fma_(l.y, uy, fma_(lz, uz, ut)));
+    const float DL = fma_(ux, Dl.x, fma_(uy, Dl.y, mul_(uz, Dlz)));
+    // gradient of L at fixed u
+    const float P0 = fma_(mul_(-2.0f, r), fma_(ux, l.x, mul_(uy, l.y)), fma_(ux, X, mul_(uy, Y)));
+    const float Pp = fma_(P0, iq, neg_(mul_(uz, mul_(lz, ir))));
+    const float2 dL = fma_(dr, sp(Pp), mul_(f2(fma_(r, ux, neg_(mul_(a, uy))), fma_(a, ux, mul_(r, uy))), iq_));
+    const float dLz = fma_(drz, Pp, mul_(uz, ir));
+    // lowered contraction, then raise with g^{-1} = eta - f l l
+    const float A = fma_(L, Df, mul_(f, DL));
+    const float fL = mul_(f, L);
+    const float nhL2 = mul_(mul_(-0.5f, L), L);
+    const float2 G = fma_(l, sp(A), fma_(sp(fL), Dl, fma_(sp(nhL2), df, neg_(mul_(sp(fL), dL)))));
+    const float Gz = fma_(lz, A, fma_(fL, Dlz, fma_(nhL2, dfz, neg_(mul_(fL, dLz)))));
+    const float Lam = fma_(l.x, G.x, fma_(l.y, G.y, fma_(lz, Gz, neg_(A))));
+    const float fLam = mul_(f, Lam);
+    gxy = fma_(sp(fLam), l, neg_(G));
+    gz = fma_(fLam, lz, neg_(Gz));
+    gt = fma_(-1.0f, fLam, A);
 }
 
 template <class V> PRR_DEV Vec4<V> scl(V h, const Vec4<V> &g) { return {mul_(h, g.x), mul_(h, g.y), mul_(h, g.z), mul_(h, g.w)}; }
@@ -196,8 +267,6 @@ template <class V> PRR_DEV StageOut<V> stages(const StageIn<V> &in)
 // estimate are component-wise, so half of their instructions go away; the
 // geodesic stays scalar (its operands mix components).  Same mathematics as
 // stages<float>; rounding differs in the last bits.
-PRR_DEV float2 f2(float a, float b) { return make_float2(a, b); }
-PRR_DEV float2 sp(float a) { return make_float2(a, a); }
 
 PRR_DEV StageOut<float> stages_xy(const StageIn<float> &in)
 {
@@ -208,7 +277,23 @@ PRR_DEV StageOut<float> stages_xy(const StageIn<float> &in)
     const float2 u01 = f2(in.u.x, in.u.y), u23 = f2(in.u.z, in.u.w);
 #define PC(v) sp((float)(v))
     // k_i = h G(z_i), held as pairs
-#define GEOD(Kp, Kq, zx01, zx23, zu01, zu23)                                                                           {                                                                                                                      const Vec4<float> g = geod<float>({zx01.x, zx01.y, zx23.x, 0.0f}, {zu01.x, zu01.y, zu23.x, zu23.y}, in.M, in.a);         Kp = mul_(H, f2(g.x, g.y));                                                                                        Kq = mul_(H, f2(g.z, g.w));                                                                                    }
+#if PRR_GEOD_XY
+#define GEOD(Kp, Kq, zx01, zx23, zu01, zu23)                                                                           \
+    {                                                                                                                  \
+        float2 gxy;                                                                                                    \
+        float gz, gt;                                                                                                  \
+        geod_xy(zx01, zx23.x, zu01, zu23.x, zu23.y, in.M, in.a, gxy, gz, gt);                                          \
+        Kp = mul_(H, gxy);                                                                                             \
+        Kq = mul_(H, f2(gz, gt));                                                                                      \
+    }
+#else
+#define GEOD(Kp, Kq, zx01, zx23, zu01, zu23)                                                                           \
+    {                                                                                                                  \
+        const Vec4<float> g = geod<float>({zx01.x, zx01.y, zx23.x, 0.0f}, {zu01.x, zu01.y, zu23.x, zu23.y}, in.M, in.a); \
+        Kp = mul_(H, f2(g.x, g.y));                                                                                    \
+        Kq = mul_(H, f2(g.z, g.w));                                                                                    \
+    }
+#endif
     float2 k1p, k1q, k2p, k2q, k3p, k3q, k4p, k4q, k5p, k5q, k6p, k6q;
     float2 zxp, zxq, zup, zuq;
     GEOD(k1p, k1q, x01, x23, u01, u23)
