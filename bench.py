@@ -20,6 +20,9 @@ Reported (one JSON line on rank 0):
   accuracy        fraction of pixels within 1/255 of an FP64 render
   cpu_baseline    the reference's own solver (host build, Kerr plug-in) on a
                   bounded sample of the same frame, on this host's cores
+  reference_cuda  the reference's own CUDA build (its sources, nvcc, sm_100a)
+                  on this GPU: trace_RKF at eps 1e-6 on a band of rows, and
+                  its whole frame pipeline at the deck's eps 1e-3
 """
 from __future__ import annotations
 
@@ -188,6 +191,87 @@ def cpu_reference_sample(frame, textures, budget_s: float, nthreads: int, eps: f
                         for b, r in zip(order[:done] % nbx, order[:done] // nbx) for t in range(8)])
     return {"rays": rays, "seconds": secs, "mrays_s": rays / secs / 1e6 if secs > 0 else None,
             "infinite_geo_fraction": float(np.mean(results == abi.RESULT_INFINITE_GEO)) if len(results) else None}
+
+
+def bench_reference_cuda(width: int, height: int, timeout_s: float = 240.0):
+    """The reference's own CUDA build on this GPU, in a child process (the reference ends its process
+    on any CUDA error, prr.cpp:37-47, and resets the device): see reference_cuda_child."""
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as td:
+        out = Path(td) / "refcuda.json"
+        try:
+            r = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--refcuda-child", str(out),
+                                "--width", str(width), "--height", str(height)],
+                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=timeout_s)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": f"the reference CUDA run did not finish in {timeout_s:.0f} s"}
+        if r.returncode != 0 or not out.exists():
+            return {"unavailable": f"the reference CUDA run exited with status {r.returncode}"}
+        return json.loads(out.read_text())
+
+
+def reference_cuda_child(out_path: str, width: int, height: int, layer: int = 134, nlines: int = 4) -> int:
+    """oracle/_ref/libprr_refcu_kerr.so: the reference's sources compiled with nvcc for sm_100a, the
+    Kerr plug-in header, its <<<>>> launches.  trace_RKF at the workload's eps = 1e-6 on one band of
+    `nlines` rows (layer `layer`, through the shadow; at this tolerance most rays run to the
+    1e6-attempt cap, so the whole frame would take minutes), then its frame pipeline renderframe
+    (prr.cpp:237-341, PNG save included) at the deck's eps = 1e-3.  Writes a JSON object."""
+    import ctypes as C
+
+    from parrelray_b200 import abi, scenes
+
+    frame = scenes.kerr_1080p_ssaa4(width, height)
+    textures = scenes.standard_textures()
+    res = bench_reference_cuda_run(C, abi, scenes, frame, textures, layer, nlines)
+    Path(out_path).write_text(json.dumps(res))
+    return 0
+
+
+def bench_reference_cuda_run(C, abi, scenes, frame, textures, layer, nlines):
+    sys.path.insert(0, str(REPO / "tests"))
+    from oracles import write_deck
+
+    path = REPO / "oracle" / "_ref" / "libprr_refcu_kerr.so"
+    if not path.exists():
+        return {"unavailable": "reference CUDA build (oracle/_ref/libprr_refcu_kerr.so) not built"}
+    lib = C.CDLL(str(path))
+    lib.prr_refcu_load.restype = C.c_int
+    lib.prr_refcu_load.argtypes = [C.c_char_p]
+    lib.prr_refcu_trace_rows.restype = C.c_double
+    lib.prr_refcu_trace_rows.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+    lib.prr_refcu_render.restype = C.c_double
+    lib.prr_refcu_render.argtypes = [C.c_int, C.POINTER(C.c_float)]
+    lib.prr_refcu_set_eps.restype = None
+    lib.prr_refcu_set_eps.argtypes = [C.c_float]
+    ref_frame = scenes.kerr_1080p_ssaa4(frame.width, frame.height, mode=abi.MODE_REFERENCE, eps=1e-6,
+                                        horizon_eps=0.001)
+    _, a_deg, b_deg = scenes.camera_pose(25.0, 80.0)
+    deck = write_deck(Path("/tmp/prrbenchrefcu"), ref_frame, textures, fov_deg=50.0, a_deg=a_deg, b_deg=b_deg)
+    nf = lib.prr_refcu_load(str(deck).encode())
+    if nf != 1:
+        return {"unavailable": f"prr_refcu_load returned {nf}"}
+    layers = np.array([layer], dtype=np.int32)
+    counts = np.zeros(5, dtype=np.int64)
+    ms = lib.prr_refcu_trace_rows(0, nlines, 1, layers.ctypes.data_as(C.POINTER(C.c_int)),
+                                  counts.ctypes.data_as(C.POINTER(C.c_longlong)))
+    if ms < 0:
+        return {"unavailable": "prr_refcu_trace_rows failed"}
+    rays = int(counts.sum())
+    res = {"what": "the reference's own kernels (kernels/solver.cuh trace_RKF, 8x8 blocks, one ray per thread) "
+                   "built with nvcc for sm_100a, Kerr-Schild plug-in header",
+           "eps_1e-6_sample": {"rows": f"{layer * nlines}-{(layer + 1) * nlines - 1}", "rays": rays, "ms": ms,
+                               "mrays_s": rays / (ms * 1e-3) / 1e6,
+                               "infinite_geo_fraction": float(counts[abi.RESULT_INFINITE_GEO] / max(rays, 1))}}
+    lib.prr_refcu_set_eps(1e-3)
+    img = np.zeros((frame.height, frame.width, 3), dtype=np.float32)
+    secs = lib.prr_refcu_render(0, img.ctypes.data_as(C.POINTER(C.c_float)))
+    if secs > 0:
+        res["eps_1e-3_frame"] = {"seconds": secs, "mrays_s": frame.nrays / secs / 1e6,
+                                 "what": "renderframe at the deck's default tolerance (not the workload's 1e-6), "
+                                         "wall time of its launches, synchronisations and PNG save",
+                                 "black_pixel_fraction": float(np.mean(img.max(axis=-1) <= 0.0))}
+    return res
 
 
 def bench_trajectory(ctx, torch, stream, plain_stride: int = 10):
@@ -476,6 +560,8 @@ def main():
     ap.add_argument("--no-trajectory", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--no-emission", action="store_true")
+    ap.add_argument("--no-refcuda", action="store_true", help="skip the reference's own CUDA build")
+    ap.add_argument("--refcuda-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--adjoint-size", type=int, default=512, help="side of the square differentiable-render frame")
     ap.add_argument("--adam", type=int, default=0, help="also run an N-iteration Adam fit of (a, i) (0: off)")
     ap.add_argument("--adam-lr", type=float, default=0.01)
@@ -488,6 +574,8 @@ def main():
                          "(default: prr_autotune on a quarter-size copy of the frame, outside the timed region)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.refcuda_child:
+        return reference_cuda_child(args.refcuda_child, args.width, args.height)
     global RESULT_OUT
     RESULT_OUT = reserve_stdout()
     if args.impl == "reference":
@@ -660,6 +748,8 @@ def main():
                                                    f"{r['seconds']:.1f}s; reference trace_RKF + Kerr-Schild plug-in at "
                                                    f"eps=1e-6 (absolute, FP32)",
                                          "infinite_geo_fraction": r["infinite_geo_fraction"]}
+        if not args.no_refcuda and ws == 1:
+            extra["reference_cuda"] = bench_reference_cuda(args.width, args.height)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,

@@ -54,17 +54,6 @@ assert n == 1, "tex2d.cuh: non-const operator[](f2) not found"
 open(p, "w", encoding="utf-8").write(s2)
 PY
 
-# 2. host emulation of kernel launches
-python3 - "$OUT/src/prr.cpp" <<'PY'
-import sys, re
-p = sys.argv[1]
-s = open(p, encoding="utf-8-sig").read()
-pat = re.compile(r"(\w+)<<<\s*([^,>]+?)\s*,\s*([^>]+?)\s*>>>\((.*?)\);")
-s2, n = pat.subn(lambda m: f"prr_ref_launch({m.group(2)}, {m.group(3)}, [&] {{ {m.group(1)}({m.group(4)}); }});", s)
-assert n == 7, f"prr.cpp: expected 7 kernel launches, rewrote {n}"
-open(p, "w", encoding="utf-8").write(s2)
-PY
-
 # 4. declare `u` in the SPHERICAL branch of initRays
 python3 - "$OUT/src/kernels/solver.cuh" <<'PY'
 import sys
@@ -93,6 +82,35 @@ cat > "$OUT/src/main/metric.h" <<'EOF'
 #endif
 EOF
 
+# The reference's own CUDA build starts from the tree as patched so far (its
+# <<<>>> launches kept), with one edit for device compilation:
+#   5. cudamaths/tex2d.cuh - checkCuda (fprintf/exit/cudaDeviceReset) and the
+#      allocating constructor tex2d(i2) are declared __device__ __host__ but are
+#      host-only code; nvcc rejects them in device code, so they become __host__.
+rm -rf "$OUT/src_cuda"
+cp -r "$OUT/src" "$OUT/src_cuda"
+python3 - "$OUT/src_cuda/cudamaths/tex2d.cuh" <<'PY'
+import sys
+p = sys.argv[1]
+s = open(p, encoding="utf-8-sig").read()
+for old, new in (("__device__ __host__ void checkCuda(", "__host__ void checkCuda("),
+                 ("__device__ __host__ tex2d(i2 resolution)", "__host__ tex2d(i2 resolution)")):
+    assert s.count(old) == 1, f"tex2d.cuh: {old} not found"
+    s = s.replace(old, new)
+open(p, "w", encoding="utf-8").write(s)
+PY
+
+# 2. host emulation of kernel launches
+python3 - "$OUT/src/prr.cpp" <<'PY'
+import sys, re
+p = sys.argv[1]
+s = open(p, encoding="utf-8-sig").read()
+pat = re.compile(r"(\w+)<<<\s*([^,>]+?)\s*,\s*([^>]+?)\s*>>>\((.*?)\);")
+s2, n = pat.subn(lambda m: f"prr_ref_launch({m.group(2)}, {m.group(3)}, [&] {{ {m.group(1)}({m.group(4)}); }});", s)
+assert n == 7, f"prr.cpp: expected 7 kernel launches, rewrote {n}"
+open(p, "w", encoding="utf-8").write(s2)
+PY
+
 # $CXX may point at a toolchain without libgomp; the system g++ has it.
 CXX="${PRR_ORACLE_CXX:-g++}"
 CXXFLAGS=(-O2 -std=c++17 -fopenmp -fPIC -ffp-contract=off -w -I "$HERE/shim" -I "$OUT/src")
@@ -115,6 +133,19 @@ build_one cart PRR_REF_METRIC_CART
 # reference's SPHERICAL switch (kernels/solver.cuh:34-41, prr.cpp:250-252,
 # main/base.h:71-83,121-124)
 build_one sph PRR_REF_METRIC_SPH -DSPHERICAL
-echo "built: $(ls "$OUT"/libprr_ref_*.so | tr '\n' ' ')"
-# the patched source copy is only a build intermediate: keep just the libraries
-rm -rf "$OUT/src"
+# the reference's CUDA build for sm_100a with the Kerr plug-in header (the bench
+# workload's metric): nvcc's defaults otherwise, as the reference's compile.bat
+# (`nvcc -x cu -w -O3`) has them
+NVCC="${NVCC:-nvcc}"
+if command -v "$NVCC" > /dev/null; then
+    "$NVCC" -gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 -w -shared -Xcompiler -fPIC \
+        -DPRR_REF_METRIC_KERR -I "$OUT/src_cuda" -o "$OUT/libprr_refcu_kerr.so" \
+        -x cu "$HERE/ref_cuda_driver.cu" \
+        -x cu "$OUT/src_cuda/main/Spacetime.cpp" \
+        -x cu "$OUT/src_cuda/main/Camera.cpp" \
+        -x cu "$OUT/src_cuda/main/Parameters.cpp" \
+        -x cu "$OUT/src_cuda/cudamaths/image.cu"
+fi
+echo "built: $(ls "$OUT"/libprr_ref*.so | tr '\n' ' ')"
+# the patched source copies are only build intermediates: keep just the libraries
+rm -rf "$OUT/src" "$OUT/src_cuda"

@@ -173,8 +173,8 @@ def build_reference(verbose: bool = False) -> bool:
     if not (ref / "kernels" / "solver.cuh").exists():
         return False
     out = ORACLE_DIR / "_ref"
-    libs = [out / f"libprr_ref_{t}.so" for t in ("schw", "flat", "kerr", "cart", "sph")]
-    deps = [ORACLE_DIR / "ref" / "build_ref.sh", ORACLE_DIR / "ref" / "ref_driver.cpp",
+    libs = [out / f"libprr_ref_{t}.so" for t in ("schw", "flat", "kerr", "cart", "sph")] + [out / "libprr_refcu_kerr.so"]
+    deps = [ORACLE_DIR / "ref" / "build_ref.sh", ORACLE_DIR / "ref" / "ref_driver.cpp", ORACLE_DIR / "ref" / "ref_cuda_driver.cu",
             PKG / "compat" / "metrics" / "kerr.cuh"] + sorted((ORACLE_DIR / "ref" / "shim").glob("*.h"))
     if all(_newer(l, deps) for l in libs):
         return True
