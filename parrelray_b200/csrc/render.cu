@@ -479,7 +479,8 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
     prr_launch_config winner = saved;
     float best_ms = 1e30f;
     // candidates: CTA size x refill interval x pixel slots per thread, each at the
-    // occupancy limit of its kernel; every candidate is timed three times (minimum kept)
+    // occupancy limit of its kernel; every candidate is timed three times (minimum kept),
+    // except that one more than 10 % slower than the best so far on its first run stops there
     const int blocks[3] = {64, 128, 256};
     const int intervals[3] = {8, 16, 32};
     // two pixel slots per thread only where the kernel has them (FP32, register contraction)
@@ -498,6 +499,7 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
                     s = run_plan(ctx, plan, nullptr, nullptr, ctx->stream, true);
                     if (s != PRR_OK) { ctx->cfg = saved; ctx->schedule = saved_sched; return s; }
                     ms = std::min(ms, ctx->last_ms);
+                    if (rep == 0 && ms > 1.1f * best_ms) break;
                 }
                 if (ms < best_ms) { best_ms = ms; winner = ctx->cfg; }
             }
