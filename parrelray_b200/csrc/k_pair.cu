@@ -204,6 +204,12 @@ template <> __device__ __forceinline__ void load_in<float2>(pv::StageIn<float2> 
 #define PRR_PAIR_XY 1
 #endif
 
+// Resident CTAs per SM the small-CTA instantiation is built for (its
+// register cap: 65536 / (64 x MINB), rounded down to the allocation unit).
+#ifndef PRR_PAIR_SMALL_MINB
+#define PRR_PAIR_SMALL_MINB 8
+#endif
+
 // Launch bounds (MAXT threads per CTA at most, MINB resident CTAs per SM at
 // least) cap the registers per thread.  One-slot threads in CTAs of up to 64
 // threads use the instantiation capped at 127 registers (8 CTAs = 16 warps
@@ -348,15 +354,15 @@ cudaError_t launch_pair(const PersistentArgs &a, int rpt, bool split, int block,
     if (grid < 1) grid = 1;
     const bool small = block <= 64;
     if (a.emission) {
-        if (small) k_pair<1, 64, 8, false, true><<<grid, block, 0, st>>>(a);
+        if (small) k_pair<1, 64, PRR_PAIR_SMALL_MINB, false, true><<<grid, block, 0, st>>>(a);
         else k_pair<1, 256, 1, false, true><<<grid, block, 0, st>>>(a);
     } else if (split) {
-        if (small) k_pair<1, 64, 8, true, false><<<grid, block, 0, st>>>(a);
+        if (small) k_pair<1, 64, PRR_PAIR_SMALL_MINB, true, false><<<grid, block, 0, st>>>(a);
         else k_pair<1, 256, 1, true, false><<<grid, block, 0, st>>>(a);
     } else if (rpt == 2) {
         k_pair<2, 256, 1, false, false><<<grid, block, 0, st>>>(a);
     } else if (rpt == 1) {
-        if (small) k_pair<1, 64, 8, false, false><<<grid, block, 0, st>>>(a);
+        if (small) k_pair<1, 64, PRR_PAIR_SMALL_MINB, false, false><<<grid, block, 0, st>>>(a);
         else k_pair<1, 256, 1, false, false><<<grid, block, 0, st>>>(a);
     } else {
         return cudaErrorInvalidValue;
@@ -369,12 +375,12 @@ int pair_occupancy(int rpt, bool split, int block, bool emission)
     int n = 0;
     const bool small = block <= 64;
     cudaError_t e;
-    if (emission) e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, false, true>, block, 0)
+    if (emission) e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, PRR_PAIR_SMALL_MINB, false, true>, block, 0)
                             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, false, true>, block, 0);
-    else if (split) e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, true, false>, block, 0)
+    else if (split) e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, PRR_PAIR_SMALL_MINB, true, false>, block, 0)
                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, true, false>, block, 0);
     else if (rpt == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<2, 256, 1, false, false>, block, 0);
-    else e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, 8, false, false>, block, 0)
+    else e = small ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 64, PRR_PAIR_SMALL_MINB, false, false>, block, 0)
                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pair<1, 256, 1, false, false>, block, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;

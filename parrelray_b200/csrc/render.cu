@@ -482,14 +482,14 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
     // occupancy limit of its kernel; every candidate is timed three times (minimum kept),
     // except that one more than 10 % slower than the best so far on its first run stops there
     const int blocks[3] = {64, 128, 256};
-    const int intervals[3] = {8, 16, 32};
+    const int intervals[4] = {8, 16, 32, 64};
     // two pixel slots per thread only where the kernel has them (FP32, register contraction)
     const int nrpt = (plan.precision == PRR_PREC_FP32 && ctx->geod_table != 1 && !plan.any_emission) ? 2 : 1;
     for (int rpt = 1; rpt <= nrpt; rpt++)
         for (int bi = 0; bi < 3; bi++) {
             const int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi], rpt, plan.any_emission);
             if (occ < 1) continue;
-            for (int ii = 0; ii < 3; ii++) {
+            for (int ii = 0; ii < 4; ii++) {
                 ctx->cfg.block_size = blocks[bi];
                 ctx->cfg.blocks_per_sm = occ;
                 ctx->cfg.compaction_interval = intervals[ii];
