@@ -117,3 +117,18 @@ def test_plugin_fixture_is_the_reference_output(name):
     out = ref.frame(0, fxaa=True)
     assert np.array_equal(out["state"], st, equal_nan=True)
     assert np.array_equal(out["image"], z["image"])
+
+
+def test_reference_cuda_build_exports_its_driver():
+    """oracle/_ref/libprr_refcu_kerr.so (the reference's own sources built with nvcc for sm_100a,
+    measured by the bench beside the product) loads without a GPU and exports its driver."""
+    import ctypes as C
+
+    from oracles import REF_DIR
+
+    p = REF_DIR / "libprr_refcu_kerr.so"
+    if not p.exists():
+        pytest.skip("reference CUDA build not built here")
+    lib = C.CDLL(str(p))
+    for name in ("prr_refcu_load", "prr_refcu_render", "prr_refcu_trace_rows", "prr_refcu_set_eps", "prr_refcu_info"):
+        assert hasattr(lib, name), name
