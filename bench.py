@@ -739,6 +739,11 @@ def main():
             d = np.abs(mine8[0].astype(np.int32) - ref8[0].astype(np.int32)).max(axis=-1)
             extra["accuracy"] = {"pixels_within_1_255_of_fp64": float(np.mean(d <= 1)),
                                  "max_abs_diff_255": int(d.max()), "fp64_ms": s64.kernel_ms}
+            if s64.trace_ms > 0:
+                # the FP64 render's tracing kernel against the measured FP64 FMA peak (same F_attempt)
+                a64 = s64.attempts * F_ATTEMPT / (s64.trace_ms * 1e-3) / 1e12
+                extra["accuracy"]["fp64_roofline"] = {"achieved": a64, "peak": fp64_peak, "unit": "TFLOP/s",
+                                                      "frac": a64 / fp64_peak, "attempts": int(s64.attempts)}
         if not args.no_cpu and ws == 1:
             r = cpu_reference_sample(frame, tex, args.cpu_seconds, os.cpu_count() or 1)
             if r:

@@ -68,19 +68,20 @@ __device__ __forceinline__ void write_state(O *st, long long rid, const PhysRay<
     o[11] = (O)R.accepted;
 }
 
-// Launch bounds: at most PRR_PERSISTENT_MAXT threads per CTA, at least
-// PRR_PERSISTENT_MINB resident CTAs per SM (caps registers per thread).
-#ifndef PRR_PERSISTENT_MAXT
-#define PRR_PERSISTENT_MAXT 256
-#endif
-#ifndef PRR_PERSISTENT_MINB
-#define PRR_PERSISTENT_MINB 1
+// Launch bounds: at most MAXT threads per CTA, at least MINB resident CTAs
+// per SM (caps registers per thread).  CTAs of up to 64 threads use the
+// instantiation built for 6 resident CTAs per SM: 168 registers, 12 warps;
+// the FP64 form is latency bound, and 12 warps instead of 8 (215 registers)
+// measured 1197 ms instead of 1369 ms on the 1080p frame, the few spilled
+// values notwithstanding.
+#ifndef PRR_PERSISTENT_SMALL_MINB
+#define PRR_PERSISTENT_SMALL_MINB 6
 #endif
 
 // EMIS: plasma emission (emission.cuh) accumulated at every accepted step of
 // frames that have it, composited into the colour.
-template <class T, int GEOD, bool EMIS>
-__global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_persistent(PersistentArgs a)
+template <class T, int GEOD, bool EMIS, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_persistent(PersistentArgs a)
 {
     const int lane = threadIdx.x & 31;
     long long item = -1;
@@ -186,7 +187,9 @@ __global__ void __launch_bounds__(PRR_PERSISTENT_MAXT, PRR_PERSISTENT_MINB) k_pe
 }
 
 // FP64 re-integration of the rays queued by a split-precision FP32 pass.
-__global__ void __launch_bounds__(128) k_fp64_requeue(PersistentArgs a)
+// 3 CTAs of 128 per SM (168 registers, 12 warps), as the FP64 persistent
+// kernel's small-CTA form: the FP64 integration is latency bound.
+__global__ void __launch_bounds__(128, 3) k_fp64_requeue(PersistentArgs a)
 {
     const int lane = threadIdx.x & 31;
     bool busy = false, need = true;
@@ -244,8 +247,15 @@ static cudaError_t launch_one(const PersistentArgs &a, int block, int blocks_per
 {
     int grid = nsm * blocks_per_sm;
     if (grid < 1) grid = 1;
-    k_persistent<T, GEOD, EMIS><<<grid, block, 0, st>>>(a);
+    if (block <= 64) k_persistent<T, GEOD, EMIS, 64, PRR_PERSISTENT_SMALL_MINB><<<grid, block, 0, st>>>(a);
+    else k_persistent<T, GEOD, EMIS, 256, 1><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
+}
+
+template <class T, int GEOD, bool EMIS> static cudaError_t occupancy_one(int *n, int block)
+{
+    if (block <= 64) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_persistent<T, GEOD, EMIS, 64, PRR_PERSISTENT_SMALL_MINB>, block, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_persistent<T, GEOD, EMIS, 256, 1>, block, 0);
 }
 
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st)
@@ -267,11 +277,9 @@ int persistent_occupancy(int precision, int geod_table, int block, int rays_per_
 {
     int n = 0;
     cudaError_t e;
-    if (precision == PRR_PREC_FP64)
-        e = emission ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<double, 0, true>, block, 0)
-                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<double, 0, false>, block, 0);
+    if (precision == PRR_PREC_FP64) e = emission ? occupancy_one<double, 0, true>(&n, block) : occupancy_one<double, 0, false>(&n, block);
     else if (precision == PRR_PREC_SPLIT) return pair_occupancy(1, true, block);
-    else if (geod_table) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_persistent<float, 1, false>, block, 0);
+    else if (geod_table) e = occupancy_one<float, 1, false>(&n, block);
     else return pair_occupancy(rays_per_thread == 2 ? 2 : 1, false, block, emission != 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
