@@ -327,8 +327,8 @@ prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, const float *d
  * No counterpart in the reference (which allocates everything itself in
  * main(), prr.cpp:359-378).  For callers that cannot allocate device memory
  * while rendering - an application that reserves its whole device budget up
- * front, work recorded into a CUDA graph, a real-time loop that must not pay
- * cudaMalloc's implicit synchronisation.  Every input and output is the
+ * front and hands out pieces of it itself, or a real-time loop that must not
+ * pay cudaMalloc's implicit synchronisation.  Every input and output is the
  * caller's: the frames (host array), the textures (PRR_MAX_TEXTURES device
  * pointers to RGBA8 data, NULL = absent, with their sizes) and the outputs
  * (device d_rgb8, and device d_rgbf, which frames with FXAA require: it

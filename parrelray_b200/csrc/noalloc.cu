@@ -3,9 +3,8 @@
 //
 // Who needs this: applications that own every byte of device memory up front
 // - an engine or service that carves its whole budget out of one arena at
-// start-up, code recorded into a CUDA graph where a cudaMalloc would break the
-// capture, or a real-time loop that cannot afford the implicit device
-// synchronisation a cudaMalloc/cudaFree may cause.  prr_render needs a
+// start-up and hands out pieces of it itself, or a real-time loop that cannot
+// afford the implicit device synchronisation a cudaMalloc/cudaFree may cause.  prr_render needs a
 // context, and a context grows its scratch buffers with cudaMalloc on demand;
 // this entry point takes every input and output from the caller and keeps its
 // only scratch (the work counters, the frame table and the per-frame pixel

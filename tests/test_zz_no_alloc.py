@@ -1,7 +1,7 @@
 """prr_render_noalloc, the entry point for callers that cannot allocate
 device memory while rendering (an application that reserves its whole device
-budget up front, work recorded into a CUDA graph, a real-time loop that must
-not pay cudaMalloc's implicit synchronisation).  The caller owns the
+budget up front and hands out pieces of it itself, or a real-time loop that
+must not pay cudaMalloc's implicit synchronisation).  The caller owns the
 textures and outputs; the library's only scratch is a fixed static device
 array.
 
