@@ -15,6 +15,19 @@
 
 namespace prr {
 
+// a / b and a^e: in FP32 a multiplication by the SFU reciprocal and the SFU
+// power (the renderer's FP32 convention, prr_device.cuh:frcp/fpow) unless
+// built with PRR_EMIS_FAST=0; in FP64 the IEEE division and pow
+#ifndef PRR_EMIS_FAST
+#define PRR_EMIS_FAST 1
+#endif
+template <class T> PRR_DEV T ediv(T a, T b) { return a / b; }
+template <class T> PRR_DEV T epow(T b, T e) { return pow(b, e); }
+#if PRR_EMIS_FAST
+template <> PRR_DEV float ediv<float>(float a, float b) { return a * frcp<float>(b); }
+template <> PRR_DEV float epow<float>(float b, float e) { return fpow<float>(b, e); }
+#endif
+
 template <class T> struct EmisRay {
     T I;       // accumulated intensity
     T trans;   // transmittance from the camera to the current point
@@ -29,8 +42,8 @@ template <class T> PRR_DEV void ks_fl(T x, T y, T z, T M, T a, T &r, T &f, T l[3
     f = 0; l[0] = l[1] = l[2] = 0;
     if (M != (T)0) {
         const T r2 = r * r, q = r2 + a * a;
-        f = (T)2 * M * r2 * r / (r2 * r2 + a * a * z * z);
-        l[0] = (r * x + a * y) / q; l[1] = (r * y - a * x) / q; l[2] = z / r;
+        f = ediv<T>((T)2 * M * r2 * r, r2 * r2 + a * a * z * z);
+        l[0] = ediv<T>(r * x + a * y, q); l[1] = ediv<T>(r * y - a * x, q); l[2] = ediv<T>(z, r);
     }
 }
 
@@ -90,8 +103,8 @@ PRR_DEV void emis_step(const FrameParams &fp, T M, T a, const V4<T> &x, const V4
     T n, theta = 1, v[3];
     bool flow = false;
     if (e.kind == PRR_EMISSION_DISK) {
-        const T c = x.z / r, hh = (T)e.height;
-        n = pow(r / (T)e.r_in, -(T)e.index) * exp(-c * c / ((T)2 * hh * hh));
+        const T c = ediv<T>(x.z, r), hh = (T)e.height;
+        n = epow<T>(ediv<T>(r, (T)e.r_in), -(T)e.index) * exp(ediv<T>(-c * c, (T)2 * hh * hh));
     } else {
         if (!plasma_sample<T>(e.grid, x.x, x.y, x.z, n, theta, v)) return;
         flow = e.grid.vel != nullptr;
@@ -99,23 +112,23 @@ PRR_DEV void emis_step(const FrameParams &fp, T M, T a, const V4<T> &x, const V4
     if (!(n > (T)0)) return;
     if (!flow) {  // circular orbits at the equatorial Keplerian angular velocity of r
         const T sm = sqrt(M), s = (T)e.sense;
-        const T om = s * sm / (r * sqrt(r) + s * a * sm);
+        const T om = ediv<T>(s * sm, r * sqrt(r) + s * a * sm);
         v[0] = -om * x.y; v[1] = om * x.x; v[2] = 0;
     }
     const T lv = l[0] * v[0] + l[1] * v[1] + l[2] * v[2] + (T)1;
     const T N = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] - (T)1 + f * lv * lv;  // g(xi, xi), xi = (v, 1)
     if (!(N < (T)0)) return;
-    const T ut = (T)1 / sqrt(-N);
+    const T ut = ediv<T>((T)1, sqrt(-N));
     const T lk = l[0] * k.x + l[1] * k.y + l[2] * k.z + k.w;
     const T nu_e = -ut * (k.x * v[0] + k.y * v[1] + k.z * v[2] - k.w + f * lk * lv);
     if (!(nu_e > (T)0)) return;
-    const T g = E.nu_cam / nu_e;
+    const T g = ediv<T>(E.nu_cam, nu_e);
     const T dl = E.nu_cam * h;
     T j = n;
     if (e.kind == PRR_EMISSION_GRID && e.temp_power != 0.0f) j *= pow(theta, (T)e.temp_power);
     const T w = e.spectral == 0.0f ? g * g : pow(g, (T)2 + (T)e.spectral);
     E.I += E.trans * w * j * dl;
-    if (e.absorb > 0.0f) E.trans *= exp(-(T)e.absorb * n * dl / g);
+    if (e.absorb > 0.0f) E.trans *= exp(ediv<T>(-(T)e.absorb * n * dl, g));
 }
 
 // The pixel colour of a finished ray: trans * colour + map(gain * I).
