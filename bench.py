@@ -211,30 +211,27 @@ def bench_reference_cuda(width: int, height: int, timeout_s: float = 240.0):
         return json.loads(out.read_text())
 
 
-def reference_cuda_child(out_path: str, width: int, height: int, layer: int = 134, nlines: int = 4) -> int:
+def reference_cuda_child(out_path: str, width: int, height: int, nlines: int = 4) -> int:
     """oracle/_ref/libprr_refcu_kerr.so: the reference's sources compiled with nvcc for sm_100a, the
-    Kerr plug-in header, its <<<>>> launches.  trace_RKF at the workload's eps = 1e-6 on one band of
-    `nlines` rows (layer `layer`, through the shadow; at this tolerance most rays run to the
-    1e6-attempt cap, so the whole frame would take minutes), then its frame pipeline renderframe
+    Kerr plug-in header, its <<<>>> launches.  trace_RKF at the workload's eps = 1e-6 on the band of
+    `nlines` rows at the middle of the frame (through the shadow; at this tolerance most rays run to
+    the 1e6-attempt cap, so the whole frame would take minutes), then its frame pipeline renderframe
     (prr.cpp:237-341, PNG save included) at the deck's eps = 1e-3.  Writes a JSON object."""
     import ctypes as C
+
+    sys.path.insert(0, str(REPO / "tests"))
+    from oracles import write_deck
 
     from parrelray_b200 import abi, scenes
 
     frame = scenes.kerr_1080p_ssaa4(width, height)
     textures = scenes.standard_textures()
-    res = bench_reference_cuda_run(C, abi, scenes, frame, textures, layer, nlines)
-    Path(out_path).write_text(json.dumps(res))
-    return 0
-
-
-def bench_reference_cuda_run(C, abi, scenes, frame, textures, layer, nlines):
-    sys.path.insert(0, str(REPO / "tests"))
-    from oracles import write_deck
+    layer = max(height // 2 - nlines, 0) // nlines  # rows 536-539 of 1080
 
     path = REPO / "oracle" / "_ref" / "libprr_refcu_kerr.so"
     if not path.exists():
-        return {"unavailable": "reference CUDA build (oracle/_ref/libprr_refcu_kerr.so) not built"}
+        Path(out_path).write_text(json.dumps({"unavailable": "reference CUDA build (oracle/_ref/libprr_refcu_kerr.so) not built"}))
+        return 0
     lib = C.CDLL(str(path))
     lib.prr_refcu_load.restype = C.c_int
     lib.prr_refcu_load.argtypes = [C.c_char_p]
@@ -250,13 +247,15 @@ def bench_reference_cuda_run(C, abi, scenes, frame, textures, layer, nlines):
     deck = write_deck(Path("/tmp/prrbenchrefcu"), ref_frame, textures, fov_deg=50.0, a_deg=a_deg, b_deg=b_deg)
     nf = lib.prr_refcu_load(str(deck).encode())
     if nf != 1:
-        return {"unavailable": f"prr_refcu_load returned {nf}"}
+        Path(out_path).write_text(json.dumps({"unavailable": f"prr_refcu_load returned {nf}"}))
+        return 0
     layers = np.array([layer], dtype=np.int32)
     counts = np.zeros(5, dtype=np.int64)
     ms = lib.prr_refcu_trace_rows(0, nlines, 1, layers.ctypes.data_as(C.POINTER(C.c_int)),
                                   counts.ctypes.data_as(C.POINTER(C.c_longlong)))
     if ms < 0:
-        return {"unavailable": "prr_refcu_trace_rows failed"}
+        Path(out_path).write_text(json.dumps({"unavailable": "prr_refcu_trace_rows failed"}))
+        return 0
     rays = int(counts.sum())
     res = {"what": "the reference's own kernels (kernels/solver.cuh trace_RKF, 8x8 blocks, one ray per thread) "
                    "built with nvcc for sm_100a, Kerr-Schild plug-in header",
@@ -271,7 +270,8 @@ def bench_reference_cuda_run(C, abi, scenes, frame, textures, layer, nlines):
                                  "what": "renderframe at the deck's default tolerance (not the workload's 1e-6), "
                                          "wall time of its launches, synchronisations and PNG save",
                                  "black_pixel_fraction": float(np.mean(img.max(axis=-1) <= 0.0))}
-    return res
+    Path(out_path).write_text(json.dumps(res))
+    return 0
 
 
 def bench_trajectory(ctx, torch, stream, plain_stride: int = 10):
