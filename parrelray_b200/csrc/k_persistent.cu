@@ -69,14 +69,19 @@ __device__ __forceinline__ void write_state(O *st, long long rid, const PhysRay<
 }
 
 // Launch bounds: at most MAXT threads per CTA, at least MINB resident CTAs
-// per SM (caps registers per thread).  CTAs of up to 64 threads use the
-// instantiation built for 6 resident CTAs per SM: 168 registers, 12 warps;
-// the FP64 form is latency bound, and 12 warps instead of 8 (215 registers)
-// measured 1197 ms instead of 1369 ms on the 1080p frame, the few spilled
-// values notwithstanding.
-#ifndef PRR_PERSISTENT_SMALL_MINB
-#define PRR_PERSISTENT_SMALL_MINB 6
+// per SM (caps registers per thread).  CTAs of up to 64 threads use an
+// instantiation built for several resident CTAs per SM.  The FP64 form is
+// latency bound: on the 1080p frame 8 CTAs (128 registers, 16 warps, spills
+// that hit L1) measured 1137 ms, 6 CTAs (168 registers) 1200 ms, 4 CTAs (215
+// registers, no spills) 1369 ms.  The FP32 Christoffel-table form keeps 6
+// (168 registers without spills).
+#ifndef PRR_PERSISTENT_SMALL_MINB_F64
+#define PRR_PERSISTENT_SMALL_MINB_F64 8
 #endif
+#ifndef PRR_PERSISTENT_SMALL_MINB_F32
+#define PRR_PERSISTENT_SMALL_MINB_F32 6
+#endif
+template <class T> constexpr int small_minb() { return sizeof(T) == 8 ? PRR_PERSISTENT_SMALL_MINB_F64 : PRR_PERSISTENT_SMALL_MINB_F32; }
 
 // EMIS: plasma emission (emission.cuh) accumulated at every accepted step of
 // frames that have it, composited into the colour.
@@ -187,9 +192,9 @@ __global__ void __launch_bounds__(MAXT, MINB) k_persistent(PersistentArgs a)
 }
 
 // FP64 re-integration of the rays queued by a split-precision FP32 pass.
-// 3 CTAs of 128 per SM (168 registers, 12 warps), as the FP64 persistent
+// 4 CTAs of 128 per SM (128 registers, 16 warps), as the FP64 persistent
 // kernel's small-CTA form: the FP64 integration is latency bound.
-__global__ void __launch_bounds__(128, 3) k_fp64_requeue(PersistentArgs a)
+__global__ void __launch_bounds__(128, 4) k_fp64_requeue(PersistentArgs a)
 {
     const int lane = threadIdx.x & 31;
     bool busy = false, need = true;
@@ -247,14 +252,14 @@ static cudaError_t launch_one(const PersistentArgs &a, int block, int blocks_per
 {
     int grid = nsm * blocks_per_sm;
     if (grid < 1) grid = 1;
-    if (block <= 64) k_persistent<T, GEOD, EMIS, 64, PRR_PERSISTENT_SMALL_MINB><<<grid, block, 0, st>>>(a);
+    if (block <= 64) k_persistent<T, GEOD, EMIS, 64, small_minb<T>()><<<grid, block, 0, st>>>(a);
     else k_persistent<T, GEOD, EMIS, 256, 1><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
 
 template <class T, int GEOD, bool EMIS> static cudaError_t occupancy_one(int *n, int block)
 {
-    if (block <= 64) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_persistent<T, GEOD, EMIS, 64, PRR_PERSISTENT_SMALL_MINB>, block, 0);
+    if (block <= 64) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_persistent<T, GEOD, EMIS, 64, small_minb<T>()>, block, 0);
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_persistent<T, GEOD, EMIS, 256, 1>, block, 0);
 }
 
