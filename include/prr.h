@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PRR_ABI_VERSION 3
+#define PRR_ABI_VERSION 4
 #define PRR_MAX_SPHERES 8
 #define PRR_MAX_TEXTURES 32
 
@@ -334,14 +334,20 @@ prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, const float *d
  * (device d_rgb8, and device d_rgbf, which frames with FXAA require: it
  * receives the combined image the FXAA pass reads; without FXAA it receives
  * the final float image and may be NULL).  PHYSICAL mode, FP32 or FP64,
- * persistent schedule, no context.  The only scratch is one static device
- * array of PRR_NOALLOC_SCRATCH_BYTES per device, so at most
- * PRR_NOALLOC_MAX_FRAMES frames per call (more is PRR_ERR_INVALID).  Calls
- * share that array: calls whose GPU work overlaps race, so order them on one
- * stream.  The first call on a device looks up the array's address; make it
- * before any stream capture.  Asynchronous on `stream` (NULL = legacy default
- * stream) once the frame table is on the device.  On failure a message is
- * written to errbuf (errlen bytes, may be NULL). */
+ * persistent schedule, no context, launch shape 64-thread CTAs at their
+ * occupancy limit with a warp refill every 64 attempts.  The only scratch is
+ * one static device array of PRR_NOALLOC_SCRATCH_BYTES per device, so at
+ * most PRR_NOALLOC_MAX_FRAMES frames per call (more is PRR_ERR_INVALID).
+ * Calls share that array and it keeps the last call's contents (each call
+ * clears what must start at zero): calls whose GPU work overlaps race, so
+ * order them on one stream.  Each call looks up the array's device address
+ * on the current device (cudaGetSymbolAddress, no allocation); the first call
+ * on a device can load the library's device code, so make it before any
+ * stream capture on that device.  Asynchronous on `stream` (NULL = legacy
+ * default stream): the frame table reaches the device in the parameters of a
+ * staging kernel, so the host never waits for the GPU and `frames` may be
+ * reused when the call returns.  On failure a message is written to errbuf
+ * (errlen bytes, may be NULL). */
 #define PRR_NOALLOC_MAX_FRAMES 64
 #define PRR_NOALLOC_SCRATCH_BYTES 65536
 prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, const uint8_t *const *d_textures,
@@ -392,12 +398,20 @@ void prr_graph_destroy(prr_graph *g);
  * (python -m parrelray_b200.build --metric <header>).  prr_load_metric_plugin
  * loads such a library into the context and returns in *metric_id the value
  * to put in prr_frame_desc.metric (PRR_METRIC_PLUGIN0 + k).  Plug-in frames
- * render in REFERENCE mode: the solver of kernels/solver.cuh calling the
- * header's hooks, then the header's rayToRGB, then the usual SSAA combine /
- * FXAA / quantisation.  The Spacetime the hooks see carries mass, spin
- * (prr_frame_desc.spin, for any plug-in) and the frame's spheres.  Loading
- * the same path twice returns the same id; libraries stay loaded until the
- * process exits. */
+ * render in either mode through the header's hooks, then the header's
+ * rayToRGB, then the usual SSAA combine / FXAA / quantisation:
+ *   REFERENCE - the solver of kernels/solver.cuh (one thread per ray);
+ *   PHYSICAL  - FP32 only (a header's getGeod computes in FP32): the
+ *               persistent warp-compacted scheduler with PHYSICAL semantics
+ *               (textbook stages, null initial data from the header's
+ *               getMetric, atol/rtol control, Kahan-compensated state,
+ *               max_steps) and the header's User_UPDATE / User_ENDLOOP
+ *               deciding hits and termination as in trace_RKF.
+ * A call's frames are all plug-in frames or all built-in ones; plug-in
+ * frames take no emission, no FP64/SPLIT and no recorded graph.  The
+ * Spacetime the hooks see carries mass, spin (prr_frame_desc.spin, for any
+ * plug-in) and the frame's spheres.  Loading the same path twice returns the
+ * same id; libraries stay loaded until the process exits. */
 #define PRR_METRIC_PLUGIN0 16
 #define PRR_MAX_PLUGINS 8
 prr_status prr_load_metric_plugin(prr_ctx *ctx, const char *path, int *metric_id);

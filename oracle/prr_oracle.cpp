@@ -7,7 +7,8 @@
 //  * PRR_MODE_REFERENCE: the reference algorithm restated in FP32 with the
 //    reference's operation order and its quirks, so that it reproduces the
 //    reference build (oracle/_ref) bit for bit on the same compiler flags.
-//    Pinned by tests/test_oracle_vs_reference.py.
+//    Pinned by tests/test_oracle_golden.py (fixtures made by the reference
+//    host build, and live runs of it where the reference tree is present).
 //  * PRR_MODE_PHYSICAL: textbook RKF45 / Euler, null initial data, mixed
 //    abs/rel error control, in FP32 or FP64.  The geodesic right-hand side is
 //    the full Christoffel table of the Kerr-Schild metric (independent of the

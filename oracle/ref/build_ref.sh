@@ -32,6 +32,12 @@ HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REPO="$(cd "$HERE/../.." && pwd)"
 REF="${PRR_REFERENCE:-/root/reference}"
 OUT="$REPO/oracle/_ref"
+# `build_ref.sh --locate` prints the reference tree it would read (nothing when
+# absent) and builds nothing: the one place that knows where the tree lives.
+if [ "${1:-}" = "--locate" ]; then
+    if [ -f "$REF/kernels/solver.cuh" ]; then echo "$REF"; fi
+    exit 0
+fi
 if [ ! -f "$REF/kernels/solver.cuh" ]; then
     echo "build_ref.sh: reference sources not found at $REF" >&2
     exit 2

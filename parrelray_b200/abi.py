@@ -188,6 +188,37 @@ def check(status: int, ctx=None) -> None:
 
 
 def defaults() -> FrameDesc:
+    """prr_frame_desc_defaults through the library."""
     d = FrameDesc()
     load().prr_frame_desc_defaults(C.byref(d))
+    return d
+
+
+def fill_defaults(d: FrameDesc) -> FrameDesc:
+    """The values prr_frame_desc_defaults writes (parrelray_b200/csrc/capi.cu), set here without
+    loading the library, so frame descriptors can be built where the library is not wanted (the
+    CPU side of the bench).  tests/test_abi.py checks the two agree byte for byte."""
+    import math
+
+    C.memset(C.byref(d), 0, C.sizeof(d))
+    d.width, d.height = 320, 180
+    d.ssaa, d.samples = SSAA_NONE, 1
+    d.vfov = 60.0 * math.pi / 180.0
+    d.cam_pos[0] = 30.0
+    d.cam_alpha, d.cam_beta = math.pi, 0.0
+    d.metric, d.mass, d.spin = METRIC_SCHWARZSCHILD, 1.0, 0.0
+    d.solver, d.mode, d.precision = SOLVER_RKF45, MODE_PHYSICAL, PREC_FP32
+    d.h, d.hmin, d.hmax, d.eps = 0.01, 0.0001, 0.1, 0.001
+    d.rtol = d.atol = 1e-6
+    d.rout, d.horizon_eps, d.max_steps = 100.0, 0.001, 10000
+    d.background_id, d.bg_filter, d.fxaa = -1, BG_RMS2X2, 0
+    d.fp64_delta, d.fp64_rfac = 1e-3, 1.05
+    d.nspheres = 0
+    for i in range(PRR_MAX_SPHERES):
+        d.spheres[i].texture_id = -1
+    d.emission = EMISSION_NONE
+    e = d.emis
+    e.index, e.height, e.r_in, e.r_out = 2.0, 0.3, 2.0, 30.0
+    e.spectral_index, e.absorb, e.gain, e.sense = 0.0, 0.0, 1.0, 1
+    e.temp_power, e.colormap = 0.0, CMAP_AFMHOT
     return d

@@ -99,6 +99,22 @@ def build_library(verbose: bool = False, ptxas_verbose: bool = False, defines: l
 COMPAT = PKG / "compat"
 
 
+def reference_tree() -> Path | None:
+    """The reference source tree the oracle recipe reads ($PRR_REFERENCE, or
+    the location oracle/ref/build_ref.sh knows), or None where it is absent
+    (e.g. on a machine that only runs prebuilt libraries)."""
+    env = os.environ.get("PRR_REFERENCE")
+    if env:
+        p = Path(env)
+        return p if (p / "kernels" / "solver.cuh").exists() else None
+    script = REPO / "oracle" / "ref" / "build_ref.sh"
+    if not script.exists():
+        return None
+    r = subprocess.run(["bash", str(script), "--locate"], capture_output=True, text=True)
+    loc = r.stdout.strip()
+    return Path(loc) if r.returncode == 0 and loc else None
+
+
 def build_metric_plugin(header: Path, name: str | None = None, verbose: bool = False,
                         lib_dir: Path | None = None, spherical: bool = False) -> Path:
     """Compiles an unchanged ParRelRay metric plug-in header (the files the
@@ -141,7 +157,9 @@ def build_plugins(verbose: bool = False) -> list[Path]:
     alternative Cartesian Schwarzschild header and its spherical-coordinate
     Schwarzschild header (with SPHERICAL), compiled unchanged."""
     outs = [build_metric_plugin(COMPAT / "metrics" / "kerr.cuh", "kerr", verbose)]
-    ref = Path(os.environ.get("PRR_REFERENCE", "/root/reference"))
+    ref = reference_tree()
+    if ref is None:
+        return outs
     for stem, name, sph in (("schwarzschild", "schwarzschild", False), ("flat", "flat", False),
                             ("schwarzschild - cart", "schwarzschildcart", False),
                             ("schwarzschild - sph", "schwarzschildsph", True)):
@@ -157,20 +175,26 @@ ORACLE_LIB = ORACLE_BUILD / "libprr_oracle.so"
 
 
 def build_oracle(verbose: bool = False) -> Path:
-    """CPU restatement (test infrastructure).  System g++ (has libgomp)."""
+    """CPU restatement (test infrastructure).  System g++ (has libgomp).  The
+    seeded texture generator (csrc/textures.cpp, integer arithmetic) is
+    compiled in as prr_oracle_make_texture, so CPU-only users of the oracle
+    (the bench's reference arm) make the workload's textures without loading
+    the product library."""
     ORACLE_BUILD.mkdir(parents=True, exist_ok=True)
     src = ORACLE_DIR / "prr_oracle.cpp"
-    if not _newer(ORACLE_LIB, [src, INCLUDE / "prr.h"]):
+    tex = CSRC / "textures.cpp"
+    if not _newer(ORACLE_LIB, [src, tex, INCLUDE / "prr.h"]):
         _run(["g++", "-O2", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
-              "-I", str(INCLUDE), str(src), "-o", str(ORACLE_LIB)], verbose)
+              "-Dprr_make_texture=prr_oracle_make_texture",
+              "-I", str(INCLUDE), str(src), str(tex), "-o", str(ORACLE_LIB)], verbose)
     return ORACLE_LIB
 
 
 def build_reference(verbose: bool = False) -> bool:
     """Reference sources compiled for the host (oracle/_ref); needs the
     reference tree, so only where it is mounted."""
-    ref = Path(os.environ.get("PRR_REFERENCE", "/root/reference"))
-    if not (ref / "kernels" / "solver.cuh").exists():
+    ref = reference_tree()
+    if ref is None:
         return False
     out = ORACLE_DIR / "_ref"
     libs = [out / f"libprr_ref_{t}.so" for t in ("schw", "flat", "kerr", "cart", "sph")] + [out / "libprr_refcu_kerr.so"]

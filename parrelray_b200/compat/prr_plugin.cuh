@@ -1,6 +1,6 @@
 #pragma once
-// prr_plugin.cuh - a REFERENCE-mode renderer built around an unchanged
-// ParRelRay metric plug-in header.
+// prr_plugin.cuh - the REFERENCE-mode and PHYSICAL-mode renderers built
+// around an unchanged ParRelRay metric plug-in header.
 //
 // The reference's "plug-in API" is compile-time: main/metric.h includes one
 // header from metrics/ that defines getMetric, getGeod, User_LOOP,
@@ -23,8 +23,14 @@
 //                   the header's hooks); writes the 48-byte Ray records;
 //   rayToRGB        the header's own kernel, launched as prr.cpp:317-319 does;
 //   k_plugin_collect per-sample colours and counters.
+// PHYSICAL-mode frames (FP32) run k_plugin_phys instead of k_plugin_trace:
+// the same hooks on the persistent, warp-compacted scheduler with the
+// PHYSICAL stepper (hook_stepper.cuh).
 // SSAA combine, FXAA and quantisation then run in the library as for the
 // built-in metrics.  Built with -fmad=false, as the built-in REFERENCE path.
+#include <algorithm>
+
+#include "hook_stepper.cuh"
 #include "kernels.cuh"
 #include "ref_stepper.cuh"
 
@@ -192,6 +198,87 @@ __global__ void __launch_bounds__(128) k_plugin_trace(const FrameParams *__restr
     }
 }
 
+// PHYSICAL mode through the header's hooks (hook_stepper.cuh) on the
+// persistent scheduler: CTAs stay resident and each lane integrates one ray
+// at a time, one RKF45 attempt per loop iteration; every `interval` attempts
+// (or when the whole warp is idle) the lanes whose ray has ended are refilled
+// together - __ballot_sync finds them, one atomicAdd on the frame's work
+// counter reserves __popc of them rays, each lane takes base + its rank - so a
+// warp never waits for its slowest ray.  Finished rays are written as Ray
+// records for the header's rayToRGB, as the reference's pipeline hands them
+// on (prr.cpp:317-319).  counters[C_WORK] must be zero at launch.
+__global__ void __launch_bounds__(128) k_plugin_phys(const FrameParams *__restrict__ fps, int frame, long long nrays,
+                                                     Ray *__restrict__ rays, float *__restrict__ state,
+                                                     unsigned long long *__restrict__ counters, int interval)
+{
+    constexpr unsigned FULL = 0xffffffffu;
+    const FrameParams &fp = fps[frame];
+    const int lane = threadIdx.x & 31;
+    const PluginHooks hk{make_camera(fp), make_space(fp, &fps[frame]), make_tracer(fp)};
+    prr::HookRay S;
+    long long rid = -1;
+    bool busy = false, need = true;
+    unsigned long long n_rays = 0, n_att = 0, n_acc = 0;
+    const unsigned ci = interval > 1 ? (unsigned)interval : 1u;
+    unsigned since = ci;
+    while (true) {
+        if (++since >= ci || __ballot_sync(FULL, busy) == 0) {
+            since = 0;
+            const unsigned m = __ballot_sync(FULL, need);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(&counters[prr::C_WORK], (unsigned long long)__popc(m));
+                base = __shfl_sync(FULL, base, leader);
+                if (need) {
+                    rid = (long long)(base + __popc(m & ((1u << lane) - 1u)));
+                    need = false;
+                    busy = rid < nrays;
+                    if (busy) {
+                        const int S_ = fp.samples;
+                        const long long pix = rid / S_;
+                        prr::hook_phys_init(fp, hk, (int)(pix % fp.width), (int)(pix / fp.width), (int)(rid - pix * S_), S);
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(FULL, busy) == 0) {
+            if (__ballot_sync(FULL, need) == 0) break;  // every lane has drawn past the last ray
+            since = ci;
+            continue;
+        }
+        if (!busy) continue;
+        if (prr::hook_phys_attempt(fp, hk, S) != prr::STEP_DONE) continue;
+        const prr::RefRay &R = S.R;
+        Ray T;
+        to_ray(R, T);
+        rays[rid] = T;
+        if (state) {
+            float *o = state + 12 * rid;
+            o[0] = R.uvx; o[1] = R.uvy; o[2] = (float)R.result;
+            o[3] = R.r.x; o[4] = R.r.y; o[5] = R.r.z; o[6] = R.r.w;
+            o[7] = R.u.x; o[8] = R.u.y; o[9] = R.u.z; o[10] = R.u.w;
+            o[11] = (float)R.accepted;
+        }
+        n_rays++;
+        n_att += (unsigned)R.attempts;
+        n_acc += (unsigned)R.accepted;
+        busy = false;
+        need = true;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n_rays += __shfl_xor_sync(FULL, n_rays, o);
+        n_att += __shfl_xor_sync(FULL, n_att, o);
+        n_acc += __shfl_xor_sync(FULL, n_acc, o);
+    }
+    if (lane == 0 && counters) {
+        atomicAdd(&counters[prr::C_RAYS], n_rays);
+        atomicAdd(&counters[prr::C_ATTEMPTS], n_att);
+        atomicAdd(&counters[prr::C_ACCEPTED], n_acc);
+    }
+}
+
 // Per-sample colour (Ray::u after rayToRGB) and outcome counters.
 __global__ void k_plugin_collect(const Ray *__restrict__ rays, long long nrays, float rout, float *__restrict__ rgb,
                                  unsigned long long *__restrict__ counters)
@@ -230,6 +317,26 @@ extern "C" const char *prr_plugin_name(void) { return PRR_PLUGIN_NAME; }
 // colours d_rgb (3 floats/ray) and, when non-null, the per-ray states d_state
 // (12 floats/ray) and counters.  Asynchronous on `stream`; returns a
 // cudaError_t.
+namespace prr_plugin {
+
+// rayToRGB as renderframe launches it (prr.cpp:317-319), then the colours
+// and outcome counters.
+inline cudaError_t colour_rays(const FrameParams &fp, const FrameParams *dfp, int frame, long long nrays, Ray *rays,
+                               float *d_rgb, unsigned long long *d_counters, cudaStream_t st)
+{
+    Camera cam = make_camera(fp);
+    Spacetime space = make_space(fp, dfp + frame);
+    Tracer trace = make_tracer(fp);
+    dim3 blocks(fp.samples * fp.width / 8 + 1, fp.height / 8 + 1), threads(8, 8);
+    rayToRGB<<<blocks, threads, 0, st>>>(rays, cam, space, trace, fp.samples);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_plugin_collect<<<(unsigned)((nrays + 255) / 256), 256, 0, st>>>(rays, nrays, fp.rout, d_rgb, d_counters);
+    return cudaGetLastError();
+}
+
+}  // namespace prr_plugin
+
 extern "C" int prr_plugin_trace(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays,
                                 float *d_state, float *d_rgb, unsigned long long *d_counters, void *stream)
 {
@@ -243,13 +350,31 @@ extern "C" int prr_plugin_trace(const void *h_fp, const void *d_fps, int frame, 
     k_plugin_trace<<<(unsigned)((nrays + block - 1) / block), block, 0, st>>>(dfp, frame, nrays, rays, d_state, d_counters);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
-    // rayToRGB as renderframe launches it (prr.cpp:317-319)
-    Camera cam = make_camera(fp);
-    Spacetime space = make_space(fp, dfp + frame);
-    Tracer trace = make_tracer(fp);
-    dim3 blocks(fp.samples * fp.width / 8 + 1, fp.height / 8 + 1), threads(8, 8);
-    rayToRGB<<<blocks, threads, 0, st>>>(rays, cam, space, trace, fp.samples);
+    return (int)colour_rays(fp, dfp, frame, nrays, rays, d_rgb, d_counters, st);
+}
+
+// PHYSICAL mode (FP32) on the persistent scheduler, same arguments and
+// outputs as prr_plugin_trace; d_counters is required (its work counter is
+// reset here).  Launches k_plugin_phys with resident CTAs of 128 threads on
+// every SM, a warp refill every 16 attempts.
+extern "C" int prr_plugin_trace_physical(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays,
+                                         float *d_state, float *d_rgb, unsigned long long *d_counters, void *stream)
+{
+    using namespace prr_plugin;
+    if (nrays <= 0) return (int)cudaSuccess;
+    if (!d_counters) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = (cudaStream_t)stream;
+    const FrameParams &fp = *(const FrameParams *)h_fp;
+    const FrameParams *dfp = (const FrameParams *)d_fps;
+    Ray *rays = (Ray *)d_rays;
+    int dev = 0, nsm = 0, bpsm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_plugin_phys, 128, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_counters + prr::C_WORK, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return (int)e;
+    const long long grid = std::min<long long>((long long)nsm * (bpsm > 0 ? bpsm : 1), (nrays + 127) / 128);
+    k_plugin_phys<<<(unsigned)grid, 128, 0, st>>>(dfp, frame, nrays, rays, d_state, d_counters, 16);
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-    k_plugin_collect<<<(unsigned)((nrays + 255) / 256), 256, 0, st>>>(rays, nrays, fp.rout, d_rgb, d_counters);
-    return (int)cudaGetLastError();
+    return (int)colour_rays(fp, dfp, frame, nrays, rays, d_rgb, d_counters, st);
 }

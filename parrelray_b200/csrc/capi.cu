@@ -174,7 +174,8 @@ prr_status prr_load_metric_plugin(prr_ctx *ctx, const char *path, int *metric_id
     auto rb = (size_t (*)(void))dlsym(h, "prr_plugin_ray_bytes");
     auto nm = (const char *(*)(void))dlsym(h, "prr_plugin_name");
     void *tr = dlsym(h, "prr_plugin_trace");
-    if (!abi || !fps || !rb || !nm || !tr) {
+    void *trp = dlsym(h, "prr_plugin_trace_physical");
+    if (!abi || !fps || !rb || !nm || !tr || !trp) {
         dlclose(h);
         fail(ctx, std::string("prr_load_metric_plugin: ") + path + " is not a prr metric plug-in (missing prr_plugin_* symbols)");
         return PRR_ERR_INVALID;
@@ -190,6 +191,7 @@ prr_status prr_load_metric_plugin(prr_ctx *ctx, const char *path, int *metric_id
     pl.handle = h;
     pl.ray_bytes = rb();
     pl.trace = (decltype(pl.trace))tr;
+    pl.trace_physical = (decltype(pl.trace_physical))trp;
     ctx->plugins.push_back(pl);
     *metric_id = PRR_METRIC_PLUGIN0 + (int)ctx->plugins.size() - 1;
     return PRR_OK;

@@ -151,6 +151,10 @@ extern "C" prr_status prr_graph_create(prr_ctx *ctx, const prr_frame_desc *frame
         ctx->err = "prr_graph_create: graphs record the PHYSICAL-mode persistent renderer; REFERENCE frames render with prr_render";
         s = PRR_ERR_UNSUPPORTED;
     }
+    if (s == PRR_OK && g->plan.plugin) {
+        ctx->err = "prr_graph_create: graphs record the built-in metrics; metric plug-in frames render with prr_render";
+        s = PRR_ERR_UNSUPPORTED;
+    }
     if (s != PRR_OK) { delete g; return s; }
     if (cudaSetDevice(ctx->device) != cudaSuccess) { ctx->err = "prr_graph_create: cudaSetDevice failed"; delete g; return PRR_ERR_CUDA; }
     const RenderPlan &plan = g->plan;

@@ -10,20 +10,25 @@
 // only scratch (the work counters, the frame table and the per-frame pixel
 // prefix) in one fixed static device array below.
 //
+// The host never waits for the GPU here: the frame table travels to the
+// scratch array inside the parameters of a small staging kernel (kernel
+// parameters are copied at launch, so the host tables may go away when the
+// call returns), and every launch is stream-ordered on the caller's stream.
+//
 // Limits and sharing rules:
 //  * at most PRR_NOALLOC_MAX_FRAMES frames per call (larger n is rejected
 //    with PRR_ERR_INVALID before anything is launched);
 //  * the scratch array exists once per device for the life of the process
 //    (every GPU that loads the library holds its PRR_NOALLOC_SCRATCH_BYTES);
 //  * every call on a device shares it and it keeps the previous call's
-//    contents, so the counters are cleared at the start of each call, and
-//    calls whose GPU work overlaps (different streams, or host threads
-//    without ordering) race on it: order them on one stream;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//    contents, so the staging kernel clears the counters at the start of
+//    each call, and calls whose GPU work overlaps (different streams, or host
+//    threads without ordering) race on it: order them on one stream;
+//  * each call looks up the array's device address with cudaGetSymbolAddress
+//    (it allocates nothing), with the calling thread's current device; the
+//    first call on a device can load the library's device code there, so
+//    make that first call before any stream capture on that device.
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "kernels.cuh"
@@ -45,9 +50,34 @@ static_assert(kFramesOffset + PRR_NOALLOC_MAX_FRAMES * sizeof(FrameParams) <= kS
 // The scratch: work counters | pixel prefix (n+1) | frame table (n).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void *g_scratch_addr[kMaxDevices] = {};
+// Frames staged per launch of k_noalloc_stage: the chunk rides in the kernel
+// parameters (at most 32,764 bytes of parameters per launch on sm_70 and
+// later with CUDA 12.1+ drivers; kept well below that).
+constexpr int kChunkFrames = 32;
+struct FrameChunk {
+    int first, count, nframes, clear;
+    long long total_pixels;
+    FrameParams f[kChunkFrames];
+};
+static_assert(sizeof(FrameChunk) + 64 <= 32000, "staging chunk exceeds the kernel parameter space");
+static_assert(sizeof(FrameParams) % 4 == 0, "frame parameters are copied as 32-bit words");
+
+// Copies one chunk of the frame table into the scratch array, writes the
+// chunk's entries of the pixel prefix (and its end on the last chunk) and,
+// on the first chunk, clears the counters.
+__global__ void k_noalloc_stage(const FrameChunk c, unsigned char *scratch)
+{
+    unsigned long long *counters = (unsigned long long *)scratch;
+    long long *begin = (long long *)(scratch + kBeginOffset);
+    FrameParams *fps = (FrameParams *)(scratch + kFramesOffset);
+    const unsigned words = (unsigned)(c.count * sizeof(FrameParams) / 4);
+    const unsigned *src = (const unsigned *)c.f;
+    unsigned *dst = (unsigned *)(fps + c.first);
+    for (unsigned i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+    if ((int)threadIdx.x < c.count) begin[c.first + threadIdx.x] = c.f[threadIdx.x].pix_begin;
+    if (threadIdx.x == 0 && c.first + c.count == c.nframes) begin[c.nframes] = c.total_pixels;
+    if (c.clear && threadIdx.x < C_COUNT) counters[threadIdx.x] = 0ull;
+}
 
 void set_err(char *buf, size_t len, const std::string &msg)
 {
@@ -72,24 +102,19 @@ extern "C" prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, co
     }
     if (!d_rgb8) { set_err(errbuf, errlen, "d_rgb8 (device output) is required"); return PRR_ERR_INVALID; }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         set_err(errbuf, errlen, "no usable CUDA device");
         return PRR_ERR_NO_DEVICE;
     }
-    // once per device, with that device current: the array's device address
+    // the array's device address on the current device (in host code its
+    // name is only a host-side stand-in)
     void *scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_addr[dev]) {
-            cudaError_t e = cudaGetSymbolAddress(&g_scratch_addr[dev], g_noalloc_scratch);
-            if (e != cudaSuccess) {
-                g_scratch_addr[dev] = nullptr;
-                set_err(errbuf, errlen, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-                return PRR_ERR_CUDA;
-            }
-        }
-        scratch = g_scratch_addr[dev];
+    cudaError_t e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+    if (e != cudaSuccess || !scratch) {
+        cudaGetLastError();
+        set_err(errbuf, errlen, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+        return PRR_ERR_CUDA;
     }
     // Validate and lay out the frames with a context that owns nothing: its
     // texture slots point at the caller's device textures.
@@ -121,29 +146,38 @@ extern "C" prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, co
     }
     cudaStream_t st = (cudaStream_t)stream;
     unsigned char *base = (unsigned char *)scratch;
-    unsigned long long *counters = (unsigned long long *)base;
-    long long *begin = (long long *)(base + kBeginOffset);
-    FrameParams *fps = (FrameParams *)(base + kFramesOffset);
     int nsm = 0;
-    cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, kCountersBytes, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(begin, plan.pix_begin.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(fps, plan.fp.data(), n * sizeof(FrameParams), cudaMemcpyHostToDevice, st);
-    // the host tables are freed on return: complete the copies first
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // the frame table, the pixel prefix and cleared counters, stream-ordered
+    for (int first = 0; first < n && e == cudaSuccess; first += kChunkFrames) {
+        FrameChunk c;
+        memset(&c, 0, sizeof(c));
+        c.first = first;
+        c.count = n - first < kChunkFrames ? n - first : kChunkFrames;
+        c.nframes = n;
+        c.clear = first == 0;
+        c.total_pixels = plan.total_pixels;
+        memcpy(c.f, plan.fp.data() + first, c.count * sizeof(FrameParams));
+        k_noalloc_stage<<<1, 256, 0, st>>>(c, base);
+        e = cudaGetLastError();
+    }
     PersistentArgs a;
     memset(&a, 0, sizeof(a));
-    a.frames = fps;
-    a.frame_pix_begin = begin;
+    a.frames = (const FrameParams *)(base + kFramesOffset);
+    a.frame_pix_begin = (const long long *)(base + kBeginOffset);
     a.nframes = n;
     a.total_pixels = plan.total_pixels;
     a.image = d_rgbf;
     a.rgb8 = d_rgb8;
-    a.counters = counters;
-    a.compaction_interval = 1;
+    a.counters = (unsigned long long *)base;
     a.emission = plan.any_emission;
-    const int block = 128;
-    int bpsm = persistent_occupancy(plan.precision, 0, block, 1, plan.any_emission);
+    // the launch shape prr_autotune picks for the 1080p Kerr workload: CTAs of
+    // 64 threads at their occupancy limit, one pixel per thread, a warp refill
+    // every 64 attempts
+    const int block = 64;
+    a.compaction_interval = 64;
+    a.rays_per_thread = 1;
+    const int bpsm = persistent_occupancy(plan.precision, 0, block, 1, plan.any_emission);
     if (e == cudaSuccess) e = launch_persistent(a, plan.precision, block, bpsm > 0 ? bpsm : 1, nsm, st);
     for (int f = 0; f < n && e == cudaSuccess; f++) {
         const FrameParams &p = plan.fp[f];

@@ -35,8 +35,11 @@ struct MetricPlugin {
     std::string path, name;
     void *handle = nullptr;
     size_t ray_bytes = 0;
+    // REFERENCE mode (prr_plugin_trace) and PHYSICAL mode (prr_plugin_trace_physical), same arguments
     int (*trace)(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays, float *d_state,
                  float *d_rgb, unsigned long long *d_counters, void *stream) = nullptr;
+    int (*trace_physical)(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays, float *d_state,
+                          float *d_rgb, unsigned long long *d_counters, void *stream) = nullptr;
 };
 
 struct prr_ctx {
@@ -78,6 +81,7 @@ struct RenderPlan {
     int precision = PRR_PREC_FP32;
     bool any_fxaa = false;
     bool any_emission = false;  // some frame has plasma emission
+    bool plugin = false;        // the frames use metric plug-ins (then every frame does)
 };
 
 // The plug-in of a frame's metric id, or null for a built-in metric.

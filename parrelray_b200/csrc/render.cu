@@ -135,6 +135,7 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
     plan.precision = frames[0].precision;
     plan.any_fxaa = false;
     plan.any_emission = false;
+    plan.plugin = false;
     for (int f = 0; f < n; f++) {
         const prr_frame_desc &d = frames[f];
         FrameParams &p = plan.fp[f];
@@ -162,7 +163,12 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
         const MetricPlugin *plugin = frame_plugin(ctx, d.metric);
         if ((d.metric < PRR_METRIC_FLAT || d.metric > PRR_METRIC_KERR) && !plugin)
             return bad(ctx, f, "unknown metric (built-in 0-2, or an id from prr_load_metric_plugin)");
-        if (plugin && d.mode != PRR_MODE_REFERENCE) return bad(ctx, f, "metric plug-ins render in REFERENCE mode");
+        if (f == 0) plan.plugin = plugin != nullptr;
+        if ((plugin != nullptr) != plan.plugin)
+            return bad(ctx, f, "frames with metric plug-ins and frames with built-in metrics need separate calls");
+        if (plugin && d.mode == PRR_MODE_PHYSICAL && d.precision != PRR_PREC_FP32)
+            return bad(ctx, f, "metric plug-ins render PHYSICAL mode in FP32 (a header's getGeod computes in FP32)");
+        if (plugin && d.emission != PRR_EMISSION_NONE) return bad(ctx, f, "metric plug-ins render without plasma emission");
         if (!std::isfinite(d.mass) || d.mass < 0.0f) return bad(ctx, f, "mass must be >= 0");
         // M = 0 is allowed for Schwarzschild: the reference renders its example deck (input/sim.params:30,52) so
         if (d.metric == PRR_METRIC_KERR && d.mass <= 0.0f) return bad(ctx, f, "Kerr needs mass > 0");
@@ -303,7 +309,7 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
     };
 
     bool trace_timed = false;
-    if (plan.mode == PRR_MODE_REFERENCE || ctx->schedule == PRR_SCHED_PLAIN) {
+    if (plan.mode == PRR_MODE_REFERENCE || ctx->schedule == PRR_SCHED_PLAIN || plan.plugin) {
         long long max_rays = 0;
         for (const auto &p : plan.fp) max_rays = std::max(max_rays, (long long)p.width * p.height * p.samples);
         if ((s = alloc(ctx, ctx->sample_rgb, (size_t)max_rays * 3 * sizeof(float), "per-sample colours")) != PRR_OK) return s;
@@ -315,7 +321,8 @@ prr_status run_plan(prr_ctx *ctx, const RenderPlan &plan, uint8_t *d_rgb8, float
             long long nr = (long long)p.width * p.height * p.samples;
             if (const MetricPlugin *pl = frame_plugin(ctx, p.metric)) {
                 if ((s = alloc(ctx, ctx->rays, (size_t)nr * pl->ray_bytes, "plug-in ray records")) != PRR_OK) return s;
-                PRR_CK(ctx, (cudaError_t)pl->trace(&p, d_fp, f, nr, ctx->rays.p, nullptr, rgb, counters, st));
+                auto tr = p.mode == PRR_MODE_PHYSICAL ? pl->trace_physical : pl->trace;
+                PRR_CK(ctx, (cudaError_t)tr(&p, d_fp, f, nr, ctx->rays.p, nullptr, rgb, counters, st));
                 launches += 3;
             } else if (plan.mode == PRR_MODE_REFERENCE) {
                 PRR_CK(ctx, launch_ref_trace(d_fp, f, nr, nullptr, rgb, counters, st));
@@ -395,7 +402,9 @@ prr_status trace_plan(prr_ctx *ctx, const RenderPlan &plan, float *h_state, doub
     PRR_CK(ctx, cudaEventRecord(ctx->e0, st));
     if (const MetricPlugin *pl = frame_plugin(ctx, p.metric)) {
         if ((s = alloc(ctx, ctx->rays, (size_t)nr * pl->ray_bytes, "plug-in ray records")) != PRR_OK) return s;
-        PRR_CK(ctx, (cudaError_t)pl->trace(&p, d_fp, 0, nr, ctx->rays.p, (float *)ctx->state.p, rgb, counters, st));
+        if (h_state64) { ctx->err = "prr_trace_rays_f64: metric plug-ins trace in FP32"; return PRR_ERR_UNSUPPORTED; }
+        auto tr = p.mode == PRR_MODE_PHYSICAL ? pl->trace_physical : pl->trace;
+        PRR_CK(ctx, (cudaError_t)tr(&p, d_fp, 0, nr, ctx->rays.p, (float *)ctx->state.p, rgb, counters, st));
         ctx->last_launches = 3;
     } else if (plan.mode == PRR_MODE_REFERENCE) {
         PRR_CK(ctx, launch_ref_trace(d_fp, 0, nr, (float *)ctx->state.p, rgb, counters, st));

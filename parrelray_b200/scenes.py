@@ -59,8 +59,7 @@ def make_frame(width: int, height: int, *, r: float, incl_deg: float, fov_deg: f
                horizon_eps: float = 0.01, max_steps: int = 10000, spheres=(), background: bool = True,
                h: float = 0.01, hmin: float = 1e-4, hmax: float = 0.1, eps: float = 1e-3,
                bg_filter: int = abi.BG_RMS2X2) -> abi.FrameDesc:
-    d = abi.FrameDesc()
-    abi.load().prr_frame_desc_defaults(d)
+    d = abi.fill_defaults(abi.FrameDesc())
     d.width, d.height = width, height
     d.samples = samples
     d.ssaa = abi.SSAA_NONE if samples == 1 else abi.SSAA_REGULAR

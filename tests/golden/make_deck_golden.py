@@ -154,8 +154,9 @@ def main() -> int:
     rp = RefParser()
     out = {"source": "reference readParams/par/pari/parf/headerExists/parExists/checkFrame (host build)",
            "decks": DECKS, "results": {name: rp.table(text) for name, text in DECKS.items()}}
-    ref_inputs = Path("/root/reference/input")
-    if ref_inputs.exists():
+    tree = build.reference_tree()
+    ref_inputs = tree / "input" if tree else None
+    if ref_inputs and ref_inputs.exists():
         # the reference's example decks, parsed by the reference (tables only)
         for p in sorted(ref_inputs.glob("*.params")):
             out["results"]["reference_" + p.stem] = rp.table(p.read_text(encoding="utf-8", errors="surrogateescape"))

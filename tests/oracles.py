@@ -68,8 +68,26 @@ class Oracle:
                                                   C.POINTER(C.c_longlong), C.c_longlong, C.c_int, C.POINTER(C.c_double)]
         lib.prr_oracle_set_plasma.restype = C.c_int
         lib.prr_oracle_set_plasma.argtypes = [C.POINTER(abi.PlasmaDesc)]
+        lib.prr_oracle_make_texture.restype = C.c_int
+        lib.prr_oracle_make_texture.argtypes = [C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_uint8)]
         self.lib = lib
         self._plasma_keep = None
+
+    def make_texture(self, kind: int, seed: int, w: int, h: int) -> np.ndarray:
+        """The seeded procedural texture of prr_make_texture, made without the product library."""
+        out = np.empty((h, w, 4), dtype=np.uint8)
+        if self.lib.prr_oracle_make_texture(kind, seed, w, h, out.ctypes.data_as(C.POINTER(C.c_uint8))):
+            raise ValueError("bad texture request")
+        return out
+
+    def standard_textures(self) -> dict[int, np.ndarray]:
+        """scenes.standard_textures() (the starfield and the three sphere textures), made here."""
+        from parrelray_b200 import scenes
+
+        tex = {scenes.SKY_ID: self.make_texture(1, 1234, *scenes.SKY_TEX_SIZE)}
+        for k in range(3):
+            tex[scenes.SPHERE_ID0 + k] = self.make_texture(0, 100 + k, *scenes.SPHERE_TEX_SIZE)
+        return tex
 
     def set_plasma(self, density=None, lo=None, hi=None, temperature=None, velocity=None) -> None:
         """The plasma grid of GRID emission, as Context.upload_plasma takes it; no density clears it."""
@@ -172,6 +190,42 @@ class Oracle:
         g = (C.c_double * 16)()
         self.lib.prr_oracle_metric(metric, M, a, pa, g)
         return np.array(g[:]).reshape(4, 4)
+
+
+def kerr_criticality(state: np.ndarray, M: float, a: float, n_grid: int = 48) -> np.ndarray:
+    """Per ray, |min over r in [r_+, 6M] of R(r)/r^4|, with R the Boyer-Lindquist radial potential
+    (r^2 + a^2 - a xi)^2 - Delta (eta + (xi - a)^2) of the ray's conserved xi = L_z/E and
+    eta = Q/E^2 (Carter), evaluated from a Kerr-Schild state (columns 3..10 of Oracle.trace /
+    Context.trace_rays: x y z t, u^x u^y u^z u^t).  A photon orbit is a double root of R; for
+    Schwarzschild min R/r^4 = 1 - (b/b_c)^2, so a value below 2 delta marks a ray within a
+    relative delta of the critical impact parameter.  The same test as the renderer's
+    near_critical (parrelray_b200/csrc/phys_stepper.cuh), vectorised in FP64."""
+    st = np.asarray(state, dtype=np.float64)
+    x, y, z = st[:, 3], st[:, 4], st[:, 5]
+    u = st[:, 7:11]
+    R2 = x * x + y * y + z * z
+    bq = R2 - a * a
+    r = np.sqrt(0.5 * (bq + np.sqrt(bq * bq + 4 * a * a * z * z)))
+    q = r * r + a * a
+    f = 2 * M * r ** 3 / (r ** 4 + a * a * z * z)
+    l = np.stack([(r * x + a * y) / q, (r * y - a * x) / q, z / r, np.ones_like(r)], 1)
+    eta = np.array([1.0, 1.0, 1.0, -1.0])
+    L = np.sum(l * u, 1)
+    p = eta * u + (f * L)[:, None] * l  # p_m = g_mn u^n
+    E = -p[:, 3]
+    Lz = x * p[:, 1] - y * p[:, 0]
+    ct = z / r
+    st2 = np.maximum(1.0 - ct * ct, 1e-300)
+    sn = np.sqrt(st2)
+    pth = (ct / sn) * (x * p[:, 0] + y * p[:, 1]) - r * sn * p[:, 2]
+    Q = pth * pth + ct * ct * (-a * a * E * E + Lz * Lz / st2)
+    xi, et = Lz / E, Q / (E * E)
+    rp = M + np.sqrt(max(M * M - a * a, 0.0))
+    rr = np.linspace(rp * 1.0001, 6.0 * M, n_grid + 1)[None, :]
+    A = rr * rr + a * a - a * xi[:, None]
+    D = rr * rr - 2 * M * rr + a * a
+    pot = (A * A - D * (et[:, None] + (xi[:, None] - a) ** 2)) / rr ** 4
+    return np.abs(pot.min(axis=1))
 
 
 def _safe_dir(base: Path) -> Path:

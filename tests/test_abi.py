@@ -29,7 +29,7 @@ def test_struct_layouts_match(built):
 
 def test_version_and_status_strings(built):
     lib = abi.load()
-    assert lib.prr_abi_version() == 3
+    assert lib.prr_abi_version() == 4
     assert lib.prr_status_string(abi.OK) == b"ok"
     assert b"device" in lib.prr_status_string(abi.ERR_NO_DEVICE)
 
@@ -41,6 +41,14 @@ def test_defaults_follow_the_reference_deck(built):
     assert d.eps == pytest.approx(1e-3)
     assert d.horizon_eps == pytest.approx(1e-3)
     assert d.solver == abi.SOLVER_RKF45 and d.max_steps == 10000
+
+
+def test_library_free_defaults_equal_the_library_defaults(built):
+    """scenes builds frames with abi.fill_defaults (no library load); it must write the same bytes
+    as prr_frame_desc_defaults."""
+    a = bytes(abi.defaults())
+    b = bytes(abi.fill_defaults(abi.FrameDesc()))
+    assert a == b
 
 
 def test_null_arguments_are_rejected_without_a_device(built):

@@ -19,10 +19,11 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from parrelray_b200 import Deck, PrrError, abi, scenes
+from parrelray_b200 import Deck, PrrError, abi, build, scenes
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "decks.json"
-REF_INPUT = Path("/root/reference/input")
+_REF = build.reference_tree()
+REF_INPUT = _REF / "input" if _REF else Path("/nonexistent")
 
 
 def _f(x):

@@ -14,6 +14,11 @@ with prr_load_metric_plugin renders what the reference renders with it.
   (states (r, theta, phi, t), built with SPHERICAL) against the reference's
   own frame pipeline built with the same header and switch
   (tests/golden/plugin_sph_*.npz).
+* PHYSICAL mode through a header's hooks on the persistent scheduler: the
+  reference's own metrics/schwarzschild.cuh renders the single-frame
+  Schwarzschild workload (320x180, tolerance 1e-6) within 1/255 of the FP64
+  host oracle on >= 99.9% of pixels, and the shipped Kerr header renders the
+  Kerr test frame (a = 0.95, 2x2 SSAA, three spheres) to the same bar.
 """
 import numpy as np
 import pytest
@@ -89,10 +94,16 @@ def test_plugin_loading_rules(gpu, small_textures):
     from parrelray_b200 import scenes
 
     gpu.upload_textures(small_textures)
-    d = scenes.schwarzschild_320()
-    d.metric = a  # PHYSICAL mode
+    d = scenes.schwarzschild_320(precision=abi.PREC_FP64)
+    d.metric = a  # PHYSICAL mode in FP64: a header's getGeod is FP32
     with pytest.raises(abi.PrrError) as e:
         gpu.render(d)
+    assert e.value.status == abi.ERR_INVALID
+    b = scenes.schwarzschild_320()
+    d = scenes.schwarzschild_320()
+    d.metric = a
+    with pytest.raises(abi.PrrError) as e:  # plug-in and built-in frames in one call
+        gpu.render([d, b])
     assert e.value.status == abi.ERR_INVALID
     d.metric = abi.METRIC_PLUGIN0 + 7  # not loaded
     d.mode = abi.MODE_REFERENCE
@@ -158,3 +169,54 @@ def test_reference_spherical_header(gpu, case):
     imgs, _, _ = gpu.render(d)
     npx = d.width * d.height
     assert pixel_rule(imgs[0], quantize(z["image"])) >= min(0.999, 1 - 1.0 / npx - 1e-12)
+
+
+def test_reference_schwarzschild_header_physical_mode(gpu, oracle, std_textures):
+    """The reference's own metrics/schwarzschild.cuh, compiled unchanged, renders the single-frame
+    Schwarzschild workload (M = 1, camera r = 30M, inclination 85 deg, FOV 60 deg, 320x180, one
+    sphere R = 1M at r = 10M, tolerance 1e-6) in PHYSICAL mode on the persistent scheduler; the
+    header's User_ENDLOOP stops at r <= rs + 0.001 (metrics/schwarzschild.cuh:70), so the oracle
+    stops there too."""
+    from parrelray_b200 import scenes
+
+    p = plugin_path("schwarzschild")
+    if not p.exists():
+        pytest.skip(f"{p.name} is built only where the reference's headers are available")
+    d = scenes.schwarzschild_320(horizon_eps=0.001)
+    gpu.upload_textures(std_textures)
+    d.metric = gpu.load_metric_plugin(p)
+    imgs, _, stats = gpu.render(d)
+    assert stats.rays == 57600 and stats.attempts >= stats.accepted > 0
+    assert stats.n_infinite == 0 and stats.n_math_error == 0
+    assert stats.n_intersection > 0 and stats.n_captured > 0 and stats.n_escaped > 0
+    d64 = scenes.schwarzschild_320(horizon_eps=0.001, precision=abi.PREC_FP64)
+    _, _, ref = oracle.render(d64, std_textures, precision=1)
+    ok = pixel_rule(imgs[0], quantize(ref))
+    assert ok >= 0.999, ok
+    # the built-in PHYSICAL renderer of the same metric agrees too
+    b = scenes.schwarzschild_320(horizon_eps=0.001)
+    bimg, _, _ = gpu.render(b)
+    assert pixel_rule(imgs[0], bimg[0]) >= 0.999
+
+
+def test_shipped_kerr_header_physical_mode(gpu, oracle, small_textures):
+    """The Kerr header shipped in compat/metrics/kerr.cuh (Christoffel-table geodesic, as a plug-in
+    author would write it) in PHYSICAL mode: a = 0.95, 64x36 with 2x2 SSAA and FXAA, three spheres,
+    tolerance 1e-6, against the FP64 host oracle.  Its User_ENDLOOP stops at r <= r_+ + 0.001."""
+    from parrelray_b200 import scenes
+
+    sph = [(*scenes.orbit_point(orb, ph), rad, scenes.SPHERE_ID0 + k)
+           for k, (rad, orb, ph) in enumerate(scenes.KERR_1080P_SPHERES)]
+    kw = dict(r=25.0, incl_deg=80.0, fov_deg=50.0, metric=abi.METRIC_KERR, mass=1.0, spin=0.95, samples=4,
+              fxaa=True, spheres=sph, horizon_eps=0.001)
+    d = scenes.make_frame(64, 36, **kw)
+    gpu.upload_textures(small_textures)
+    d.metric = gpu.load_metric_plugin(plugin_path("kerr"))
+    state, rgb, stats = gpu.trace_rays(d)
+    assert stats.rays == d.nrays and stats.attempts > 0
+    d64 = scenes.make_frame(64, 36, precision=abi.PREC_FP64, **kw)
+    st64, _, ref = oracle.render(d64, small_textures, precision=1)
+    assert np.mean(state[:, 2] == st64[:, 2]) >= 0.995
+    imgs, _, _ = gpu.render(d)
+    ok = pixel_rule(imgs[0], quantize(ref))
+    assert ok >= 0.999 - 1.0 / (d.width * d.height), ok

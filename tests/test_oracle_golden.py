@@ -16,17 +16,19 @@ from parrelray_b200 import abi, scenes
 
 GOLDEN = Path(__file__).parent / "golden"
 # the built-in metrics; plugin_* fixtures hold a reference metric header's own
-# outputs (tests/test_gpu_plugins.py) and have no restatement here
-CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("plugin_"))
+# outputs (tests/test_gpu_plugins.py) and have no restatement here; full_*
+# fixtures are the full-size single-frame workload in slim form
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("plugin_", "full_")))
+FULL_CASES = sorted(p.stem for p in GOLDEN.glob("full_*.npz"))
 
 
 def load_case(name):
-    from golden.make_golden import ALL_CASES as SPECS, case_frame, textures
+    from golden.make_golden import ALL_CASES as SPECS, case_frame, case_textures
 
     z = np.load(GOLDEN / f"{name}.npz")
     d, meta = case_frame(SPECS[name])
     assert json.loads(str(z["meta"]))["W"] == meta["W"]
-    return d, textures(), z
+    return d, case_textures(SPECS[name]), z
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -41,6 +43,31 @@ def test_oracle_reproduces_reference_bitwise(oracle, name):
     assert np.array_equal(img, z["image"])
     fx = oracle.post(rgb, d.width, d.height, d.samples, True)
     assert np.array_equal(fx[1:-1, 1:-1], z["fxaa"][1:-1, 1:-1])
+
+
+@pytest.mark.parametrize("name", FULL_CASES)
+def test_oracle_reproduces_full_size_reference_frame(oracle, name):
+    """The 320x180 single-frame workload in the reference's own solver: the restatement gives
+    the same result, quantised direction and 8-bit colour for every one of its 57,600 rays."""
+    from golden.make_golden import slim
+
+    d, tex, z = load_case(name)
+    st, rgb = oracle.trace(d, tex)
+    mine = slim(st[:, :11].astype(np.float32), rgb)
+    for k in ("result", "direction", "rgb8"):
+        assert np.array_equal(mine[k], z[k]), k
+    res = np.bincount(z["result"].astype(int), minlength=5)
+    assert res[abi.RESULT_SUCCESS] > 0 and res[abi.RESULT_INTERSECTION] > 0
+
+
+def test_euler_case_exercises_the_euler_solver():
+    from golden.make_golden import ALL_CASES, case_frame
+
+    d, meta = case_frame(ALL_CASES["euler_64x36_s1"])
+    assert d.solver == abi.SOLVER_EULER and meta["solver"] == "euler"
+    z = np.load(GOLDEN / "euler_64x36_s1.npz")
+    res = np.bincount(z["state"][:, 2].astype(int), minlength=5)
+    assert res[abi.RESULT_SUCCESS] > 0 and res[abi.RESULT_INTERSECTION] > 0
 
 
 @pytest.mark.parametrize("name", CASES)

@@ -54,3 +54,13 @@ def test_sphere_texture_has_checkerboard(built):
     cell_a = t[0:16, 0:32, :3].mean()
     cell_b = t[0:16, 32:64, :3].mean()
     assert abs(cell_a - cell_b) > 40
+
+
+def test_oracle_makes_the_same_textures(oracle):
+    """The CPU side of the bench makes the workload's textures with the oracle library (which
+    compiles the same generator), so it never loads the product library: same bytes."""
+    std = scenes.standard_textures()
+    mine = oracle.standard_textures()
+    assert sorted(std) == sorted(mine)
+    for k in std:
+        assert np.array_equal(std[k], mine[k]), k

@@ -20,14 +20,24 @@ from parrelray_b200 import abi, scenes
 pytestmark = pytest.mark.gpu
 
 
-def frames_pair():
+def frames_pair(precision=abi.PREC_FP32):
     sph = [(*scenes.orbit_point(orb, ph), rad, scenes.SPHERE_ID0 + k)
            for k, (rad, orb, ph) in enumerate(scenes.KERR_1080P_SPHERES)]
     a = scenes.make_frame(64, 36, r=25.0, incl_deg=80.0, fov_deg=50.0, metric=abi.METRIC_KERR, spin=0.95, samples=4,
-                          fxaa=True, spheres=sph)
+                          fxaa=True, spheres=sph, precision=precision)
     b = scenes.make_frame(48, 30, r=20.0, incl_deg=60.0, fov_deg=60.0, metric=abi.METRIC_SCHWARZSCHILD, samples=1,
-                          fxaa=False, spheres=sph[:1])
+                          fxaa=False, spheres=sph[:1], precision=precision)
     return [a, b]
+
+
+FRAME_SETS = {
+    # the FP32 renderer on a Kerr frame with SSAA + FXAA and a Schwarzschild frame without
+    "fp32": lambda: frames_pair(abi.PREC_FP32),
+    # the same frames through the FP64 renderer
+    "fp64": lambda: frames_pair(abi.PREC_FP64),
+    # plasma emission from a thick disk (the FP32 renderer's emission instantiation)
+    "emission": lambda: [scenes.eht_disk(48, samples=4)],
+}
 
 
 def device_textures(textures):
@@ -43,13 +53,23 @@ def device_textures(textures):
     return keep, ptrs, w, h
 
 
-def test_noalloc_matches_context_render_on_two_calls(gpu, small_textures):
+@pytest.mark.parametrize("kind", sorted(FRAME_SETS))
+def test_noalloc_matches_context_render_on_two_calls(gpu, small_textures, kind):
     import torch
 
+    from parrelray_b200 import LaunchConfig
+
     lib = abi.load()
-    frames = frames_pair()
+    frames = FRAME_SETS[kind]()
     gpu.upload_textures(small_textures)
-    ref8, reff, _ = gpu.render(frames, want_float=True)
+    # the context renders with the launch shape the entry point uses (64-thread CTAs at their
+    # occupancy limit, a refill every 64 attempts), so both run the same kernel instantiation
+    saved = gpu.launch_config()
+    gpu.set_schedule(abi.SCHED_PERSISTENT, LaunchConfig(64, 0, 64, 1))
+    try:
+        ref8, reff, _ = gpu.render(frames, want_float=True)
+    finally:
+        gpu.set_schedule(abi.SCHED_PERSISTENT, saved)
     keep, ptrs, w, h = device_textures(small_textures)
     npx = sum(f.width * f.height for f in frames)
     out8 = torch.empty(npx * 3, dtype=torch.uint8, device="cuda")
@@ -70,7 +90,7 @@ def test_noalloc_matches_context_render_on_two_calls(gpu, small_textures):
             n = f.width * f.height * 3
             img8 = got8[off:off + n].reshape(f.height, f.width, 3)
             # same kernels on the same frames: identical bytes
-            assert np.array_equal(img8, ref8[k]), f"call {call}, frame {k}"
+            assert np.array_equal(img8, ref8[k]), f"{kind}: call {call}, frame {k}"
             if not f.fxaa:  # with FXAA, d_rgbf holds the pre-FXAA combined image
                 assert np.array_equal(gotf[off:off + n].reshape(f.height, f.width, 3), reff[k])
             off += n
