@@ -6,23 +6,38 @@ combine, FXAA, quantisation).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 is launched with torch.distributed.run, one rank per GPU (NCCL only for
-the barrier and the max-over-ranks timing); every rank renders its own frame
-of a camera orbit (weak scaling, no data-path collective).
+N > 1 is launched with torch.distributed.run, one rank per GPU; every step
+renders N frames of a camera orbit (weak scaling), the ranks pulling them
+from a shared counter in the process group's store (parrelray_b200/shard.py);
+NCCL carries only the barrier and the max-over-ranks time, nothing on the
+data path.
 
 Reported (one JSON line on rank 0):
   value           whole-job Mrays/s, device time (CUDA events), inputs resident
   e2e             Mrays/s through prr_render with host buffers: the frame
                   descriptor in, the 8-bit image out (pinned), copies timed
   roofline        FP32 FLOP/s of the tracing kernel: attempts x F_attempt /
-                  kernel time, against the measured FMA peak of the same GPU
-  plain           the plain one-ray-per-thread schedule on the same GPU
-  accuracy        fraction of pixels within 1/255 of an FP64 render
-  cpu_baseline    the reference's own solver (host build, Kerr plug-in) on a
-                  bounded sample of the same frame, on this host's cores
+                  kernel time against the measured FMA peak of the same GPU,
+                  and the FP32 operations ncu counts per attempt beside it
+  plain           the plain one-ray-per-thread schedule on the same GPU, with
+                  the scheduler's and the geodesic form's shares of the speed-up
+  accuracy        the image against an FP64 GPU render, and a seeded set of
+                  the frame's rays against the FP64 host oracle
+  trajectory      240 frames under one CUDA graph / per-frame / plain (all 240)
+  uneven          64 uneven requests: split precision, all-FP64, all-FP32
+  adjoint         one gradient of the 512x512 differentiable render
+  adam_fit        200 Adam iterations of (a, i) through the adjoint
+  emission        the EHT-like disk frame with and without emission
+  plugin_kerr_header  the frame through the Kerr header as a metric plug-in
+  cpu_baseline    the FP64 host restatement on a seeded sample of the frame's
+                  rays, on this host's cores; the reference's own solver at
+                  eps 1e-3 for context; the 320x180 Schwarzschild frame through
+                  the reference's host build whole, beside the GPU
   reference_cuda  the reference's own CUDA build (its sources, nvcc, sm_100a)
                   on this GPU: trace_RKF at eps 1e-6 on a band of rows, and
                   its whole frame pipeline at the deck's eps 1e-3
+`--impl reference` runs the CPU arm alone: the FP64 host restatement on a
+fixed seeded sample of the frame's rays each step (see run_reference_arm).
 """
 from __future__ import annotations
 
@@ -55,6 +70,16 @@ FLOPS_STAGES = 492
 FLOPS_GEOD_KERR = 168
 F_ATTEMPT = 6 * FLOPS_GEOD_KERR + FLOPS_STAGES
 
+# FP32 operations the tracing kernel actually executes per attempt, from ncu's instruction counters
+# on the 960x540 copy of the headline frame (one launch, the launch shape the bench tunes):
+# FFMA and FFMA2 lanes x 2 (one FMA = 2 FLOP; a paired FFMA2 is two FMAs), FMUL/FADD and their paired
+# forms x 1 per result, divided by the launch's attempt counter.
+NCU_FLOP_PER_ATTEMPT = 0.0
+NCU_FLOP_RULE = ("FP32 FLOP executed, from ncu sass_thread_inst_executed_op_{ffma,fmul,fadd}{,2}: FFMA 2, FFMA2 4, "
+                 "FMUL/FADD 1, FMUL2/FADD2 2, per attempt")
+# DRAM bytes of one launch of the tracing kernel (ncu, 960x540 copy of the headline frame)
+TRAFFIC_PER_LAUNCH = 8.704512e6
+
 
 def reserve_stdout():
     """Points file descriptor 1 at stderr for the rest of the run and returns
@@ -76,10 +101,11 @@ def emit(line: dict) -> None:
 
 
 def pair_kernel_name(cfg) -> str:
-    """The FP32 renderer instantiation a launch shape selects (k_pair.cu: launch_pair)."""
+    """The FP32 renderer instantiation a launch shape selects (k_persistent.cu: launch_persistent; one
+    pixel per thread: the Hamiltonian-form k_ham, two: k_pair)."""
     if cfg.rays_per_thread == 2:
         return "k_pair<2,256,1>"
-    return "k_pair<1,64,8>" if cfg.block_size <= 64 else "k_pair<1,256,1>"
+    return "k_ham<64,8>" if cfg.block_size <= 64 else "k_ham<256,1>"
 
 
 def dist_env():
@@ -141,29 +167,81 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def build_frames(rank: int, world: int, width: int, height: int):
+def quantize(img: np.ndarray) -> np.ndarray:
+    """roundf(255 x) of the clamped float colour (cudamaths/image.cu:31)."""
+    v = np.float32(255.0) * np.clip(img.astype(np.float32), np.float32(0.0), np.float32(1.0))
+    return np.floor(v.astype(np.float64) + 0.5).astype(np.uint8)
+
+
+def pixel_rule(a8: np.ndarray, b8: np.ndarray) -> float:
+    """Fraction of pixels whose RGB differ by at most 1/255 in every channel."""
+    d = np.abs(a8.astype(np.int32) - b8.astype(np.int32)).max(axis=-1)
+    return float(np.mean(d <= 1))
+
+
+def orbit_frames(world: int, width: int, height: int) -> list:
+    """The frames of one step: one per rank, frame k with the spheres advanced k/world of an orbit
+    (frame 0 is the headline frame)."""
     from parrelray_b200 import scenes
 
-    # rank r renders the frame with the spheres advanced r/world of an orbit
-    from parrelray_b200 import abi
+    frames = []
+    for k in range(world):
+        d = scenes.kerr_1080p_ssaa4(width, height)
+        ang = 2 * math.pi * k / world
+        for j in range(d.nspheres):
+            sp = d.spheres[j]
+            x, y = sp.center[0], sp.center[1]
+            sp.center[0] = scenes.f32(x * math.cos(ang) - y * math.sin(ang))
+            sp.center[1] = scenes.f32(x * math.sin(ang) + y * math.cos(ang))
+        frames.append(d)
+    return frames
 
-    d = scenes.kerr_1080p_ssaa4(width, height)
-    if world > 1:
-        for k in range(d.nspheres):
-            s = d.spheres[k]
-            x, y = s.center[0], s.center[1]
-            ang = 2 * math.pi * rank / world
-            s.center[0] = scenes.f32(x * math.cos(ang) - y * math.sin(ang))
-            s.center[1] = scenes.f32(x * math.sin(ang) + y * math.cos(ang))
-    return d
+
+def workload_config(width: int, height: int) -> dict:
+    """The `config` object of both arms' result lines (the workload, nothing arm-specific)."""
+    return {"workload": WORKLOAD, "rays_per_step": width * height * 4, "width": width, "height": height,
+            "samples": 4, "tolerance": 1e-6, "metric": "kerr a=0.95 M=1", "camera": "r=25M i=80deg fov=50deg",
+            "l2": "GPU arm: a 256 MiB buffer (L2 is 126 MB) is written between timed steps; CPU arm: no GPU"}
 
 
-def cpu_reference_sample(frame, textures, budget_s: float, nthreads: int, eps: float = 1e-6):
-    """The reference's solver (host build of its sources, Kerr plug-in header)
-    on a bounded sample of `frame`'s rays: 8-ray blocks in a fixed
-    pseudo-random order until `budget_s` of wall time is spent.  `eps` is the
-    reference's absolute error tolerance (the workload's is 1e-6)."""
-    sys.path.insert(0, str(REPO / "tests"))
+def mapped_repo_libraries() -> list[str]:
+    """The repository's shared libraries mapped into this process (from /proc/self/maps)."""
+    out = set()
+    try:
+        for line in Path("/proc/self/maps").read_text().splitlines():
+            path = line.split()[-1] if line.split() else ""
+            if path.endswith(".so") and path.startswith(str(REPO)):
+                out.add(str(Path(path).relative_to(REPO)))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def oracle_fp64_sample(orc, frame64, textures, ids, nthreads: int) -> dict:
+    """The FP64 PHYSICAL host restatement (oracle/prr_oracle.cpp: Christoffel-table geodesic, atol/rtol
+    control at the frame's tolerance) on the rays `ids` of `frame64`, all `nthreads` host threads."""
+    t0 = time.perf_counter()
+    st, _ = orc.trace(frame64, textures, precision=1, ids=ids, nthreads=nthreads)
+    secs = time.perf_counter() - t0
+    return {"rays": int(len(ids)), "seconds": secs, "mrays_s": len(ids) / secs / 1e6,
+            "results": np.bincount(st[:, 2].astype(int), minlength=5).tolist()}
+
+
+def calibrated_ray_sample(orc, frame64, textures, target_s: float, nthreads: int, seed: int = 2024,
+                          lo: int = 1024, hi: int = 262144) -> np.ndarray:
+    """A seeded uniform sample of the frame's rays sized so the FP64 oracle traces it in about
+    `target_s` seconds on `nthreads` threads (a multiple of 1024 rays in [lo, hi]); the sample is
+    an unbiased estimate of the whole frame's per-ray cost."""
+    order = np.random.default_rng(seed).permutation(frame64.nrays)
+    probe = oracle_fp64_sample(orc, frame64, textures, np.sort(order[:lo]), nthreads)
+    n = int(min(max(round(probe["mrays_s"] * 1e6 * target_s / lo) * lo, lo), hi))
+    return np.sort(order[:n])
+
+
+def cpu_reference_sample(frame, textures, budget_s: float, nthreads: int, eps: float):
+    """The reference's own solver (its sources built for the host, oracle/_ref, with the Kerr-Schild
+    plug-in header) on a bounded sample of `frame`'s rays: 8-ray blocks in a fixed pseudo-random
+    order until `budget_s` of wall time is spent.  `eps` is the reference's absolute error tolerance."""
     from oracles import RefHost, ref_available, write_deck
 
     from parrelray_b200 import abi, scenes
@@ -189,8 +267,47 @@ def cpu_reference_sample(frame, textures, budget_s: float, nthreads: int, eps: f
     rays = done * 8
     results = np.array([ref.lib.prr_ref_ray_result(int((r * frame.width * frame.samples) + 8 * b + t))
                         for b, r in zip(order[:done] % nbx, order[:done] // nbx) for t in range(8)])
-    return {"rays": rays, "seconds": secs, "mrays_s": rays / secs / 1e6 if secs > 0 else None,
+    return {"rays": rays, "seconds": secs, "mrays_s": rays / secs / 1e6 if secs > 0 else None, "eps": eps,
             "infinite_geo_fraction": float(np.mean(results == abi.RESULT_INFINITE_GEO)) if len(results) else None}
+
+
+def single_frame_workload(ctx, nthreads: int) -> dict:
+    """The single-frame Schwarzschild workload (M = 1, camera r = 30M, inclination 85 deg, FOV 60 deg,
+    320x180, one sphere R = 1M at r = 10M, the standard textures), the frame the reference's host
+    build can render whole in seconds: its own solver on all host threads at the deck's eps = 1e-3
+    (prr.cpp:237-341: ray placement, initRays, trace_RKF, rayToRGB, combineSamples), beside this
+    library's REFERENCE mode on the GPU (same algorithm, quirks and eps) and its PHYSICAL FP32 render
+    at the workload's tolerance 1e-6 (stop at r <= 2.01M)."""
+    from oracles import RefHost, ref_available, write_deck
+
+    from parrelray_b200 import abi, scenes
+
+    tex = scenes.standard_textures()
+    ctx.upload_textures(tex)
+    ref_mode = scenes.schwarzschild_320(mode=abi.MODE_REFERENCE, eps=1e-3, horizon_eps=0.001)
+    phys = scenes.schwarzschild_320(horizon_eps=0.01)
+    res = {"workload": "schwarzschild_320: M=1, r=30M, i=85 deg, FOV 60 deg, 320x180, 1 sphere, 57,600 rays"}
+    ctx.render(ref_mode)
+    g8, _, gst = ctx.render(ref_mode)
+    ctx.render(phys)
+    _, _, pst = ctx.render(phys)
+    res["gpu_reference_mode_eps_1e-3"] = {"ms": gst.kernel_ms, "mrays_s": gst.rays / (gst.kernel_ms * 1e-3) / 1e6}
+    res["gpu_physical_fp32_tol_1e-6"] = {"ms": pst.kernel_ms, "mrays_s": pst.rays / (pst.kernel_ms * 1e-3) / 1e6,
+                                         "infinite_geo": int(pst.n_infinite)}
+    if ref_available("schw"):
+        _, a_deg, b_deg = scenes.camera_pose(30.0, 85.0)
+        deck = write_deck(Path("/tmp/prrbench320"), ref_mode, tex, fov_deg=60.0, a_deg=a_deg, b_deg=b_deg)
+        ref = RefHost("schw")
+        assert ref.load(deck) == 1
+        out = ref.frame(0, nthreads)
+        res["reference_host_eps_1e-3"] = {"seconds": out["seconds"], "threads": nthreads,
+                                          "mrays_s": ref_mode.nrays / out["seconds"] / 1e6,
+                                          "what": "the reference's frame pipeline (its sources built for the host, "
+                                                  "OpenMP over its 8x8 blocks) on the whole frame"}
+        res["gpu_reference_mode_vs_reference_host"] = {
+            "speedup": out["seconds"] / (gst.kernel_ms * 1e-3),
+            "pixels_within_1_255": pixel_rule(g8[0], quantize(out["image"]))}
+    return res
 
 
 def bench_reference_cuda(width: int, height: int, timeout_s: float = 240.0):
@@ -274,13 +391,14 @@ def reference_cuda_child(out_path: str, width: int, height: int, nlines: int = 4
     return 0
 
 
-def bench_trajectory(ctx, torch, stream, plain_stride: int = 10):
+def bench_trajectory(ctx, torch, stream, plain_stride: int = 1):
     """The 240-frame trajectory workload: Kerr a = 0.9, 960x540, no SSAA,
     orbit radius 20M -> 8M, inclination 60 -> 88 deg, tolerance 1e-6, FP32.
     (1) autotuned launch shape, whole trajectory recorded into one CUDA graph
     and replayed (one persistent launch); (2) the same frames as 240
     persistent launches, one per frame; (3) the plain one-ray-per-thread
-    schedule per frame on every `plain_stride`-th frame, scaled to 240."""
+    schedule, one render call per frame, on every frame (`plain_stride` > 1
+    renders every n-th frame and scales by rays)."""
     from parrelray_b200 import Graph, abi, scenes
 
     frames = scenes.trajectory_240()
@@ -328,10 +446,14 @@ def bench_trajectory(ctx, torch, stream, plain_stride: int = 10):
     plain_sample_ms = ev0.elapsed_time(ev1)
     sample_rays = sum(f.nrays for f in sample)
     plain_rate = sample_rays / (plain_sample_ms * 1e-3) / 1e6
-    res["plain_per_frame"] = {"mrays_s": plain_rate, "ms_240_estimated": rays / (plain_rate * 1e6) * 1e3,
-                              "sampled_frames": len(sample), "sampled_ms": plain_sample_ms,
-                              "what": f"every {plain_stride}th frame rendered with the plain schedule, one call per "
-                                      f"frame; time scaled to the 240 frames by rays"}
+    if plain_stride == 1:
+        res["plain_per_frame"] = {"ms": plain_sample_ms, "mrays_s": plain_rate, "frames": len(sample),
+                                  "what": "every frame rendered with the plain schedule, one call per frame"}
+    else:
+        res["plain_per_frame"] = {"mrays_s": plain_rate, "ms_240_estimated": rays / (plain_rate * 1e6) * 1e3,
+                                  "sampled_frames": len(sample), "sampled_ms": plain_sample_ms,
+                                  "what": f"every {plain_stride}th frame rendered with the plain schedule, one call "
+                                          f"per frame; time scaled to the 240 frames by rays"}
     res["speedup_vs_plain"] = res["graph"]["mrays_s"] / plain_rate
     res["speedup_vs_per_frame_persistent"] = pf_ms / graph_ms
     return res
@@ -504,45 +626,138 @@ def bench_adam_fit(ctx, iters: int, size: int, lr: float = 0.01, decay: float = 
 
 
 def run_reference_arm(args):
+    """The CPU arm: the headline frame's rays through the FP64 PHYSICAL host restatement
+    (oracle/prr_oracle.cpp) at the workload's tolerance 1e-6 on all host threads - the reference has
+    no Kerr solver of its own (its metrics/kerr.cuh returns a zero geodesic), and its FP32
+    absolute-error solver with the Kerr plug-in header sends most rays to its iteration cap at this
+    tolerance, so the restatement stands in for it.  Every step traces the same seeded uniform
+    sample of the frame's rays, sized so a step takes about PRR_REF_STEP_SECONDS (default 4);
+    `value` is rays per second over the timed steps and `ms_per_step` the measured step time.  The
+    reference's own solver (host build) on the same frame at eps 1e-3, where its error test still
+    works, is reported beside it for context.  Loads no library of the product."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    from parrelray_b200 import scenes
+    sys.path.insert(0, str(REPO / "tests"))
+    try:
+        from oracles import Oracle
 
-    frame = scenes.kerr_1080p_ssaa4()
-    tex = scenes.standard_textures()
+        orc = Oracle()
+    except (ImportError, FileNotFoundError) as e:
+        emit({"impl": "reference", "unavailable": f"the CPU oracle library is not built ({e})"})
+        return 0
+    from parrelray_b200 import abi, scenes
+
     nthreads = os.cpu_count() or 1
-    vals = []
-    budget = float(os.environ.get("PRR_REF_STEP_SECONDS", "8"))
+    tex = orc.standard_textures()
+    frame64 = scenes.kerr_1080p_ssaa4(args.width, args.height, precision=abi.PREC_FP64)
+    target = float(os.environ.get("PRR_REF_STEP_SECONDS", "4"))
+    ids = calibrated_ray_sample(orc, frame64, tex, target, nthreads)
+    times, results = [], None
     for it in range(args.warmup + args.steps):
-        r = cpu_reference_sample(frame, tex, budget if it >= args.warmup else 2.0, nthreads)
-        if r is None:
-            emit({"impl": "reference", "unavailable": "reference host build (oracle/_ref) not built"})
-            return 0
+        r = oracle_fp64_sample(orc, frame64, tex, ids, nthreads)
         if it >= args.warmup:
-            vals.append(r)
-    mr = sum(v["rays"] for v in vals) / sum(v["seconds"] for v in vals) / 1e6
-    ms_per_step = 1e3 * frame.nrays / (mr * 1e6)
-    # context: the same solver at eps = 1e-3, where its FP32 absolute error test still works
-    loose = cpu_reference_sample(frame, tex, 4.0, nthreads, eps=1e-3)
+            times.append(r["seconds"])
+            results = r["results"]
+    secs = float(np.sum(times))
+    mr = len(ids) * len(times) / secs / 1e6
+    ms_per_step = 1e3 * secs / len(times)
+    context = cpu_reference_sample(frame64, tex, 4.0, nthreads, eps=1e-3)
+    sample = (f"{len(ids)} rays drawn uniformly (seed 2024) from the {frame64.nrays}-ray frame, the same rays "
+              f"every step, FP64 PHYSICAL restatement at tolerance 1e-6, {nthreads} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": mr, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural textures)",
-        "config": {"workload": WORKLOAD, "rays_per_frame": frame.nrays,
-                   "solver": "reference trace_RKF (kernels/solver.cuh) + Kerr-Schild plug-in, eps=1e-6 absolute"},
-        "cpu_baseline": {"value": mr, "unit": "Mrays/s", "cores": nthreads, "kind": "reference",
-                         "sample": f"{sum(v['rays'] for v in vals)} rays in 8-ray blocks drawn across the frame, "
-                                   f"{budget:.0f}s per step; ms_per_step extrapolates to the full frame",
-                         "infinite_geo_fraction": float(np.mean([v['infinite_geo_fraction'] for v in vals])),
-                         "at_eps_1e-3": {"mrays_s": loose["mrays_s"], "rays": loose["rays"],
-                                         "infinite_geo_fraction": loose["infinite_geo_fraction"],
-                                         "note": "the same solver at the deck's default tolerance, for context; "
-                                                 "not the workload's 1e-6"} if loose else None},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural textures)",
+        "config": workload_config(args.width, args.height),
+        "cpu_baseline": {"value": mr, "unit": "Mrays/s", "cores": nthreads, "kind": "port", "sample": sample,
+                         "results": {"success": results[abi.RESULT_SUCCESS],
+                                     "intersection": results[abi.RESULT_INTERSECTION],
+                                     "infinite_geo": results[abi.RESULT_INFINITE_GEO],
+                                     "math_error": results[abi.RESULT_MATH_ERROR]},
+                         "reference_solver_eps_1e-3": dict(context, what=(
+                             "the reference's own trace_RKF (its sources built for the host, Kerr-Schild plug-in "
+                             "header) on 8-ray blocks across the frame at the deck's default eps 1e-3 - context "
+                             "only: a looser tolerance than the workload's")) if context else None},
         "e2e": {"value": mr, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "libraries_loaded": mapped_repo_libraries(),
     }
     emit(line)
     return 0
+
+
+def bench_plugin_kerr(ctx, torch, stream, frame) -> dict:
+    """The headline frame through the Kerr header shipped as a metric plug-in (compat/metrics/kerr.cuh:
+    the geodesic by the full Christoffel table, as a plug-in author writes it) in PHYSICAL FP32 mode on
+    the persistent scheduler, beside the built-in metric; pixels within 1/255 of each other."""
+    from parrelray_b200 import abi
+
+    p = REPO / "parrelray_b200" / "_lib" / "libprr_metric_kerr.so"
+    if not p.exists():
+        return {"unavailable": "libprr_metric_kerr.so not built"}
+    d = abi.FrameDesc.from_buffer_copy(frame)
+    d.horizon_eps = 0.001  # the header's User_ENDLOOP stops at r_+ + 0.001
+    d.metric = ctx.load_metric_plugin(p)
+    ctx.render(d)
+    img, _, st = ctx.render(d)
+    b = abi.FrameDesc.from_buffer_copy(frame)
+    b.horizon_eps = 0.001
+    bimg, _, bst = ctx.render(b)
+    return {"plugin_ms": st.kernel_ms, "plugin_mrays_s": st.rays / (st.kernel_ms * 1e-3) / 1e6,
+            "builtin_ms": bst.kernel_ms, "builtin_mrays_s": bst.rays / (bst.kernel_ms * 1e-3) / 1e6,
+            "builtin_speedup": st.kernel_ms / bst.kernel_ms, "plugin_attempts": int(st.attempts),
+            "pixels_within_1_255": pixel_rule(img[0], bimg[0]),
+            "what": "the same 1080p frame, PHYSICAL FP32, through the shipped Kerr plug-in header (Christoffel "
+                    "table, persistent plug-in kernel + the header's rayToRGB) and through the built-in metric"}
+
+
+def bench_accuracy(ctx, frame, fp64_peak, n_oracle_rays: int = 4096) -> dict:
+    """The headline frame against FP64: (1) the whole image against an FP64 render of the same frame on
+    the GPU; (2) a fixed seeded set of the frame's rays traced by the FP64 host oracle (the checker,
+    Christoffel-table geodesic) against the FP32 product's per-ray results."""
+    from parrelray_b200 import abi
+
+    f64 = abi.FrameDesc.from_buffer_copy(frame)
+    f64.precision = abi.PREC_FP64
+    ref8, _, s64 = ctx.render(f64)
+    mine8, _, _ = ctx.render(frame)
+    d = np.abs(mine8[0].astype(np.int32) - ref8[0].astype(np.int32)).max(axis=-1)
+    res = {"pixels_within_1_255_of_fp64_gpu": float(np.mean(d <= 1)), "max_abs_diff_255": int(d.max()),
+           "fp64_ms": s64.kernel_ms}
+    if s64.trace_ms > 0:
+        # the FP64 render's tracing kernel against the measured FP64 FMA peak (same F_attempt)
+        a64 = s64.attempts * F_ATTEMPT / (s64.trace_ms * 1e-3) / 1e12
+        res["fp64_roofline"] = {"achieved": a64, "peak": fp64_peak, "unit": "TFLOP/s", "frac": a64 / fp64_peak,
+                                "attempts": int(s64.attempts)}
+    try:
+        sys.path.insert(0, str(REPO / "tests"))
+        from oracles import Oracle, kerr_criticality
+
+        orc = Oracle()
+    except (ImportError, FileNotFoundError):
+        return res
+    from parrelray_b200 import scenes
+
+    tex = scenes.standard_textures()
+    state, rgb, _ = ctx.trace_rays(frame)
+    ids = np.sort(np.random.default_rng(2024).choice(frame.nrays, size=n_oracle_rays, replace=False))
+    s64h, c64 = orc.trace(f64, tex, precision=1, ids=ids)
+    g = state[ids]
+    same = g[:, 2] == s64h[:, 2]
+    band = kerr_criticality(s64h, frame.mass, frame.spin) < 0.04
+    esc = same & (s64h[:, 2] == abi.RESULT_SUCCESS) & (np.linalg.norm(s64h[:, 3:6], axis=1) >= frame.rout) & ~band
+    u1 = g[esc, 7:10] / np.linalg.norm(g[esc, 7:10], axis=1, keepdims=True)
+    u2 = s64h[esc, 7:10] / np.linalg.norm(s64h[esc, 7:10], axis=1, keepdims=True)
+    ang = np.linalg.norm(np.cross(u1, u2), axis=1)
+    cd = np.abs(quantize(rgb[ids]).astype(np.int32) - quantize(c64).astype(np.int32)).max(axis=1)
+    res["vs_fp64_host_oracle"] = {
+        "rays": int(len(ids)), "result_agreement": float(same.mean()),
+        "escaped_outside_critical_band": int(esc.sum()),
+        "escape_angle_rad_p50_p99_max": [float(x) for x in np.percentile(ang, [50, 99, 100])] if esc.any() else None,
+        "per_sample_colour_within_1_255": float(np.mean(cd <= 1)),
+        "what": "a seeded uniform sample of the frame's rays traced by the FP64 host restatement; escape "
+                "directions compared outside a +-2% band around the critical curve"}
+    return res
 
 
 def main():
@@ -560,15 +775,18 @@ def main():
     ap.add_argument("--no-trajectory", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--no-emission", action="store_true")
+    ap.add_argument("--no-plugin", action="store_true", help="skip the Kerr plug-in header render")
     ap.add_argument("--no-refcuda", action="store_true", help="skip the reference's own CUDA build")
     ap.add_argument("--refcuda-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--adjoint-size", type=int, default=512, help="side of the square differentiable-render frame")
-    ap.add_argument("--adam", type=int, default=0, help="also run an N-iteration Adam fit of (a, i) (0: off)")
+    ap.add_argument("--adam", type=int, default=200, help="iterations of the Adam fit of (a, i) (0: off)")
     ap.add_argument("--adam-lr", type=float, default=0.01)
     ap.add_argument("--adam-decay", type=float, default=0.99)
     ap.add_argument("--adam-sphere", action="store_true",
                     help="keep the workload's sphere in the fit (its edges make the loss rougher)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--plain-stride", type=int, default=1,
+                    help="trajectory: render every n-th frame with the plain schedule (1: all 240)")
     ap.add_argument("--launch", default=None,
                     help="block,blocks_per_sm,compaction_interval,rays_per_thread for the persistent renderer "
                          "(default: prr_autotune on the frame, outside the timed region)")
@@ -583,7 +801,7 @@ def main():
 
     import torch
 
-    from parrelray_b200 import Context, LaunchConfig, abi, scenes
+    from parrelray_b200 import Context, LaunchConfig, abi, scenes, shard
 
     ws, rank, local = dist_env()
     if ws > 1:
@@ -599,7 +817,8 @@ def main():
     ctx = Context(dev)
     tex = scenes.standard_textures()
     ctx.upload_textures(tex)
-    frame = build_frames(rank, ws, args.width, args.height)
+    frames = orbit_frames(ws, args.width, args.height)
+    frame = frames[rank]  # this rank's share when every rank draws one frame (weak scaling)
     npx = frame.width * frame.height
     t_tune = time.perf_counter()
     if args.launch:
@@ -615,19 +834,33 @@ def main():
     out8 = torch.empty(npx * 3, dtype=torch.uint8, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     stream = torch.cuda.current_stream()
+    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def barrier():
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def render_device():
-        ctx.render_device(frame, out8.data_ptr(), stream=stream.cuda_stream)
+    def render_claimed(fs):
+        """This rank's renderer for shard.render_sharded: device outputs, CUDA-event time."""
+        ev_a.record(stream)
+        for f in fs:
+            ctx.render_device(f, out8.data_ptr(), stream=stream.cuda_stream)
+        ev_b.record(stream)
+        ev_b.synchronize()
+        return [None] * len(fs), ev_a.elapsed_time(ev_b)
+
+    def step():
+        flush.zero_()
+        if ws > 1:
+            # the step's frames are pulled from a shared counter (shard.py), each rank rendering what it claims
+            shard.render_sharded(frames, render_claimed, gather_to=None)
+        else:
+            ctx.render_device(frame, out8.data_ptr(), stream=stream.cuda_stream)
 
     # warm-up (also the stats of one frame: attempts for the roofline)
     for _ in range(args.warmup):
-        flush.zero_()
-        render_device()
+        step()
     torch.cuda.synchronize()
     _, _, st = ctx.render(frame)
 
@@ -637,8 +870,7 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        flush.zero_()
-        render_device()
+        step()
     ev1.record(stream)
     barrier()
     clocks = sampler.stop()
@@ -669,13 +901,19 @@ def main():
     if rank == 0:
         fp32_peak, fp64_peak = ctx.measure_peak()
         achieved = st.attempts * F_ATTEMPT / (st.trace_ms * 1e-3) / 1e12
+        counted = st.attempts * NCU_FLOP_PER_ATTEMPT / (st.trace_ms * 1e-3) / 1e12
         roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                    "frac": achieved / fp32_peak, "traffic": 8.704512e6,
-                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one k_pair launch on the "
-                                      "960x540 frame (profiles/k_pair_kerr960x540_ssaa4_full.md): the textures; "
-                                      "they do not grow with the frame, and the outputs stay in L2",
+                    "frac": achieved / fp32_peak, "traffic": TRAFFIC_PER_LAUNCH,
+                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of the tracing "
+                                      "kernel on the 960x540 copy of this frame (ncu): the textures; they do not "
+                                      "grow with the frame, and the outputs stay in L2",
                     "kernel": pair_kernel_name(ctx.launch_config()), "kernel_ms": st.trace_ms,
                     "flop_per_attempt": F_ATTEMPT, "attempts": st.attempts,
+                    "frac_basis": "algorithmic: attempts x F_attempt (the work of one RKF45 attempt in the Kerr-Schild "
+                                  "contraction form, FMA = 2) / kernel time",
+                    "ncu_counted": {"achieved": counted, "frac": counted / fp32_peak,
+                                    "flop_per_attempt": NCU_FLOP_PER_ATTEMPT,
+                                    "rule": NCU_FLOP_RULE},
                     "peak_source": "measured on this GPU: FMA-chain kernel (prr_measure_peak), burst",
                     "fp64_peak_tflops": fp64_peak}
         extra["roofline"] = roofline
@@ -700,8 +938,12 @@ def main():
             ctx.set_option(abi.OPT_GEOD_TABLE, -1)
             extra["plain"] = {"value": rays / (plain_ms * 1e-3) / 1e6, "ms_per_step": plain_ms,
                               "speedup": plain_ms / ms,
+                              "speedup_scheduler_only": plain_contraction_ms / ms,
+                              "speedup_scheduler_only_table": plain_ms / table_ms,
+                              "speedup_geodesic_form_only": plain_ms / plain_contraction_ms,
                               "what": "one ray per thread, 64-row layers, AoS rays in HBM, textbook stages, "
-                                      "Christoffel-table geodesic",
+                                      "Christoffel-table geodesic; speedup = both changes, scheduler_only = the "
+                                      "persistent compaction scheduler with the geodesic form held fixed",
                               "breakdown_ms": {"plain_table": plain_ms, "plain_contraction": plain_contraction_ms,
                                                "persistent_table": table_ms, "persistent_contraction": ms}}
         if not args.no_adjoint:
@@ -718,41 +960,48 @@ def main():
             for _ in range(2):  # the first call sizes the checkpoint buffer
                 abi.check(abi.load().prr_adjoint(ctx.h, C.byref(start), dl.ctypes.data_as(abi._fp), 0,
                                                  g.ctypes.data_as(abi._dp), C.byref(ast)), ctx.h)
-            extra["adjoint"] = {"ms": ast.kernel_ms, "fp64_forward_ms": ast.trace_ms, "unit": "ms",
-                                "workload": f"kerr a=0.3 i=45 r=20, {n}x{n}, 1 sphere, bilinear sky, FP64, tol 1e-6; "
+            extra["adjoint"] = {"ms": ast.kernel_ms, "forward_ms": ast.trace_ms, "unit": "ms",
+                                "workload": f"kerr a=0.3 i=45 r=20, {n}x{n}, 1 sphere, bilinear sky, tol 1e-6; "
                                             "d(L2 to the a=0.7 render)/d(a, M, i, r, phase)",
                                 "grad": g.tolist(), "accepted_steps": ast.accepted}
         if args.adam > 0 and ws == 1:
             extra["adam_fit"] = bench_adam_fit(ctx, args.adam, args.adjoint_size, args.adam_lr, args.adam_decay,
                                                args.adam_sphere)
         if not args.no_trajectory and ws == 1:
-            extra["trajectory"] = bench_trajectory(ctx, torch, stream)
+            extra["trajectory"] = bench_trajectory(ctx, torch, stream, plain_stride=args.plain_stride)
         if not args.no_uneven and ws == 1:
             extra["uneven"] = bench_uneven(ctx, torch, stream, tex)
         if not args.no_emission and ws == 1:
             extra["emission"] = bench_emission(ctx, torch, stream)
+        ctx.upload_textures(tex)
+        if not args.no_plugin and ws == 1:
+            extra["plugin_kerr_header"] = bench_plugin_kerr(ctx, torch, stream, frame)
         if not args.no_accuracy:
-            f64 = build_frames(rank, ws, args.width, args.height)
-            f64.precision = abi.PREC_FP64
-            ref8, _, s64 = ctx.render(f64)
-            mine8, _, _ = ctx.render(frame)
-            d = np.abs(mine8[0].astype(np.int32) - ref8[0].astype(np.int32)).max(axis=-1)
-            extra["accuracy"] = {"pixels_within_1_255_of_fp64": float(np.mean(d <= 1)),
-                                 "max_abs_diff_255": int(d.max()), "fp64_ms": s64.kernel_ms}
-            if s64.trace_ms > 0:
-                # the FP64 render's tracing kernel against the measured FP64 FMA peak (same F_attempt)
-                a64 = s64.attempts * F_ATTEMPT / (s64.trace_ms * 1e-3) / 1e12
-                extra["accuracy"]["fp64_roofline"] = {"achieved": a64, "peak": fp64_peak, "unit": "TFLOP/s",
-                                                      "frac": a64 / fp64_peak, "attempts": int(s64.attempts)}
+            extra["accuracy"] = bench_accuracy(ctx, frame, fp64_peak)
         if not args.no_cpu and ws == 1:
-            r = cpu_reference_sample(frame, tex, args.cpu_seconds, os.cpu_count() or 1)
-            if r:
-                extra["cpu_baseline"] = {"value": r["mrays_s"], "unit": "Mrays/s", "cores": os.cpu_count(),
-                                         "kind": "reference",
-                                         "sample": f"{r['rays']} rays (8-ray blocks across the frame) in "
-                                                   f"{r['seconds']:.1f}s; reference trace_RKF + Kerr-Schild plug-in at "
-                                                   f"eps=1e-6 (absolute, FP32)",
-                                         "infinite_geo_fraction": r["infinite_geo_fraction"]}
+            # the cpu_baseline leg: the CPU restatement and the reference's host build, on this host's cores
+            sys.path.insert(0, str(REPO / "tests"))
+            try:
+                from oracles import Oracle
+
+                orc = Oracle()
+            except (ImportError, FileNotFoundError):
+                orc = None
+            nthreads = os.cpu_count() or 1
+            if orc is not None:
+                f64 = abi.FrameDesc.from_buffer_copy(frame)
+                f64.precision = abi.PREC_FP64
+                ids = calibrated_ray_sample(orc, f64, tex, args.cpu_seconds, nthreads)
+                r = oracle_fp64_sample(orc, f64, tex, ids, nthreads)
+                extra["cpu_baseline"] = {
+                    "value": r["mrays_s"], "unit": "Mrays/s", "cores": nthreads, "kind": "port",
+                    "sample": f"{r['rays']} rays drawn uniformly (seed 2024) from the frame, FP64 PHYSICAL "
+                              f"restatement (oracle/prr_oracle.cpp) at tolerance 1e-6, {r['seconds']:.1f} s"}
+                ctxr = cpu_reference_sample(frame, tex, 4.0, nthreads, eps=1e-3)
+                if ctxr:
+                    extra["cpu_baseline"]["reference_solver_eps_1e-3"] = ctxr
+            extra.setdefault("cpu_baseline", {})["single_frame_workload"] = single_frame_workload(ctx, nthreads)
+            ctx.upload_textures(tex)
         if not args.no_refcuda and ws == 1:
             rc = bench_reference_cuda(args.width, args.height)
             if "eps_1e-3_frame" in rc:
@@ -771,11 +1020,10 @@ def main():
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural textures)",
-            "config": {"workload": WORKLOAD, "rays_per_step": rays, "width": frame.width, "height": frame.height,
-                       "samples": frame.samples, "schedule": "persistent",
-                       "launch": {k: getattr(ctx.launch_config(), k) for k, _ in LaunchConfig._fields_},
-                       "launch_source": tuned_on, "autotune_s": round(t_tune, 2),
-                       "l2": "256 MiB buffer written between timed steps (inside the timed region)"},
+            "config": workload_config(args.width, args.height),
+            "launch": {"schedule": "persistent" + (", frames pulled from a shared counter" if ws > 1 else ""),
+                       "shape": {k: getattr(ctx.launch_config(), k) for k, _ in LaunchConfig._fields_},
+                       "source": tuned_on, "autotune_s": round(t_tune, 2)},
             "e2e": e2e, "clocks": clocks, "gpu_launches": int(st.kernel_launches) * args.steps,
         }
         line.update(extra)

@@ -428,6 +428,12 @@ prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, prr_launch_co
                                      everywhere (A/B runs) */
 #define PRR_OPT_WATCHDOG_CYCLES 2 /* >0: persistent kernels stop after this many SM clock cycles and the
                                      call returns PRR_ERR_TIMEOUT; 0: off (default) */
+#define PRR_OPT_HAMILTONIAN 3     /* FP32 PHYSICAL renders with one pixel per thread and no emission:
+                                     1 (default) integrate (x, p) in Hamiltonian form (p_t conserved, six
+                                     state components); 0: integrate (x, u) with the geodesic contraction.
+                                     Both use the same tableau, error test, caps, hooks and colours; in the
+                                     Hamiltonian form the coordinate time is not integrated, so r.w of
+                                     prr_trace_rays is 0 there */
 prr_status prr_set_option(prr_ctx *ctx, int option, long long value);
 
 /* Measures FP32 and FP64 FMA throughput (TFLOP/s) of the context's device

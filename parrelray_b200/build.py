@@ -28,7 +28,7 @@ INCLUDE = REPO / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NO_FMAD = {"k_reference.cu", "post.cu"}
 CU_SOURCES = ["capi.cu", "render.cu", "k_reference.cu", "post.cu", "k_persistent.cu", "k_plain.cu", "fma_peak.cu",
-              "noalloc.cu", "k_adjoint.cu", "graph.cu", "frame_loop.cu", "k_pair.cu"]
+              "noalloc.cu", "k_adjoint.cu", "graph.cu", "frame_loop.cu", "k_pair.cu", "k_ham.cu"]
 CPP_SOURCES = ["textures.cpp", "deck.cpp", "image_io.cpp"]
 
 

@@ -85,6 +85,7 @@ prr_status record(prr_graph *g, cudaStream_t st)
     a.total_pixels = plan.total_pixels;
     a.counters = (unsigned long long *)g->counters.p;
     a.geod_table = ctx->geod_table == 1;
+    a.hamiltonian = ctx->hamiltonian;
     a.compaction_interval = g->cfg.compaction_interval;
     a.watchdog_cycles = ctx->watchdog_cycles;
     a.rays_per_thread = g->cfg.rays_per_thread;

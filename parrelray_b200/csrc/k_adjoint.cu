@@ -2,20 +2,26 @@
 // d(loss)/d(spin a, mass M, camera inclination i, camera distance r, orbital
 // phase of one sphere) given dL/d(image).
 //
-// Per ray, FP64, with the accepted step sizes and every discrete event
+// Per ray, with the accepted step sizes and every discrete event
 // (accept/reject, intersection mode, termination, which sphere is hit)
-// frozen at the forward run:
+// frozen at the forward run.  The forward steps run in the frame's precision
+// (TF = float: the FP32 PHYSICAL stepper with Kahan-compensated updates;
+// TF = double: FP64); the adjoint and the gradient reduction are FP64:
 //   1. forward: the PHYSICAL stepper runs the ray and saves its full state
 //      every ADJ_K accepted steps (checkpoints in HBM, per thread);
 //   2. colour adjoint: dL/dc of the ray's sample through the SSAA combine,
 //      then lambda_N = dL/dc . dc/dy_N (+ the sphere-phase term) with c the
 //      bilinear sky or the sphere texture at the hit point;
-//   3. reverse: for each segment, last first, the ADJ_K steps are recomputed
-//      from the checkpoint (bit-identical: same stepper) and lambda is pulled
-//      back through each step y_{n+1} = y_n + sum_i b_i k_i, k_i = h f(z_i),
-//      z_i = y_n + sum_j a_ij k_j (Fehlberg, 4th order); the products
-//      lambda^T dG/dz of the geodesic acceleration come from its hand-written
-//      reverse sweep (geod_vjp.cuh);
+//   3. reverse: for each segment, last first, the steps are recomputed from
+//      the checkpoint (bit-identical: same stepper) in two levels - a pass
+//      that keeps a sub-checkpoint every ADJ_SUB steps, then, sub-segment by
+//      sub-segment, a pass that keeps the ADJ_SUB states - so a thread holds
+//      a few hundred bytes of states instead of a whole segment; lambda is
+//      pulled back through each step of x' = u, u' = G(x, u) in the stepper's
+//      form (only the velocity increments ku_i = h G(z_i) are kept: the
+//      stage points z_i are rebuilt from them, and their adjoints carry the
+//      position coupling); the products lambda^T dG/dz come from the
+//      geodesic's hand-written reverse sweep (geod_vjp.cuh);
 //   4. lambda_0 is pulled back through the initial data (camera position,
 //      ray direction, null u^t), also by dual numbers.
 // Gradients are accumulated per thread and reduced in FP64.
@@ -30,16 +36,6 @@ namespace prr {
 
 using DC = Dual<13>;  // initial data / colour: 8 state components + 5 parameters
 enum { P_SPIN = 0, P_MASS = 1, P_INCL = 2, P_CAMR = 3, P_PHASE = 4 };
-
-// exact Fehlberg tableau and 4th-order weights
-__constant__ double c_rkA[6][6] = {
-    {0, 0, 0, 0, 0, 0},
-    {1.0 / 4.0, 0, 0, 0, 0, 0},
-    {3.0 / 32.0, 9.0 / 32.0, 0, 0, 0, 0},
-    {1932.0 / 2197.0, -7200.0 / 2197.0, 7296.0 / 2197.0, 0, 0, 0},
-    {439.0 / 216.0, -8.0, 3680.0 / 513.0, -845.0 / 4104.0, 0, 0},
-    {-8.0 / 27.0, 2.0, -3544.0 / 2565.0, 1859.0 / 4104.0, -11.0 / 40.0, 0}};
-__constant__ double c_rkB[6] = {25.0 / 216.0, 0.0, 1408.0 / 2565.0, 2197.0 / 4104.0, -1.0 / 5.0, 0.0};
 
 // Sphere::getColor at p + v d for a T-valued centre (derivative-carrying
 // version of sphere_colour; same arithmetic in FP64).
@@ -97,50 +93,99 @@ __device__ void initial_state(const FrameParams &fp, const AdjParams &ap, float 
     }
 }
 
-__device__ void geod_val(const Hot<double> &q, const double z[8], double G[4])
+// Fehlberg coefficients for runtime stage indices: A (stage weights), B = A*A
+// (the position stages, phys_stepper.cuh) and c = A*1.
+__constant__ double c_A[6][5] = {{0, 0, 0, 0, 0},
+                                 {Fehlberg::A21, 0, 0, 0, 0},
+                                 {Fehlberg::A31, Fehlberg::A32, 0, 0, 0},
+                                 {Fehlberg::A41, Fehlberg::A42, Fehlberg::A43, 0, 0},
+                                 {Fehlberg::A51, Fehlberg::A52, Fehlberg::A53, Fehlberg::A54, 0},
+                                 {Fehlberg::A61, Fehlberg::A62, Fehlberg::A63, Fehlberg::A64, Fehlberg::A65}};
+__constant__ double c_B[6][5] = {{0, 0, 0, 0, 0},
+                                 {0, 0, 0, 0, 0},
+                                 {Fehlberg::B31, 0, 0, 0, 0},
+                                 {Fehlberg::B41, Fehlberg::B42, 0, 0, 0},
+                                 {Fehlberg::B51, Fehlberg::B52, Fehlberg::B53, 0, 0},
+                                 {Fehlberg::B61, Fehlberg::B62, Fehlberg::B63, Fehlberg::B64, 0}};
+__constant__ double c_c[6] = {0.0, Fehlberg::c2, Fehlberg::c3, Fehlberg::c4, Fehlberg::c5, Fehlberg::c6};
+__constant__ double c_K4[6] = {Fehlberg::K41, Fehlberg::K42, Fehlberg::K43, Fehlberg::K44, Fehlberg::K45, Fehlberg::K46};
+__constant__ double c_beta[6] = {Fehlberg::b1, Fehlberg::b2, Fehlberg::b3, Fehlberg::b4, Fehlberg::b5, 0.0};
+
+// Stage point i of the Fehlberg step from y = (x, u), h and the velocity
+// increments ku_0..ku_{i-1} (x' = u is linear in the stages: phys_stepper.cuh):
+//   z_i^u = u + sum_m A_im ku_m,  z_i^x = x + h (c_i u + sum_m B_im ku_m).
+__device__ __forceinline__ void stage_point(const double y[8], double h, const double ku[6][4], int i, V4<double> &zx,
+                                            V4<double> &zu)
 {
-    if (q.metric == PRR_METRIC_FLAT) { G[0] = G[1] = G[2] = G[3] = 0.0; return; }
-    V4<double> g = geod_ks<double, true>({z[0], z[1], z[2], z[3]}, {z[4], z[5], z[6], z[7]}, q.M, q.a);
-    G[0] = g.x; G[1] = g.y; G[2] = g.z; G[3] = g.w;
+    double sx[4], su[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) { su[c] = y[4 + c]; sx[c] = c_c[i] * y[4 + c]; }
+    for (int m = 0; m < i; m++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) { su[c] += c_A[i][m] * ku[m][c]; sx[c] += c_B[i][m] * ku[m][c]; }
+    zx = {y[0] + h * sx[0], y[1] + h * sx[1], y[2] + h * sx[2], y[3] + h * sx[3]};
+    zu = {su[0], su[1], su[2], su[3]};
 }
 
-// lambda <- lambda . dPhi/dy at (y, h); th[0..1] += lambda . dPhi/d(spin, mass)
+// The geodesic's reverse sweep, one copy in the kernel (called at every stage).
+__device__ __noinline__ void geod_vjp_call(const V4<double> &zx, const V4<double> &zu, double M, double a,
+                                           const double w[4], double gx[4], double gu[4], double &gM, double &ga)
+{
+    geod_vjp(zx, zu, M, a, w, gx, gu, gM, ga);
+}
+
+// lambda <- lambda . dPhi/dy at (y, h), Phi the 4th-order Fehlberg step
+//   u+ = u + sum_m K4_m ku_m,  x+ = x + h (u + sum_m beta_m ku_m);
+// th[0..1] += lambda . dPhi/d(spin, mass).  Only the six velocity increments
+// ku (24 doubles) and their adjoints (24 doubles) are kept; the stage points
+// are rebuilt from them.
 __device__ void step_vjp(const Hot<double> &q, const double y[8], double h, double lam[8], double th[2])
 {
-    double z[6][8], k[6][8];
+    if (q.metric == PRR_METRIC_FLAT) {  // G = 0: x+ = x + h u
+#pragma unroll
+        for (int c = 0; c < 4; c++) lam[4 + c] += h * lam[c];
+        return;
+    }
+    double ku[6][4];
+#pragma unroll 1
     for (int i = 0; i < 6; i++) {
-        for (int c = 0; c < 8; c++) {
-            double s = y[c];
-            for (int j = 0; j < i; j++) s += c_rkA[i][j] * k[j][c];
-            z[i][c] = s;
-        }
-        double G[4];
-        geod_val(q, z[i], G);
-        for (int c = 0; c < 4; c++) { k[i][c] = h * z[i][4 + c]; k[i][4 + c] = h * G[c]; }
+        V4<double> zx, zu;
+        stage_point(y, h, ku, i, zx, zu);
+        const V4<double> g = geod_ks<double, true>(zx, zu, q.M, q.a);
+        ku[i][0] = h * g.x; ku[i][1] = h * g.y; ku[i][2] = h * g.z; ku[i][3] = h * g.w;
     }
-    double kb[6][8], yb[8];
-    for (int c = 0; c < 8; c++) yb[c] = lam[c];
-    for (int i = 0; i < 6; i++)
-        for (int c = 0; c < 8; c++) kb[i][c] = c_rkB[i] * lam[c];
+    // adjoints of the outputs: of ku_m, and of (x, u) through the direct terms
+    double kb[6][4], ox[4], ou[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        ox[c] = lam[c];
+        ou[c] = lam[4 + c] + h * lam[c];
+#pragma unroll
+        for (int m = 0; m < 6; m++) kb[m][c] = c_K4[m] * lam[4 + c] + h * c_beta[m] * lam[c];
+    }
+#pragma unroll 1
     for (int i = 5; i >= 0; i--) {
-        double zb[8];
-        // k_i = h (z_u, G(z)):  zb = h (d f/dz)^T kb_i, by the reverse sweep of the geodesic
-        if (q.metric == PRR_METRIC_FLAT) {
-            for (int c = 0; c < 8; c++) zb[c] = 0.0;
-        } else {
-            double gx[4], gu[4], gM, ga;
-            const double wv[4] = {kb[i][4], kb[i][5], kb[i][6], kb[i][7]};
-            geod_vjp({z[i][0], z[i][1], z[i][2], z[i][3]}, {z[i][4], z[i][5], z[i][6], z[i][7]}, q.M, q.a, wv, gx, gu, gM, ga);
-            for (int c = 0; c < 4; c++) { zb[c] = h * gx[c]; zb[4 + c] = h * gu[c]; }
-            th[0] += h * ga;
-            th[1] += h * gM;
+        V4<double> zx, zu;
+        stage_point(y, h, ku, i, zx, zu);
+        double gx[4], gu[4], gM, ga;
+        const double wv[4] = {kb[i][0], kb[i][1], kb[i][2], kb[i][3]};
+        geod_vjp_call(zx, zu, q.M, q.a, wv, gx, gu, gM, ga);
+        th[0] += h * ga;
+        th[1] += h * gM;
+        double zbx[4], zbu[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            zbx[c] = h * gx[c];
+            zbu[c] = h * gu[c];
+            ox[c] += zbx[c];
+            ou[c] += zbu[c] + h * c_c[i] * zbx[c];
         }
-        for (int c = 0; c < 4; c++) zb[4 + c] += h * kb[i][c];
-        for (int c = 0; c < 8; c++) yb[c] += zb[c];
-        for (int j = 0; j < i; j++)
-            for (int c = 0; c < 8; c++) kb[j][c] += c_rkA[i][j] * zb[c];
+        for (int m = 0; m < i; m++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) kb[m][c] += c_A[i][m] * zbu[c] + h * c_B[i][m] * zbx[c];
     }
-    for (int c = 0; c < 8; c++) lam[c] = yb[c];
+#pragma unroll
+    for (int c = 0; c < 4; c++) { lam[c] = ox[c]; lam[4 + c] = ou[c]; }
 }
 
 struct AdjointArgs {
@@ -148,7 +193,7 @@ struct AdjointArgs {
     AdjParams ap;
     const float *dL_dimage;    // W*H*3 (device)
     const float *image;        // forward combined image W*H*3 (device)
-    PhysRay<double> *ckpt;     // per thread: max_ckpt checkpoints
+    void *ckpt;                // per thread: max_ckpt checkpoints (PhysRay<TF>)
     int max_ckpt;
     double *grad;              // 5 doubles, accumulated
     unsigned long long *counters;
@@ -156,26 +201,38 @@ struct AdjointArgs {
     const unsigned *order;     // ray visit order (null: 0, 1, 2, ...)
 };
 
-constexpr int ADJ_K = 64;
+constexpr int ADJ_K = 64;    // accepted steps between checkpoints (HBM)
+constexpr int ADJ_SUB = 16;  // accepted steps between sub-checkpoints of the reverse sweep (per thread)
+static_assert(ADJ_K % ADJ_SUB == 0, "sub-segments tile a segment");
 
 // At least PRR_ADJ_MINB resident CTAs of 128 threads per SM (caps registers).
 #ifndef PRR_ADJ_MINB
 #define PRR_ADJ_MINB 1
 #endif
 
-__global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
+template <class TF> __device__ __forceinline__ void state8(const PhysRay<TF> &R, double y[8])
+{
+    y[0] = (double)R.x.x; y[1] = (double)R.x.y; y[2] = (double)R.x.z; y[3] = (double)R.x.w;
+    y[4] = (double)R.u.x; y[5] = (double)R.u.y; y[6] = (double)R.u.z; y[7] = (double)R.u.w;
+}
+
+template <class TF> __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
 {
     const FrameParams &fp = *A.frame;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nth = (long long)gridDim.x * blockDim.x;
-    PhysRay<double> *ck = A.ckpt + tid * A.max_ckpt;
-    Hot<double> q = make_hot<double>(fp);
+    PhysRay<TF> *ck = (PhysRay<TF> *)A.ckpt + tid * A.max_ckpt;
+    Hot<TF> qf = make_hot<TF>(fp);
+    qf.a = fp.metric == PRR_METRIC_KERR ? (TF)A.ap.spin : (TF)0;
+    qf.M = fp.metric == PRR_METRIC_FLAT ? (TF)0 : (TF)A.ap.mass;
+    Hot<double> q = make_hot<double>(fp);  // the adjoint's (FP64) copy
     q.a = fp.metric == PRR_METRIC_KERR ? A.ap.spin : 0.0;
     q.M = fp.metric == PRR_METRIC_FLAT ? 0.0 : A.ap.mass;
     double gacc[5] = {0, 0, 0, 0, 0};
     unsigned long long n_bad = 0, n_steps = 0;
     const int S = fp.samples;
-    double ystore[ADJ_K][8], hstore[ADJ_K];
+    TF ystore[ADJ_SUB][8], hstore[ADJ_SUB];
+    PhysRay<TF> sub[ADJ_K / ADJ_SUB];
     for (long long k = tid; k < A.nrays; k += nth) {
         const long long rid = A.order ? (long long)A.order[k] : k;
         long long pix = rid / S;
@@ -186,18 +243,18 @@ __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
         ray_uv(fp, px, py, s, uvx, uvy);
         double y0[8], dy0[8][5];
         initial_state(fp, A.ap, uvx, uvy, y0, dy0);
-        PhysRay<double> R;
-        R.x = {y0[0], y0[1], y0[2], y0[3]};
-        R.u = {y0[4], y0[5], y0[6], y0[7]};
+        PhysRay<TF> R;
+        R.x = {(TF)y0[0], (TF)y0[1], (TF)y0[2], (TF)y0[3]};
+        R.u = {(TF)y0[4], (TF)y0[5], (TF)y0[6], (TF)y0[7]};
         R.cx = {0, 0, 0, 0}; R.cu = {0, 0, 0, 0};
-        R.h = fp.h; R.trace_h = fp.h; R.l = 0; R.i = 0; R.accepted = 0; R.intersect = 0;
+        R.h = (TF)fp.h; R.trace_h = (TF)fp.h; R.l = 0; R.i = 0; R.accepted = 0; R.intersect = 0;
         ck[0] = R;
         int result = 0, hit = -1;
         V3<float> col;
         bool ok = true;
         while (true) {
             int before = R.accepted;
-            int st = phys_attempt<double, 0>(fp, q, R, result, col, -1.0, &hit);
+            int st = phys_attempt<TF, 0>(fp, qf, R, result, col, (TF)-1, &hit);
             if (st == STEP_CONTINUE && R.accepted > before && R.accepted % ADJ_K == 0) {
                 int slot = R.accepted / ADJ_K;
                 if (slot >= A.max_ckpt) { ok = false; break; }
@@ -208,7 +265,7 @@ __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
         if (!ok) { n_bad++; continue; }
         const int N = R.accepted;
         n_steps += (unsigned long long)N;
-        bool escaped = result == PRR_RESULT_SUCCESS && metric_radius<double>(fp, R.x.x, R.x.y, R.x.z) >= (double)fp.rout;
+        bool escaped = result == PRR_RESULT_SUCCESS && metric_radius<TF>(fp, R.x.x, R.x.y, R.x.z) >= (TF)fp.rout;
         if (!(escaped || result == PRR_RESULT_INTERSECTION)) continue;  // black: no gradient
         // dL/dc for this sample
         const float *gI = A.dL_dimage + 3 * pix;
@@ -228,7 +285,8 @@ __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
         double lam[8] = {0, 0, 0, 0, 0, 0, 0, 0}, th[2] = {0, 0};
         {
             DC st[8];
-            const double yN[8] = {R.x.x, R.x.y, R.x.z, R.x.w, R.u.x, R.u.y, R.u.z, R.u.w};
+            double yN[8];
+            state8(R, yN);
             for (int c = 0; c < 8; c++) st[c] = DC::var(yN[c], c);
             V3<DC> cd;
             if (escaped) {
@@ -256,25 +314,43 @@ __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
                 gacc[P_PHASE] += gc[c] * cc3[c].d[8 + P_PHASE];
             }
         }
-        // reverse sweep, segment by segment
+        // reverse sweep, segment by segment, each in two recompute passes
+        int r2 = 0, h2 = -1;
+        V3<float> c2;
         for (int seg = (N - 1) / ADJ_K; seg >= 0 && N > 0; seg--) {
-            PhysRay<double> Rs = ck[seg];
             const int lo = seg * ADJ_K, hi = min(N, lo + ADJ_K);
-            int r2 = 0, h2 = -1;
-            V3<float> c2;
-            while (Rs.accepted < hi) {
-                int before = Rs.accepted;
-                double yb[8] = {Rs.x.x, Rs.x.y, Rs.x.z, Rs.x.w, Rs.u.x, Rs.u.y, Rs.u.z, Rs.u.w};
-                double hb = Rs.h;
-                int st = phys_attempt<double, 0>(fp, q, Rs, r2, c2, -1.0, &h2);
-                if (Rs.accepted > before) {
-                    int slot = before - lo;
-                    for (int c = 0; c < 8; c++) ystore[slot][c] = yb[c];
-                    hstore[slot] = hb;
-                }
+            const int nsub = (hi - lo + ADJ_SUB - 1) / ADJ_SUB;
+            // pass 1: the segment's sub-checkpoints
+            PhysRay<TF> Rs = ck[seg];
+            sub[0] = Rs;
+            while (Rs.accepted < lo + (nsub - 1) * ADJ_SUB) {
+                int st = phys_attempt<TF, 0>(fp, qf, Rs, r2, c2, (TF)-1, &h2);
+                const int j = (Rs.accepted - lo) / ADJ_SUB;
+                if ((Rs.accepted - lo) % ADJ_SUB == 0 && j < nsub) sub[j] = Rs;
                 if (st != STEP_CONTINUE) break;
             }
-            for (int n = hi - 1; n >= lo; n--) step_vjp(q, ystore[n - lo], hstore[n - lo], lam, th);
+            // pass 2: each sub-segment, last first: keep its states, then pull lambda back
+            for (int j = nsub - 1; j >= 0; j--) {
+                Rs = sub[j];
+                const int slo = lo + j * ADJ_SUB, shi = min(hi, slo + ADJ_SUB);
+                while (Rs.accepted < shi) {
+                    const int before = Rs.accepted;
+                    TF yb[8] = {Rs.x.x, Rs.x.y, Rs.x.z, Rs.x.w, Rs.u.x, Rs.u.y, Rs.u.z, Rs.u.w};
+                    const TF hb = Rs.h;
+                    int st = phys_attempt<TF, 0>(fp, qf, Rs, r2, c2, (TF)-1, &h2);
+                    if (Rs.accepted > before) {
+                        const int slot = before - slo;
+                        for (int c = 0; c < 8; c++) ystore[slot][c] = yb[c];
+                        hstore[slot] = hb;
+                    }
+                    if (st != STEP_CONTINUE) break;
+                }
+                for (int n = shi - 1; n >= slo; n--) {
+                    double y[8];
+                    for (int c = 0; c < 8; c++) y[c] = (double)ystore[n - slo][c];
+                    step_vjp(q, y, (double)hstore[n - slo], lam, th);
+                }
+            }
         }
         gacc[P_SPIN] += th[0];
         gacc[P_MASS] += th[1];
@@ -294,20 +370,21 @@ __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
 
 cudaError_t launch_adjoint(const FrameParams *d_fp, const AdjointParamsHost &p, const float *dL, const float *image,
                            void *ckpt, int max_ckpt, int threads_total, double *grad, unsigned long long *counters,
-                           long long nrays, const unsigned *order, cudaStream_t st)
+                           long long nrays, const unsigned *order, int precision, cudaStream_t st)
 {
     AdjointArgs A;
     A.frame = d_fp;
     A.ap = {p.spin, p.mass, p.incl, p.cam_r, p.phase, p.sph_R, p.sph_z, p.sphere};
     A.dL_dimage = dL;
     A.image = image;
-    A.ckpt = (PhysRay<double> *)ckpt;
+    A.ckpt = ckpt;
     A.max_ckpt = max_ckpt;
     A.grad = grad;
     A.counters = counters;
     A.nrays = nrays;
     A.order = order;
-    k_adjoint<<<threads_total / 128, 128, 0, st>>>(A);
+    if (precision == PRR_PREC_FP32) k_adjoint<float><<<threads_total / 128, 128, 0, st>>>(A);
+    else k_adjoint<double><<<threads_total / 128, 128, 0, st>>>(A);
     return cudaGetLastError();
 }
 
@@ -344,12 +421,17 @@ cudaError_t launch_adjoint_order(const int *steps, long long nrays, unsigned *or
                                                      32, st);
 }
 
-size_t adjoint_checkpoint_bytes() { return sizeof(PhysRay<double>); }
+size_t adjoint_checkpoint_bytes(int precision)
+{
+    return precision == PRR_PREC_FP32 ? sizeof(PhysRay<float>) : sizeof(PhysRay<double>);
+}
 
-int adjoint_blocks_per_sm()
+int adjoint_blocks_per_sm(int precision)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint, 128, 0) != cudaSuccess) { cudaGetLastError(); return 1; }
+    cudaError_t e = precision == PRR_PREC_FP32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint<float>, 128, 0)
+                                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint<double>, 128, 0);
+    if (e != cudaSuccess) { cudaGetLastError(); return 1; }
     return n > 0 ? n : 1;
 }
 

@@ -1,0 +1,496 @@
+// k_ham.cu - the FP32 renderer of PHYSICAL frames (one pixel in flight per
+// thread, no split precision, no emission) with the geodesic in Hamiltonian
+// form.
+//
+// The geodesics of the Kerr-Schild metric g = eta + f l(x)l are integrated
+// as the canonical system of H = 1/2 g^{ab} p_a p_b with the inverse metric
+// g^{-1} = eta - f l l (l^a = eta^{ab} l_b, l^t = -1):
+//     dx^i/dlambda = p_i - f Lam l_i,
+//     dp_i/dlambda = 1/2 Lam^2 d_i f + f Lam d_i Lam,   Lam = l^a p_a,
+// and p_t = -E is a constant of the motion (the metric does not depend on
+// t), so the state is (x, y, z, p_x, p_y, p_z): six components instead of the
+// eight of (x, u), no coordinate time, and no directional derivatives or
+// raised contraction in the right-hand side (about 74 FP32 operations and 4
+// SFU operations per evaluation, against about 110 for the contraction
+// geod_ks evaluates for du/dlambda).  The velocity u = dx/dlambda, which the
+// sphere test, the sky lookup and the per-ray outputs need, is formed from
+// (x, p) where it is used.
+//
+// Everything else is the PHYSICAL mode of phys_stepper.cuh, unchanged:
+// Fehlberg's RKF45 tableau with the 4th-order solution propagated, the mixed
+// error test max_i |y5_i - y4_i| / (atol + rtol max(|y_i|, |y4_i|)) <= 1 over
+// the state's components, the step update 0.9 h err^(-1/5) clamped to
+// [hmin, hmax], Kahan-compensated FP32 updates, the reference's
+// accept/reject, intersection-mode, sphere-window and termination rules
+// (kernels/solver.cuh:142-219, metrics/schwarzschild.cuh:55-79,
+// scene/sphere.h:34-64), l < 1000 and the max_steps caps.  Initial data are
+// phys_init's null u, lowered once: p = g u.
+//
+// Scheduling is k_pair's (k_pair.cu): persistent CTAs, each lane owns one
+// pixel and integrates its SSAA samples in order with the RMS combine in
+// registers, one attempt per loop iteration, warp-aggregated refill of the
+// lanes whose pixel is complete every compaction_interval attempts.  The
+// three coordinate pairs (x, y), (p_x, p_y) and (z, p_z) share Blackwell's
+// paired FP32 instructions in the stage combinations, and the x/y twins of
+// the right-hand side (gradients, l, the gradient of Lam, the derivatives)
+// share them too.
+#include "kernels.cuh"
+#include "phys_pair.cuh"
+
+namespace prr {
+
+namespace {
+
+using namespace pv;
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ int find_frame_h(const long long *begin, int n, long long item)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(begin + mid) <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void warp_sum_add_h(unsigned long long *p, unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(p, v);
+}
+
+__device__ __forceinline__ uint8_t q8h(float v) { return (uint8_t)roundf(255.0f * fminf(fmaxf(v, 0.0f), 1.0f)); }
+
+// Per-ray constants of the right-hand side.
+struct HamConst {
+    float M2, a, a2, a4, pt;  // 2M, a, a^2, 4 a^2, p_t
+};
+
+// dy/dlambda at (P = (x, y), Q = (p_x, p_y), W = (z, p_z)); outputs dP, dQ, dW
+// in the same pairing.  r is the Kerr-Schild radius, r^4 - (R^2 - a^2) r^2 -
+// a^2 z^2 = 0; f = 2 M r^3 / (r^4 + a^2 z^2); l = ((r x + a y)/q, (r y - a
+// x)/q, z/r) with q = r^2 + a^2 (l_t = 1).
+PRR_DEV void ham_rhs(float2 P, float2 Q, float2 W, const HamConst &c, float2 &dP, float2 &dQ, float2 &dW)
+{
+    const float X = P.x, Y = P.y, z = W.x, pz = W.y;
+    const float Z2 = mul_(z, z);
+    const float R2 = fma_(X, X, fma_(Y, Y, Z2));
+    const float b = add_(R2, -c.a2);
+    const float S2 = fma_(b, b, mul_(c.a4, Z2));
+    const float iS = rsq_(S2);
+    const float S = mul_(S2, iS);
+    const float r2 = mul_(0.5f, add_(b, S));
+    const float ir = rsq_(r2);
+    const float r = mul_(r2, ir);
+    const float q = add_(r2, c.a2), iq = rcp_(q);
+    const float Sig = fma_(r2, r2, mul_(c.a2, Z2)), iSig = rcp_(Sig);
+    const float2 iq_ = sp(iq);
+    // gradients of r and f
+    const float2 dr = mul_(P, sp(mul_(r, iS)));
+    const float drz = mul_(mul_(z, q), mul_(iS, ir));
+    const float r3 = mul_(r2, r);
+    const float f = mul_(mul_(c.M2, r3), iSig);
+    const float c1 = mul_(f, fma_(mul_(-4.0f, r3), iSig, mul_(3.0f, ir)));
+    const float2 df = mul_(sp(c1), dr);
+    const float dfz = fma_(c1, drz, mul_(mul_(-2.0f, f), mul_(c.a2, mul_(z, iSig))));
+    // l and Lam = l.p - p_t
+    const float2 l = mul_(fma_(sp(r), P, f2(mul_(c.a, Y), neg_(mul_(c.a, X)))), iq_);
+    const float lz = mul_(z, ir);
+    const float px = Q.x, py = Q.y;
+    const float Lam = fma_(l.x, px, fma_(l.y, py, fma_(lz, pz, neg_(c.pt))));
+    // gradient of l.p at fixed p
+    const float P0 = fma_(mul_(-2.0f, r), fma_(px, l.x, mul_(py, l.y)), fma_(px, X, mul_(py, Y)));
+    const float Pp = fma_(P0, iq, neg_(mul_(pz, mul_(lz, ir))));
+    const float2 dL = fma_(dr, sp(Pp), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
+    const float dLz = fma_(drz, Pp, mul_(pz, ir));
+    // Hamilton's equations
+    const float fL = mul_(f, Lam);
+    const float hL2 = mul_(mul_(0.5f, Lam), Lam);
+    dQ = fma_(sp(hL2), df, mul_(sp(fL), dL));
+    dP = fma_(sp(neg_(fL)), l, Q);
+    dW = f2(fma_(neg_(fL), lz, pz), fma_(hL2, dfz, mul_(fL, dLz)));
+}
+
+// u = dx/dlambda (spatial) and u^t = -p_t + f Lam at (x, p), in FP32 with IEEE
+// square roots: used by the sphere test, the sky lookup and the outputs.
+PRR_DEV V4<float> ham_velocity(float x, float y, float z, float px, float py, float pz, const HamConst &c)
+{
+    const float R2 = x * x + y * y + z * z;
+    const float b = R2 - c.a2;
+    const float r2 = 0.5f * (b + sqrtf(b * b + c.a4 * z * z));
+    const float r = sqrtf(r2);
+    const float q = r2 + c.a2;
+    const float f = c.M2 * r2 * r / (r2 * r2 + c.a2 * z * z);
+    const float lx = (r * x + c.a * y) / q, ly = (r * y - c.a * x) / q, lz = z / r;
+    const float Lam = lx * px + ly * py + lz * pz - c.pt;
+    const float fL = f * Lam;
+    return {px - fL * lx, py - fL * ly, pz - fL * lz, fL - c.pt};
+}
+
+struct HamRay {
+    float2 P, Q, W;     // (x, y), (p_x, p_y), (z, p_z)
+    float2 cP, cQ, cW;  // Kahan compensation
+    float h, trace_h, l;
+    int i, accepted, intersect;
+};
+
+struct HSlot {
+    int frame, px, py, s, S;
+    float acc0, acc1, acc2;
+    bool busy, need;
+    HamRay R;
+    HamConst c;
+    Hot<float> q;
+};
+
+// phys_init's null initial data, lowered: p_a = g_ab u^b.
+__device__ __forceinline__ void ham_init(const FrameParams &fp, HSlot &sl, int s)
+{
+    PhysRay<float> U;
+    phys_init<float>(fp, sl.px, sl.py, s, U);
+    const float M = fp.metric == PRR_METRIC_FLAT ? 0.0f : fp.M, a = fp.metric == PRR_METRIC_KERR ? fp.a : 0.0f;
+    float g[16];
+    metric_ks<float>(U.x.x, U.x.y, U.x.z, M, a, g);
+    const float u[4] = {U.u.x, U.u.y, U.u.z, U.u.w};
+    float p[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) p[m] = g[4 * m] * u[0] + g[4 * m + 1] * u[1] + g[4 * m + 2] * u[2] + g[4 * m + 3] * u[3];
+    HamRay &R = sl.R;
+    R.P = make_float2(U.x.x, U.x.y);
+    R.Q = make_float2(p[0], p[1]);
+    R.W = make_float2(U.x.z, p[2]);
+    R.cP = R.cQ = R.cW = make_float2(0.0f, 0.0f);
+    R.h = fp.h; R.trace_h = fp.h; R.l = 0.0f;
+    R.i = 0; R.accepted = 0; R.intersect = 0;
+    sl.c = {2.0f * M, a, a * a, 4.0f * a * a, p[3]};
+}
+
+struct HamStep {
+    float2 dP, dQ, dW;  // 4th-order increments
+    float err, hn;
+};
+
+// The six Fehlberg stages on the pairs, the 4th-order increments, the scaled
+// error norm and the next step (as pv::stages does for (x, u)).
+PRR_DEV HamStep ham_stages(const HamRay &R, const HamConst &c, const Hot<float> &q)
+{
+    using F = Fehlberg;
+    const float h = R.h;
+    const float2 H = sp(h);
+    const float2 P = R.P, Q = R.Q, W = R.W;
+#define PC(v) sp((float)(v))
+#define RHS(kP, kQ, kW, zP, zQ, zW)                                                                                    \
+    {                                                                                                                  \
+        float2 dP_, dQ_, dW_;                                                                                          \
+        ham_rhs(zP, zQ, zW, c, dP_, dQ_, dW_);                                                                         \
+        kP = mul_(H, dP_); kQ = mul_(H, dQ_); kW = mul_(H, dW_);                                                        \
+    }
+    float2 k1P, k1Q, k1W, k2P, k2Q, k2W, k3P, k3Q, k3W, k4P, k4Q, k4W, k5P, k5Q, k5W, k6P, k6Q, k6W;
+    RHS(k1P, k1Q, k1W, P, Q, W)
+#define ST2(Y) fma_(PC(F::A21), k1##Y, Y)
+    RHS(k2P, k2Q, k2W, ST2(P), ST2(Q), ST2(W))
+#undef ST2
+#define ST3(Y) fma_(PC(F::A32), k2##Y, fma_(PC(F::A31), k1##Y, Y))
+    RHS(k3P, k3Q, k3W, ST3(P), ST3(Q), ST3(W))
+#undef ST3
+#define ST4(Y) fma_(PC(F::A43), k3##Y, fma_(PC(F::A42), k2##Y, fma_(PC(F::A41), k1##Y, Y)))
+    RHS(k4P, k4Q, k4W, ST4(P), ST4(Q), ST4(W))
+#undef ST4
+#define ST5(Y) fma_(PC(F::A54), k4##Y, fma_(PC(F::A53), k3##Y, fma_(PC(F::A52), k2##Y, fma_(PC(F::A51), k1##Y, Y))))
+    RHS(k5P, k5Q, k5W, ST5(P), ST5(Q), ST5(W))
+#undef ST5
+#define ST6(Y)                                                                                                         \
+    fma_(PC(F::A65), k5##Y, fma_(PC(F::A64), k4##Y, fma_(PC(F::A63), k3##Y, fma_(PC(F::A62), k2##Y,                \
+                                                                              fma_(PC(F::A61), k1##Y, Y)))))
+    RHS(k6P, k6Q, k6W, ST6(P), ST6(Q), ST6(W))
+#undef ST6
+#undef RHS
+    HamStep o;
+    float2 err2 = sp(0.0f);
+    const float2 rtol = sp(q.rtol), atol = sp(q.atol);
+#define FIN(Y, OUT)                                                                                                    \
+    {                                                                                                                  \
+        const float2 d = fma_(PC(F::K45), k5##Y, fma_(PC(F::K44), k4##Y, fma_(PC(F::K43), k3##Y, mul_(PC(F::K41), k1##Y)))); \
+        const float2 e = fma_(PC(F::E6), k6##Y, fma_(PC(F::E5), k5##Y, fma_(PC(F::E4), k4##Y,                          \
+                                                                          fma_(PC(F::E3), k3##Y, mul_(PC(F::E1), k1##Y))))); \
+        const float2 sc = fma_(rtol, max_(abs_(Y), abs_(add_(Y, d))), atol);                                           \
+        err2 = max_(err2, mul_(abs_(e), rcp_(sc)));                                                                    \
+        OUT = d;                                                                                                       \
+    }
+    FIN(P, o.dP) FIN(Q, o.dQ) FIN(W, o.dW)
+#undef FIN
+#undef PC
+    const float err = fmaxf(err2.x, err2.y);
+    o.err = err;
+    const float hn = mul_(mul_(0.9f, h), pow_(err, -0.2f));
+    o.hn = min_(max_(hn, q.hmin), q.hmax);
+    return o;
+}
+
+PRR_DEV void kahan2(float2 &s, float2 &c, float2 v)
+{
+    kahan_add(s.x, c.x, v.x);
+    kahan_add(s.y, c.y, v.y);
+}
+
+// phys_accept (phys_stepper.cuh) on the Hamiltonian state.
+PRR_DEV int ham_accept(const FrameParams &fp, const HSlot &sl, HamRay &R, const HamStep &st, int &result,
+                       V3<float> &colour, V4<float> &u_out)
+{
+    const Hot<float> &q = sl.q;
+    const float h = R.h, hn = st.hn;
+    if (R.intersect && R.i > 10000) R.intersect = 0;
+    if (R.i > 8 * q.max_steps) { result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0}; return STEP_DONE; }
+    if (st.err > 1.0f && h != q.hmin && !R.intersect) { R.h = hn; return STEP_CONTINUE; }
+
+    // candidate new state
+    float2 Pn = R.P, Qn = R.Q, Wn = R.W, cPn = R.cP, cQn = R.cQ, cWn = R.cW;
+    kahan2(Pn, cPn, st.dP);
+    kahan2(Qn, cQn, st.dQ);
+    kahan2(Wn, cWn, st.dW);
+    if (isnan(Pn.x + Pn.y + Wn.x + Qn.x + Qn.y + Wn.y)) {
+        result = PRR_RESULT_MATH_ERROR; colour = {0, 0, 0};
+        u_out = ham_velocity(R.P.x, R.P.y, R.W.x, R.Q.x, R.Q.y, R.W.y, sl.c);
+        return STEP_DONE;
+    }
+    const float xn = Pn.x, yn = Pn.y, zn = Wn.x;
+
+    // sphere geometry, shared by User_UPDATE (window h) and User_ENDLOOP
+    // (window = next step, or the previous one in intersection mode); the
+    // velocity is formed only near a sphere
+    bool hitU = false;
+    int candH = -1, candN = -1, candT = -1;
+    float dH = 1e11f, dN = 1e11f, dT = 1e11f;
+    float vx = 0, vy = 0, vz = 0, v2 = 0;
+    bool near = false;
+    for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<float>(fp.sph[s], xn, yn, zn);
+    if (near) {
+        const V4<float> un = ham_velocity(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
+        const float k = frsqrt<float>(un.x * un.x + un.y * un.y + un.z * un.z);
+        vx = un.x * k; vy = un.y * k; vz = un.z * k;
+        v2 = vx * vx + vy * vy + vz * vz;
+        for (int s = 0; s < q.nspheres; s++) {
+            float d;
+            if (!sphere_d<float>(fp.sph[s], xn, yn, zn, vx, vy, vz, v2, d)) continue;
+            const float dd = d * d;
+            if (!(dd > v2 * h)) { hitU = true; if (d <= dH) { dH = d; candH = s; } }
+            if (!(dd > v2 * hn) && d <= dN) { dN = d; candN = s; }
+            if (!(dd > v2 * R.trace_h) && d <= dT) { dT = d; candT = s; }
+        }
+    }
+    if (hitU && !R.intersect) {  // enter intersection mode; the step is retried at hmin
+        R.intersect = 1; R.h = q.hmin;
+        return STEP_CONTINUE;
+    }
+    R.P = Pn; R.Q = Qn; R.W = Wn; R.cP = cPn; R.cQ = cQn; R.cW = cWn;
+    R.accepted += 1;
+    int candE;
+    float dE;
+    if (!hitU) {
+        if (!R.intersect) R.h = hn;
+        R.trace_h = R.h;
+        if (R.intersect) { candE = candH; dE = dH; } else { candE = candN; dE = dN; }
+    } else {
+        candE = candT; dE = dT;
+    }
+    // User_ENDLOOP, on the squared radius
+    float r2 = xn * xn + yn * yn + zn * zn;
+    if (q.metric == PRR_METRIC_KERR) {
+        const float b = r2 - q.a * q.a;
+        const float S2 = b * b + 4.0f * q.a * q.a * zn * zn;
+        r2 = 0.5f * (b + S2 * frsqrt<float>(S2));
+    }
+    const bool escaped = r2 >= q.rout * q.rout;
+    if (escaped || (q.metric != PRR_METRIC_FLAT && r2 <= q.rstop * q.rstop)) {
+        result = PRR_RESULT_SUCCESS;
+        u_out = ham_velocity(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
+        colour = escaped ? escape_colour<float>(fp, u_out) : V3<float>{0.0f, 0.0f, 0.0f};
+        return STEP_DONE;
+    }
+    if (candE >= 0) {
+        result = PRR_RESULT_INTERSECTION;
+        colour = sphere_colour<float>(fp.sph[candE], xn, yn, zn, vx, vy, vz, dE);
+        u_out = {colour.x, colour.y, colour.z, 0.0f};
+        return STEP_DONE;
+    }
+    R.l += R.h;
+    if (R.accepted >= q.max_steps) {
+        result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0};
+        u_out = ham_velocity(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
+        return STEP_DONE;
+    }
+    return STEP_CONTINUE;
+}
+
+struct HCounts {
+    unsigned long long att = 0, acc = 0, rays = 0, esc = 0, cap = 0, hit = 0, inf = 0, nan = 0;
+};
+
+// A finished ray: counters, per-ray outputs, SSAA accumulation, next sample
+// or pixel output.  Returns true when the slot's pixel is complete.
+__device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, int result, V3<float> col,
+                                           const V4<float> &u, HCounts &c)
+{
+    const FrameParams &fp = a.frames[sl.frame];
+    c.att += (unsigned)sl.R.i;
+    c.acc += (unsigned)sl.R.accepted;
+    c.rays++;
+    const float x = sl.R.P.x, y = sl.R.P.y, z = sl.R.W.x;
+    if (a.ray_state || a.sample_rgb || a.ray_steps) {  // per-ray outputs (single-frame runs)
+        const long long rid = ((long long)sl.py * fp.width + sl.px) * sl.S + sl.s;
+        if (a.ray_steps) a.ray_steps[fp.ray_begin + rid] = sl.R.accepted;
+        if (a.ray_state) {
+            float uvx, uvy;
+            ray_uv(fp, sl.px, sl.py, sl.s, uvx, uvy);
+            float *o = a.ray_state + 12 * rid;
+            o[0] = uvx; o[1] = uvy; o[2] = (float)result;
+            o[3] = x; o[4] = y; o[5] = z; o[6] = 0.0f;  // the coordinate time is not integrated
+            o[7] = u.x; o[8] = u.y; o[9] = u.z; o[10] = u.w;
+            o[11] = (float)sl.R.accepted;
+        }
+        if (a.sample_rgb) {
+            float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
+            o[0] = col.x; o[1] = col.y; o[2] = col.z;
+        }
+    }
+    if (result == PRR_RESULT_SUCCESS) {
+        if (metric_radius<float>(fp, x, y, z) >= sl.q.rout) c.esc++; else c.cap++;
+    } else if (result == PRR_RESULT_INTERSECTION) c.hit++;
+    else if (result == PRR_RESULT_INFINITE_GEO) c.inf++;
+    else c.nan++;
+    if (sl.S == 1) {
+        sl.acc0 = fminf(fmaxf(col.x, 0.f), 1.f); sl.acc1 = fminf(fmaxf(col.y, 0.f), 1.f); sl.acc2 = fminf(fmaxf(col.z, 0.f), 1.f);
+    } else {
+        sl.acc0 += fminf(fmaxf(col.x * col.x, 0.f), 1.f);
+        sl.acc1 += fminf(fmaxf(col.y * col.y, 0.f), 1.f);
+        sl.acc2 += fminf(fmaxf(col.z * col.z, 0.f), 1.f);
+    }
+    sl.s += 1;
+    if (sl.s < sl.S) {
+        ham_init(fp, sl, sl.s);
+        return false;
+    }
+    float o0 = sl.acc0, o1 = sl.acc1, o2 = sl.acc2;
+    if (sl.S > 1) { o0 = sqrtf(o0 / (float)sl.S); o1 = sqrtf(o1 / (float)sl.S); o2 = sqrtf(o2 / (float)sl.S); }
+    const long long op = fp.pix_begin + (long long)sl.py * fp.width + sl.px;
+    if (a.image) { a.image[3 * op] = o0; a.image[3 * op + 1] = o1; a.image[3 * op + 2] = o2; }
+    if (a.rgb8 && !fp.fxaa) { a.rgb8[3 * op] = q8h(o0); a.rgb8[3 * op + 1] = q8h(o1); a.rgb8[3 * op + 2] = q8h(o2); }
+    return true;
+}
+
+__device__ __forceinline__ void ham_start(const PersistentArgs &a, HSlot &sl, long long it)
+{
+    sl.frame = find_frame_h(a.frame_pix_begin, a.nframes, it);
+    const FrameParams &fp = a.frames[sl.frame];
+    const long long p = it - __ldg(a.frame_pix_begin + sl.frame);
+    sl.px = (int)(p % fp.width);
+    sl.py = (int)(p / fp.width);
+    sl.S = fp.samples;
+    sl.s = 0;
+    sl.acc0 = sl.acc1 = sl.acc2 = 0.f;
+    sl.q = make_hot<float>(fp);
+    ham_init(fp, sl, 0);
+    sl.busy = true;
+}
+
+}  // namespace
+
+// Resident CTAs per SM the small-CTA instantiation is built for.
+#ifndef PRR_HAM_SMALL_MINB
+#define PRR_HAM_SMALL_MINB 8
+#endif
+
+template <int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    HSlot sl;
+    HCounts cnt;
+    sl.busy = false; sl.need = true;
+    sl.frame = 0; sl.px = sl.py = sl.s = 0; sl.S = 1;
+    sl.acc0 = sl.acc1 = sl.acc2 = 0.f;
+    const long long t0 = clock64();
+    unsigned iter = 0;
+    const unsigned ci = a.compaction_interval > 1 ? (unsigned)a.compaction_interval : 1u;
+    unsigned since = ci;
+    while (true) {
+        // ---- warp-aggregated refill of the lanes whose pixel is complete ----
+        if (++since >= ci || __ballot_sync(FULL, sl.busy) == 0) {
+            since = 0;
+            const unsigned m = __ballot_sync(FULL, sl.need);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(&a.counters[C_WORK], (unsigned long long)__popc(m));
+                base = __shfl_sync(FULL, base, leader);
+                if (sl.need) {
+                    const long long it = (long long)base + __popc(m & lt);
+                    sl.need = false;
+                    if (it < a.total_pixels) ham_start(a, sl, it);
+                    else sl.busy = false;
+                }
+            }
+        }
+        if (__ballot_sync(FULL, sl.busy) == 0) {
+            if (__ballot_sync(FULL, sl.need) == 0) break;  // the queue is exhausted for every lane
+            since = ci;
+            continue;
+        }
+        if (a.watchdog_cycles > 0 && ((++iter) & 255u) == 0) {
+            unsigned stop = 0;
+            if (lane == 0) {
+                if (clock64() - t0 > a.watchdog_cycles) atomicExch((unsigned long long *)&a.counters[C_TIMEOUT], 1ull);
+                stop = (unsigned)*(volatile unsigned long long *)&a.counters[C_TIMEOUT];
+            }
+            if (__shfl_sync(FULL, stop, 0)) break;
+        }
+        if (!sl.busy) continue;
+        // the loop bound of trace_RKF (l < 1000, solver.cuh:158) and the attempt counter
+        if (!(sl.R.l < 1000.0f)) {
+            const V4<float> u = ham_velocity(sl.R.P.x, sl.R.P.y, sl.R.W.x, sl.R.Q.x, sl.R.Q.y, sl.R.W.y, sl.c);
+            if (ham_finish(a, sl, PRR_RESULT_INFINITE_GEO, {0.f, 0.f, 0.f}, u, cnt)) { sl.busy = false; sl.need = true; }
+            continue;
+        }
+        sl.R.i += 1;
+        const HamStep st = ham_stages(sl.R, sl.c, sl.q);
+        int result = 0;
+        V3<float> col;
+        V4<float> u;
+        const int r = ham_accept(a.frames[sl.frame], sl, sl.R, st, result, col, u);
+        if (r == STEP_CONTINUE) continue;
+        if (ham_finish(a, sl, result, col, u, cnt)) { sl.busy = false; sl.need = true; }
+    }
+    warp_sum_add_h(&a.counters[C_ATTEMPTS], cnt.att);
+    warp_sum_add_h(&a.counters[C_ACCEPTED], cnt.acc);
+    warp_sum_add_h(&a.counters[C_RAYS], cnt.rays);
+    warp_sum_add_h(&a.counters[C_ESCAPED], cnt.esc);
+    warp_sum_add_h(&a.counters[C_CAPTURED], cnt.cap);
+    warp_sum_add_h(&a.counters[C_INTERSECTION], cnt.hit);
+    warp_sum_add_h(&a.counters[C_INFINITE], cnt.inf);
+    warp_sum_add_h(&a.counters[C_MATH_ERROR], cnt.nan);
+}
+
+cudaError_t launch_ham(const PersistentArgs &a, int block, int blocks_per_sm, int nsm, cudaStream_t st)
+{
+    if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
+    int grid = nsm * blocks_per_sm;
+    if (grid < 1) grid = 1;
+    if (block <= 64) k_ham<64, PRR_HAM_SMALL_MINB><<<grid, block, 0, st>>>(a);
+    else k_ham<256, 1><<<grid, block, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+int ham_occupancy(int block)
+{
+    int n = 0;
+    cudaError_t e = block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<64, PRR_HAM_SMALL_MINB>, block, 0)
+                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<256, 1>, block, 0);
+    if (e != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n;
+}
+
+}  // namespace prr

@@ -56,17 +56,24 @@ struct PersistentArgs {
     int compaction_interval;     // attempts between warp refills (>= 1)
     long long watchdog_cycles;   // 0 = off
     int rays_per_thread;         // FP32: pixel slots in flight per thread (1 or 2; 0 = 1)
-    int *ray_steps;              // optional: accepted steps per ray (FP64/table/split kernels, single frame)
+    int *ray_steps;              // optional: accepted steps per ray (not k_pair; single frame)
     int emission;                // 1 = some frame has plasma emission (the kernels with emission.cuh)
+    int hamiltonian;             // 1 = FP32 one-slot renders integrate (x, p) in Hamiltonian form (k_ham.cu)
 };
-// Dispatches to the kernel of the precision: FP32 with the register
-// contraction and the FP32 pass of SPLIT -> k_pair (k_pair.cu,
-// rays_per_thread slots per thread); FP64 and the Christoffel-table
-// variant -> k_persistent.
+// Dispatches to the kernel of the precision: FP32 with one pixel slot per
+// thread, no emission and a.hamiltonian -> k_ham (k_ham.cu); other FP32
+// renders with the register contraction and the FP32 pass of SPLIT ->
+// k_pair (k_pair.cu, rays_per_thread slots per thread); FP64 and the
+// Christoffel-table variant -> k_persistent.
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st);
 
 // k_persistent.cu: resident CTAs per SM of the kernel launch_persistent picks.
-int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread = 1, int emission = 0);
+int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread = 1, int emission = 0,
+                         int hamiltonian = 0);
+
+// k_ham.cu: the FP32 renderer in Hamiltonian form (one pixel slot per thread).
+cudaError_t launch_ham(const PersistentArgs &a, int block, int blocks_per_sm, int nsm, cudaStream_t st);
+int ham_occupancy(int block);
 
 // k_pair.cu: the FP32 renderer with `rpt` pixel slots per thread; `split`:
 // the FP32 pass of a split-precision render (rpt 1; needs sample_rgb and
@@ -86,22 +93,23 @@ cudaError_t launch_plain_frame(const FrameParams *d_fp, const FrameParams &h_fp,
                                unsigned long long *counters, int geod_table, cudaStream_t st, int *launches);
 size_t plain_ray_record_bytes();
 
-// k_adjoint.cu: discrete adjoint of one PHYSICAL frame (FP64).
+// k_adjoint.cu: discrete adjoint of one PHYSICAL frame: forward steps in
+// `precision` (PRR_PREC_FP32 or FP64), adjoint and reduction in FP64.
 struct AdjointParamsHost {
     double spin, mass, incl, cam_r, phase, sph_R, sph_z;
     int sphere;
 };
 cudaError_t launch_adjoint(const FrameParams *d_fp, const AdjointParamsHost &p, const float *dL, const float *image,
                            void *ckpt, int max_ckpt, int threads_total, double *grad, unsigned long long *counters,
-                           long long nrays, const unsigned *order, cudaStream_t st);
+                           long long nrays, const unsigned *order, int precision, cudaStream_t st);
 // k_adjoint.cu: ray order for the adjoint, longest first: `order` receives the
 // ray indices sorted by descending accepted-step count `steps` (nrays
 // entries), so the rays a warp processes together have similar lengths.
 // scratch: adjoint_order_bytes(nrays) bytes.
 size_t adjoint_order_bytes(long long nrays);
 cudaError_t launch_adjoint_order(const int *steps, long long nrays, unsigned *order, void *scratch, cudaStream_t st);
-size_t adjoint_checkpoint_bytes();
-int adjoint_blocks_per_sm();  // resident 128-thread CTAs of k_adjoint per SM
+size_t adjoint_checkpoint_bytes(int precision);
+int adjoint_blocks_per_sm(int precision);  // resident 128-thread CTAs of k_adjoint per SM
 constexpr int ADJ_CHECKPOINT_INTERVAL = 64;
 
 // fma_peak.cu

@@ -171,13 +171,14 @@ extern "C" prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, co
     a.rgb8 = d_rgb8;
     a.counters = (unsigned long long *)base;
     a.emission = plan.any_emission;
+    a.hamiltonian = 1;
     // the launch shape prr_autotune picks for the 1080p Kerr workload: CTAs of
     // 64 threads at their occupancy limit, one pixel per thread, a warp refill
     // every 64 attempts
     const int block = 64;
     a.compaction_interval = 64;
     a.rays_per_thread = 1;
-    const int bpsm = persistent_occupancy(plan.precision, 0, block, 1, plan.any_emission);
+    const int bpsm = persistent_occupancy(plan.precision, 0, block, 1, plan.any_emission, 1);
     if (e == cudaSuccess) e = launch_persistent(a, plan.precision, block, bpsm > 0 ? bpsm : 1, nsm, st);
     for (int f = 0; f < n && e == cudaSuccess; f++) {
         const FrameParams &p = plan.fp[f];

@@ -121,7 +121,8 @@ prr_status emission_params(prr_ctx *ctx, int f, const prr_frame_desc &d, EmisPar
 int resolve_bpsm(prr_ctx *ctx, int precision, bool emission)
 {
     if (ctx->cfg.blocks_per_sm > 0) return ctx->cfg.blocks_per_sm;
-    int b = persistent_occupancy(precision, ctx->geod_table == 1, ctx->cfg.block_size, ctx->cfg.rays_per_thread, emission);
+    int b = persistent_occupancy(precision, ctx->geod_table == 1, ctx->cfg.block_size, ctx->cfg.rays_per_thread, emission,
+                                 ctx->hamiltonian);
     return b > 0 ? b : 1;
 }
 
@@ -261,6 +262,7 @@ static PersistentArgs persistent_args(prr_ctx *ctx, const RenderPlan &plan)
     a.total_pixels = plan.total_pixels;
     a.counters = (unsigned long long *)ctx->counters.p;
     a.geod_table = ctx->geod_table == 1;
+    a.hamiltonian = ctx->hamiltonian;
     a.compaction_interval = ctx->cfg.compaction_interval;
     a.watchdog_cycles = ctx->watchdog_cycles;
     a.rays_per_thread = ctx->cfg.rays_per_thread;
@@ -496,7 +498,8 @@ extern "C" prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, pr
     const int nrpt = (plan.precision == PRR_PREC_FP32 && ctx->geod_table != 1 && !plan.any_emission) ? 2 : 1;
     for (int rpt = 1; rpt <= nrpt; rpt++)
         for (int bi = 0; bi < 3; bi++) {
-            const int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi], rpt, plan.any_emission);
+            const int occ = persistent_occupancy(plan.precision, ctx->geod_table == 1, blocks[bi], rpt, plan.any_emission,
+                                                 ctx->hamiltonian);
             if (occ < 1) continue;
             for (int ii = 0; ii < 4; ii++) {
                 ctx->cfg.block_size = blocks[bi];
@@ -542,8 +545,10 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
         ctx->err = "prr_adjoint: needs an orbit camera (position (r sin i, 0, r cos i), yaw pi, pitch i - pi/2)";
         return PRR_ERR_INVALID;
     }
+    // forward steps in FP32 for FP32 frames, FP64 otherwise (SPLIT included); the adjoint is FP64
+    const int prec = d.precision == PRR_PREC_FP32 ? PRR_PREC_FP32 : PRR_PREC_FP64;
     prr_frame_desc f64 = d;
-    f64.precision = PRR_PREC_FP64;
+    f64.precision = prec;
     RenderPlan plan;
     prr_status s = build_plan(ctx, &f64, 1, plan);
     if (s != PRR_OK) return s;
@@ -572,9 +577,9 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
         ap.phase = std::atan2((double)S.center[1], (double)S.center[0]);
         ap.sph_z = S.center[2];
     }
-    const int threads = ctx->nsm * adjoint_blocks_per_sm() * 128;  // one resident wave
+    const int threads = ctx->nsm * adjoint_blocks_per_sm(prec) * 128;  // one resident wave
     const int max_ckpt = d.max_steps / ADJ_CHECKPOINT_INTERVAL + 2;
-    if ((s = alloc(ctx, ctx->adj_ckpt, (size_t)threads * max_ckpt * adjoint_checkpoint_bytes(), "adjoint checkpoints")) != PRR_OK) return s;
+    if ((s = alloc(ctx, ctx->adj_ckpt, (size_t)threads * max_ckpt * adjoint_checkpoint_bytes(prec), "adjoint checkpoints")) != PRR_OK) return s;
     if ((s = alloc(ctx, ctx->adj_dl, (size_t)npx * 3 * sizeof(float) + 8 * sizeof(double), "adjoint inputs")) != PRR_OK) return s;
     float *d_dl = (float *)ctx->adj_dl.p;
     double *d_grad = (double *)((char *)ctx->adj_dl.p + ((size_t)npx * 3 * sizeof(float) + 7) / 8 * 8);
@@ -585,7 +590,7 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
     PRR_CK(ctx, cudaEventRecord(ctx->e0, st));
     PRR_CK(ctx, launch_adjoint_order(d_steps, nrays, d_order, d_sort_scratch, st));
     PRR_CK(ctx, launch_adjoint((const FrameParams *)ctx->frames.p, ap, d_dl, (const float *)ctx->image.p, ctx->adj_ckpt.p,
-                               max_ckpt, threads, d_grad, (unsigned long long *)ctx->counters.p, nrays, d_order, st));
+                               max_ckpt, threads, d_grad, (unsigned long long *)ctx->counters.p, nrays, d_order, prec, st));
     PRR_CK(ctx, cudaEventRecord(ctx->e1, st));
     PRR_CK(ctx, cudaMemcpyAsync(grads, d_grad, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
     PRR_CK(ctx, cudaStreamSynchronize(st));

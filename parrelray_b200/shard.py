@@ -112,7 +112,8 @@ def render_sharded(frames: Sequence, render: Callable[[list], tuple[list, float]
             ms = float(t)
     else:
         raise ValueError("schedule must be 'pull' or 'static'")
-    t = torch.tensor([ms], dtype=torch.float64)
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"  # NCCL reduces device tensors only
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     max_ms = float(t.item())
     if gather_to is None:
