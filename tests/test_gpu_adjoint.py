@@ -109,3 +109,25 @@ def test_torch_wrapper_and_adam_fit(gpu, small_textures):
     assert losses[-1] < 0.75 * losses[0], fit
     assert 0.33 < q[0].item() < 0.99, fit
     assert math.radians(46.0) < q[1].item() < math.radians(70.0), fit
+
+
+def test_fp32_forward_adjoint_tracks_the_fp64_one(gpu, small_textures):
+    """The differentiable-render workload's form: forward steps in FP32 (tolerance 1e-6, Kahan-
+    compensated), adjoint and reduction in FP64.  Against the all-FP64 adjoint of the same frame
+    and loss: the two discrete maps differ only where an FP32 step decision flips, so the gradient
+    vectors agree to 2% (their norms), and each component the loss depends on strongly to 5%."""
+    tex = dict(small_textures)
+    tex[scenes.SKY_ID] = smooth_sky()
+    gpu.upload_textures(tex)
+    kw = dict(size=64, spin=0.3, incl_deg=45.0)
+    _, tgt, _ = gpu.render(scenes.kerr_512_adjoint(spin=0.7, incl_deg=60.0, size=64, precision=abi.PREC_FP64),
+                           want_float=True)
+    d64 = scenes.kerr_512_adjoint(precision=abi.PREC_FP64, **kw)
+    _, cur, _ = gpu.render(d64, want_float=True)
+    dl = 2.0 * (cur[0] - tgt[0])
+    g64, s64 = gpu_adjoint(gpu, d64, dl)
+    g32, s32 = gpu_adjoint(gpu, scenes.kerr_512_adjoint(precision=abi.PREC_FP32, **kw), dl)
+    assert s32.n_math_error == 0 and s32.accepted > 0
+    assert np.linalg.norm(g32 - g64) <= 0.02 * np.linalg.norm(g64), (g32, g64)
+    big = np.abs(g64) > 0.1 * np.abs(g64).max()
+    assert np.all(np.abs(g32[big] - g64[big]) <= 0.05 * np.abs(g64[big])), (g32, g64)
