@@ -70,15 +70,16 @@ FLOPS_STAGES = 492
 FLOPS_GEOD_KERR = 168
 F_ATTEMPT = 6 * FLOPS_GEOD_KERR + FLOPS_STAGES
 
-# FP32 operations the tracing kernel actually executes per attempt, from ncu's instruction counters
-# on the 960x540 copy of the headline frame (one launch, the launch shape the bench tunes):
-# FFMA and FFMA2 lanes x 2 (one FMA = 2 FLOP; a paired FFMA2 is two FMAs), FMUL/FADD and their paired
-# forms x 1 per result, divided by the launch's attempt counter.
-NCU_FLOP_PER_ATTEMPT = 0.0
+# FP32 operations the tracing kernels actually execute per attempt, from ncu's instruction counters on
+# the 960x540 copy of the headline frame (one launch, 64-thread CTAs at 8 per SM, refill every 64
+# attempts): FFMA x 2 FLOP, paired FFMA2 x 4 (two FMAs per thread instruction), FMUL/FADD x 1, paired
+# FMUL2/FADD2 x 2, summed and divided by the launch's attempt counter.  k_ham (the Hamiltonian form)
+# executes 1,055 FLOP per attempt; k_pair (the (x, u) contraction, the form F_ATTEMPT counts) 1,532.
+NCU_FLOP_PER_ATTEMPT = {"k_ham": 1055.0, "k_pair": 1532.0}
 NCU_FLOP_RULE = ("FP32 FLOP executed, from ncu sass_thread_inst_executed_op_{ffma,fmul,fadd}{,2}: FFMA 2, FFMA2 4, "
                  "FMUL/FADD 1, FMUL2/FADD2 2, per attempt")
 # DRAM bytes of one launch of the tracing kernel (ncu, 960x540 copy of the headline frame)
-TRAFFIC_PER_LAUNCH = 8.704512e6
+TRAFFIC_PER_LAUNCH = 8.76544e6
 
 
 def reserve_stdout():
@@ -902,7 +903,9 @@ def main():
     if rank == 0:
         fp32_peak, fp64_peak = ctx.measure_peak()
         achieved = st.attempts * F_ATTEMPT / (st.trace_ms * 1e-3) / 1e12
-        counted = st.attempts * NCU_FLOP_PER_ATTEMPT / (st.trace_ms * 1e-3) / 1e12
+        kname = pair_kernel_name(ctx.launch_config())
+        ncu_flop = NCU_FLOP_PER_ATTEMPT["k_ham" if kname.startswith("k_ham") else "k_pair"]
+        counted = st.attempts * ncu_flop / (st.trace_ms * 1e-3) / 1e12
         roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                     "frac": achieved / fp32_peak, "traffic": TRAFFIC_PER_LAUNCH,
                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of the tracing "
@@ -910,11 +913,13 @@ def main():
                                       "grow with the frame, and the outputs stay in L2",
                     "kernel": pair_kernel_name(ctx.launch_config()), "kernel_ms": st.trace_ms,
                     "flop_per_attempt": F_ATTEMPT, "attempts": st.attempts,
-                    "frac_basis": "algorithmic: attempts x F_attempt (the work of one RKF45 attempt in the Kerr-Schild "
-                                  "contraction form, FMA = 2) / kernel time",
+                    "frac_basis": "algorithmic: attempts x F_attempt (the work of one RKF45 attempt of the (x, u) "
+                                  "system in the Kerr-Schild contraction form, FMA = 2; ncu counts 1,532 executed "
+                                  "for it) / kernel time",
                     "ncu_counted": {"achieved": counted, "frac": counted / fp32_peak,
-                                    "flop_per_attempt": NCU_FLOP_PER_ATTEMPT,
-                                    "rule": NCU_FLOP_RULE},
+                                    "flop_per_attempt": ncu_flop, "rule": NCU_FLOP_RULE,
+                                    "note": "the FP32 work the kernel executes; the Hamiltonian form does one "
+                                            "attempt in fewer operations than F_attempt counts"},
                     "peak_source": "measured on this GPU: FMA-chain kernel (prr_measure_peak), burst",
                     "fp64_peak_tflops": fp64_peak}
         extra["roofline"] = roofline
