@@ -131,6 +131,60 @@ PRR_DEV void emis_step(const FrameParams &fp, T M, T a, const V4<T> &x, const V4
     if (e.absorb > 0.0f) E.trans *= exp(ediv<T>(-(T)e.absorb * n * dl, g));
 }
 
+// The same step for a ray carried by its covariant momentum p_mu (the
+// Hamiltonian form of the FP32 renderer): k.u_e = p_mu u_e^mu needs no
+// lowering, so nu_e = -u_e^t (p_i v^i + p_t); p_t is the constant of the
+// motion.  Same model, same arithmetic otherwise.
+template <class T>
+PRR_DEV void emis_step_p(const FrameParams &fp, T M, T a, T x, T y, T z, T px, T py, T pz, T pt, T h, EmisRay<T> &E)
+{
+    const EmisParams &e = fp.em;
+    if (e.kind == PRR_EMISSION_NONE) return;
+    T r, f, l[3];
+    ks_fl<T>(x, y, z, M, a, r, f, l);
+    if (!(r >= (T)e.r_in && r <= (T)e.r_out)) return;
+    T n, theta = 1, v[3];
+    bool flow = false;
+    if (e.kind == PRR_EMISSION_DISK) {
+        const T c = ediv<T>(z, r), hh = (T)e.height;
+        n = epow<T>(ediv<T>(r, (T)e.r_in), -(T)e.index) * exp(ediv<T>(-c * c, (T)2 * hh * hh));
+    } else {
+        if (!plasma_sample<T>(e.grid, x, y, z, n, theta, v)) return;
+        flow = e.grid.vel != nullptr;
+    }
+    if (!(n > (T)0)) return;
+    if (!flow) {
+        const T sm = sqrt(M), s = (T)e.sense;
+        const T om = ediv<T>(s * sm, r * sqrt(r) + s * a * sm);
+        v[0] = -om * y; v[1] = om * x; v[2] = 0;
+    }
+    const T lv = l[0] * v[0] + l[1] * v[1] + l[2] * v[2] + (T)1;
+    const T N = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] - (T)1 + f * lv * lv;  // g(xi, xi), xi = (v, 1)
+    if (!(N < (T)0)) return;
+    const T ut = ediv<T>((T)1, sqrt(-N));
+    const T nu_e = -ut * (px * v[0] + py * v[1] + pz * v[2] + pt);
+    if (!(nu_e > (T)0)) return;
+    const T g = ediv<T>(E.nu_cam, nu_e);
+    const T dl = E.nu_cam * h;
+    T j = n;
+    if (e.kind == PRR_EMISSION_GRID && e.temp_power != 0.0f) j *= pow(theta, (T)e.temp_power);
+    const T w = e.spectral == 0.0f ? g * g : pow(g, (T)2 + (T)e.spectral);
+    E.I += E.trans * w * j * dl;
+    if (e.absorb > 0.0f) E.trans *= exp(ediv<T>(-(T)e.absorb * n * dl, g));
+}
+
+// emis_init for the momentum form: nu_cam = -p_t / sqrt(1 - f) at the camera.
+template <class T> PRR_DEV void emis_init_p(const FrameParams &fp, T x, T y, T z, T pt, EmisRay<T> &E)
+{
+    const T M = fp.metric == PRR_METRIC_FLAT ? (T)0 : (T)fp.M;
+    const T a = fp.metric == PRR_METRIC_KERR ? (T)fp.a : (T)0;
+    T r, f, l[3];
+    ks_fl<T>(x, y, z, M, a, r, f, l);
+    E.nu_cam = -pt / sqrt((T)1 - f);
+    E.I = 0;
+    E.trans = 1;
+}
+
 // The pixel colour of a finished ray: trans * colour + map(gain * I).
 template <class T> PRR_DEV V3<float> emis_colour(const FrameParams &fp, const EmisRay<T> &E, V3<float> c)
 {

@@ -1,6 +1,6 @@
 // k_ham.cu - the FP32 renderer of PHYSICAL frames (one pixel in flight per
-// thread, no split precision, no emission) with the geodesic in Hamiltonian
-// form.
+// thread) with the geodesic in Hamiltonian form; with SPLIT, the FP32 pass of a
+// split-precision render; with EMIS, plasma emission along the rays.
 //
 // The geodesics of the Kerr-Schild metric g = eta + f l(x)l are integrated
 // as the canonical system of H = 1/2 g^{ab} p_a p_b with the inverse metric
@@ -34,6 +34,15 @@
 // paired FP32 instructions in the stage combinations, and the x/y twins of
 // the right-hand side (gradients, l, the gradient of Lam, the derivatives)
 // share them too.
+//
+// SPLIT (split precision): per-sample colours go to sample_rgb (the per-pixel
+// combine runs after the FP64 pass), and rays near a photon orbit
+// (near_critical on the initial data) or that dip below fp64_rfac * r_+ are
+// queued for k_fp64_requeue (k_persistent.cu), which integrates them again
+// from the camera in FP64, as for k_pair's split pass.
+//
+// EMIS: the emission of emission.cuh at every accepted step, in its momentum
+// form (emis_step_p: k.u_e = p_mu u_e^mu, no lowering needed).
 #include "kernels.cuh"
 #include "phys_pair.cuh"
 
@@ -141,16 +150,20 @@ struct HSlot {
     int frame, px, py, s, S;
     float acc0, acc1, acc2;
     bool busy, need;
+    bool crit;      // split precision: the sample's initial data are near a photon orbit
+    float flag_r;   // split precision: queue the ray for FP64 below this radius
     HamRay R;
     HamConst c;
     Hot<float> q;
+    EmisRay<float> E;  // emission kernels only
 };
 
 // phys_init's null initial data, lowered: p_a = g_ab u^b.
-__device__ __forceinline__ void ham_init(const FrameParams &fp, HSlot &sl, int s)
+template <bool SPLIT, bool EMIS = false> __device__ __forceinline__ void ham_init(const FrameParams &fp, HSlot &sl, int s)
 {
     PhysRay<float> U;
     phys_init<float>(fp, sl.px, sl.py, s, U);
+    if constexpr (SPLIT) sl.crit = near_critical<float>(fp, U);
     const float M = fp.metric == PRR_METRIC_FLAT ? 0.0f : fp.M, a = fp.metric == PRR_METRIC_KERR ? fp.a : 0.0f;
     float g[16];
     metric_ks<float>(U.x.x, U.x.y, U.x.z, M, a, g);
@@ -166,6 +179,7 @@ __device__ __forceinline__ void ham_init(const FrameParams &fp, HSlot &sl, int s
     R.h = fp.h; R.trace_h = fp.h; R.l = 0.0f;
     R.i = 0; R.accepted = 0; R.intersect = 0;
     sl.c = {2.0f * M, a, a * a, 4.0f * a * a, p[3]};
+    if constexpr (EMIS) emis_init_p<float>(fp, U.x.x, U.x.y, U.x.z, p[3], sl.E);
 }
 
 struct HamStep {
@@ -237,7 +251,8 @@ PRR_DEV void kahan2(float2 &s, float2 &c, float2 v)
 }
 
 // phys_accept (phys_stepper.cuh) on the Hamiltonian state.
-PRR_DEV int ham_accept(const FrameParams &fp, const HSlot &sl, HamRay &R, const HamStep &st, int &result,
+template <bool EMIS>
+PRR_DEV int ham_accept(const FrameParams &fp, HSlot &sl, HamRay &R, const HamStep &st, int &result,
                        V3<float> &colour, V4<float> &u_out)
 {
     const Hot<float> &q = sl.q;
@@ -287,6 +302,7 @@ PRR_DEV int ham_accept(const FrameParams &fp, const HSlot &sl, HamRay &R, const 
     }
     R.P = Pn; R.Q = Qn; R.W = Wn; R.cP = cPn; R.cQ = cQn; R.cW = cWn;
     R.accepted += 1;
+    if constexpr (EMIS) emis_step_p<float>(fp, q.M, q.a, xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c.pt, h, sl.E);
     int candE;
     float dE;
     if (!hitU) {
@@ -316,6 +332,7 @@ PRR_DEV int ham_accept(const FrameParams &fp, const HSlot &sl, HamRay &R, const 
         u_out = {colour.x, colour.y, colour.z, 0.0f};
         return STEP_DONE;
     }
+    if (sl.flag_r > 0.0f && r2 < sl.flag_r * sl.flag_r) return STEP_FLAG64;
     R.l += R.h;
     if (R.accepted >= q.max_steps) {
         result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0};
@@ -326,20 +343,45 @@ PRR_DEV int ham_accept(const FrameParams &fp, const HSlot &sl, HamRay &R, const 
 }
 
 struct HCounts {
-    unsigned long long att = 0, acc = 0, rays = 0, esc = 0, cap = 0, hit = 0, inf = 0, nan = 0;
+    unsigned long long att = 0, acc = 0, rays = 0, esc = 0, cap = 0, hit = 0, inf = 0, nan = 0, f64 = 0;
 };
 
-// A finished ray: counters, per-ray outputs, SSAA accumulation, next sample
-// or pixel output.  Returns true when the slot's pixel is complete.
-__device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, int result, V3<float> col,
-                                           const V4<float> &u, HCounts &c)
+// Split precision: a ray queued for the FP64 pass.  Its colour slot is zeroed
+// here and overwritten by k_fp64_requeue, which counts it as a ray.  Returns
+// true when the slot's pixel is complete.
+__device__ __forceinline__ bool ham_flag(const PersistentArgs &a, HSlot &sl, HCounts &c)
 {
     const FrameParams &fp = a.frames[sl.frame];
     c.att += (unsigned)sl.R.i;
     c.acc += (unsigned)sl.R.accepted;
+    c.f64++;
+    const long long rid = ((long long)sl.py * fp.width + sl.px) * sl.S + sl.s;
+    const unsigned long long slot = atomicAdd(&a.counters[C_FP64_QUEUED], 1ull);
+    if ((long long)slot < a.fp64_capacity) a.fp64_queue[slot] = ((unsigned long long)sl.frame << 40) | (unsigned long long)rid;
+    float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
+    o[0] = o[1] = o[2] = 0.f;
+    sl.s += 1;
+    if (sl.s < sl.S) {
+        ham_init<true>(fp, sl, sl.s);
+        return false;
+    }
+    return true;
+}
+
+// A finished ray: counters, per-ray outputs, SSAA accumulation (split
+// precision: the per-sample colour), next sample or pixel output.  Returns
+// true when the slot's pixel is complete.
+template <bool SPLIT, bool EMIS>
+__device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, int result, V3<float> col,
+                                           const V4<float> &u, HCounts &c)
+{
+    const FrameParams &fp = a.frames[sl.frame];
+    if constexpr (EMIS) col = emis_colour<float>(fp, sl.E, col);
+    c.att += (unsigned)sl.R.i;
+    c.acc += (unsigned)sl.R.accepted;
     c.rays++;
     const float x = sl.R.P.x, y = sl.R.P.y, z = sl.R.W.x;
-    if (a.ray_state || a.sample_rgb || a.ray_steps) {  // per-ray outputs (single-frame runs)
+    if (!SPLIT && (a.ray_state || a.sample_rgb || a.ray_steps)) {  // per-ray outputs (single-frame runs)
         const long long rid = ((long long)sl.py * fp.width + sl.px) * sl.S + sl.s;
         if (a.ray_steps) a.ray_steps[fp.ray_begin + rid] = sl.R.accepted;
         if (a.ray_state) {
@@ -361,6 +403,17 @@ __device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, i
     } else if (result == PRR_RESULT_INTERSECTION) c.hit++;
     else if (result == PRR_RESULT_INFINITE_GEO) c.inf++;
     else c.nan++;
+    if constexpr (SPLIT) {
+        const long long rid = ((long long)sl.py * fp.width + sl.px) * sl.S + sl.s;
+        float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
+        o[0] = col.x; o[1] = col.y; o[2] = col.z;
+        sl.s += 1;
+        if (sl.s < sl.S) {
+            ham_init<true>(fp, sl, sl.s);
+            return false;
+        }
+        return true;
+    }
     if (sl.S == 1) {
         sl.acc0 = fminf(fmaxf(col.x, 0.f), 1.f); sl.acc1 = fminf(fmaxf(col.y, 0.f), 1.f); sl.acc2 = fminf(fmaxf(col.z, 0.f), 1.f);
     } else {
@@ -370,7 +423,7 @@ __device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, i
     }
     sl.s += 1;
     if (sl.s < sl.S) {
-        ham_init(fp, sl, sl.s);
+        ham_init<false, EMIS>(fp, sl, sl.s);
         return false;
     }
     float o0 = sl.acc0, o1 = sl.acc1, o2 = sl.acc2;
@@ -381,7 +434,7 @@ __device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, i
     return true;
 }
 
-__device__ __forceinline__ void ham_start(const PersistentArgs &a, HSlot &sl, long long it)
+template <bool SPLIT, bool EMIS> __device__ __forceinline__ void ham_start(const PersistentArgs &a, HSlot &sl, long long it)
 {
     sl.frame = find_frame_h(a.frame_pix_begin, a.nframes, it);
     const FrameParams &fp = a.frames[sl.frame];
@@ -392,7 +445,8 @@ __device__ __forceinline__ void ham_start(const PersistentArgs &a, HSlot &sl, lo
     sl.s = 0;
     sl.acc0 = sl.acc1 = sl.acc2 = 0.f;
     sl.q = make_hot<float>(fp);
-    ham_init(fp, sl, 0);
+    sl.flag_r = SPLIT ? fp.fp64_rfac * kerr_r_plus<float>(sl.q.M, sl.q.a) : -1.0f;
+    ham_init<SPLIT, EMIS>(fp, sl, 0);
     sl.busy = true;
 }
 
@@ -403,14 +457,15 @@ __device__ __forceinline__ void ham_start(const PersistentArgs &a, HSlot &sl, lo
 #define PRR_HAM_SMALL_MINB 8
 #endif
 
-template <int MAXT, int MINB>
+template <int MAXT, int MINB, bool SPLIT, bool EMIS>
 __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
 {
+    static_assert(!(SPLIT && EMIS), "emission renders in FP32 or FP64, not split");
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     HSlot sl;
     HCounts cnt;
-    sl.busy = false; sl.need = true;
+    sl.busy = false; sl.need = true; sl.crit = false; sl.flag_r = -1.0f;
     sl.frame = 0; sl.px = sl.py = sl.s = 0; sl.S = 1;
     sl.acc0 = sl.acc1 = sl.acc2 = 0.f;
     const long long t0 = clock64();
@@ -430,7 +485,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
                 if (sl.need) {
                     const long long it = (long long)base + __popc(m & lt);
                     sl.need = false;
-                    if (it < a.total_pixels) ham_start(a, sl, it);
+                    if (it < a.total_pixels) ham_start<SPLIT, EMIS>(a, sl, it);
                     else sl.busy = false;
                 }
             }
@@ -449,10 +504,15 @@ __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
             if (__shfl_sync(FULL, stop, 0)) break;
         }
         if (!sl.busy) continue;
+        // split precision: a ray near a photon orbit goes to the FP64 pass before its first attempt
+        if (SPLIT && sl.R.i == 0 && sl.crit) {
+            if (ham_flag(a, sl, cnt)) { sl.busy = false; sl.need = true; }
+            continue;
+        }
         // the loop bound of trace_RKF (l < 1000, solver.cuh:158) and the attempt counter
         if (!(sl.R.l < 1000.0f)) {
             const V4<float> u = ham_velocity(sl.R.P.x, sl.R.P.y, sl.R.W.x, sl.R.Q.x, sl.R.Q.y, sl.R.W.y, sl.c);
-            if (ham_finish(a, sl, PRR_RESULT_INFINITE_GEO, {0.f, 0.f, 0.f}, u, cnt)) { sl.busy = false; sl.need = true; }
+            if (ham_finish<SPLIT, EMIS>(a, sl, PRR_RESULT_INFINITE_GEO, {0.f, 0.f, 0.f}, u, cnt)) { sl.busy = false; sl.need = true; }
             continue;
         }
         sl.R.i += 1;
@@ -460,9 +520,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
         int result = 0;
         V3<float> col;
         V4<float> u;
-        const int r = ham_accept(a.frames[sl.frame], sl, sl.R, st, result, col, u);
+        const int r = ham_accept<EMIS>(a.frames[sl.frame], sl, sl.R, st, result, col, u);
         if (r == STEP_CONTINUE) continue;
-        if (ham_finish(a, sl, result, col, u, cnt)) { sl.busy = false; sl.need = true; }
+        const bool done = (SPLIT && r == STEP_FLAG64) ? ham_flag(a, sl, cnt) : ham_finish<SPLIT, EMIS>(a, sl, result, col, u, cnt);
+        if (done) { sl.busy = false; sl.need = true; }
     }
     warp_sum_add_h(&a.counters[C_ATTEMPTS], cnt.att);
     warp_sum_add_h(&a.counters[C_ACCEPTED], cnt.acc);
@@ -472,25 +533,42 @@ __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
     warp_sum_add_h(&a.counters[C_INTERSECTION], cnt.hit);
     warp_sum_add_h(&a.counters[C_INFINITE], cnt.inf);
     warp_sum_add_h(&a.counters[C_MATH_ERROR], cnt.nan);
+    if (SPLIT) warp_sum_add_h(&a.counters[C_FP64], cnt.f64);
 }
 
-cudaError_t launch_ham(const PersistentArgs &a, int block, int blocks_per_sm, int nsm, cudaStream_t st)
+template <bool SPLIT, bool EMIS> static cudaError_t ham_launch(const PersistentArgs &a, int block, int grid, cudaStream_t st)
 {
-    if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
-    int grid = nsm * blocks_per_sm;
-    if (grid < 1) grid = 1;
-    if (block <= 64) k_ham<64, PRR_HAM_SMALL_MINB><<<grid, block, 0, st>>>(a);
-    else k_ham<256, 1><<<grid, block, 0, st>>>(a);
+    if (block <= 64) k_ham<64, PRR_HAM_SMALL_MINB, SPLIT, EMIS><<<grid, block, 0, st>>>(a);
+    else k_ham<256, 1, SPLIT, EMIS><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-int ham_occupancy(int block)
+template <bool SPLIT, bool EMIS> static int ham_occ(int block)
 {
     int n = 0;
-    cudaError_t e = block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<64, PRR_HAM_SMALL_MINB>, block, 0)
-                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<256, 1>, block, 0);
+    cudaError_t e = block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<64, PRR_HAM_SMALL_MINB, SPLIT, EMIS>, block, 0)
+                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<256, 1, SPLIT, EMIS>, block, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
+}
+
+cudaError_t launch_ham(const PersistentArgs &a, bool split, int block, int blocks_per_sm, int nsm, cudaStream_t st)
+{
+    if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
+    if (split && (!a.sample_rgb || !a.fp64_queue)) return cudaErrorInvalidValue;
+    if (split && a.emission) return cudaErrorInvalidValue;
+    int grid = nsm * blocks_per_sm;
+    if (grid < 1) grid = 1;
+    if (split) return ham_launch<true, false>(a, block, grid, st);
+    if (a.emission) return ham_launch<false, true>(a, block, grid, st);
+    return ham_launch<false, false>(a, block, grid, st);
+}
+
+int ham_occupancy(int block, bool split, bool emission)
+{
+    if (split) return ham_occ<true, false>(block);
+    if (emission) return ham_occ<false, true>(block);
+    return ham_occ<false, false>(block);
 }
 
 }  // namespace prr

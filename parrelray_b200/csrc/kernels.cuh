@@ -61,8 +61,8 @@ struct PersistentArgs {
     int hamiltonian;             // 1 = FP32 one-slot renders integrate (x, p) in Hamiltonian form (k_ham.cu)
 };
 // Dispatches to the kernel of the precision: FP32 with one pixel slot per
-// thread, no emission and a.hamiltonian -> k_ham (k_ham.cu); other FP32
-// renders with the register contraction and the FP32 pass of SPLIT ->
+// thread (emission included) and the FP32 pass of SPLIT, with a.hamiltonian
+// -> k_ham (k_ham.cu); other FP32 renders with the register contraction ->
 // k_pair (k_pair.cu, rays_per_thread slots per thread); FP64 and the
 // Christoffel-table variant -> k_persistent.
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st);
@@ -71,9 +71,11 @@ cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block,
 int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread = 1, int emission = 0,
                          int hamiltonian = 0);
 
-// k_ham.cu: the FP32 renderer in Hamiltonian form (one pixel slot per thread).
-cudaError_t launch_ham(const PersistentArgs &a, int block, int blocks_per_sm, int nsm, cudaStream_t st);
-int ham_occupancy(int block);
+// k_ham.cu: the FP32 renderer in Hamiltonian form (one pixel slot per thread);
+// `split`: the FP32 pass of a split-precision render (needs sample_rgb and
+// fp64_queue); a.emission: the instantiation with plasma emission.
+cudaError_t launch_ham(const PersistentArgs &a, bool split, int block, int blocks_per_sm, int nsm, cudaStream_t st);
+int ham_occupancy(int block, bool split = false, bool emission = false);
 
 // k_pair.cu: the FP32 renderer with `rpt` pixel slots per thread; `split`:
 // the FP32 pass of a split-precision render (rpt 1; needs sample_rgb and
