@@ -576,16 +576,15 @@ def smooth_sky(w: int = 512, h: int = 256) -> np.ndarray:
     return t
 
 
-def adjoint_diagnosis(ctx, size: int, extra: dict, h: float = 1e-3) -> dict:
-    """At the fit's start (a = 0.3, i = 45 deg; FP64 renders and adjoint) and for its linearised loss
+def adjoint_diagnosis(ctx, size: int, extra: dict, h: float = 1e-3, margin: int = 2) -> dict:
+    """At the fit's start (a = 0.3, i = 45 deg; FP64 renders and adjoint) and for the linearised loss
     sum(w * image), w = 2 (image - target): the adjoint gradient against central differences of the
-    renders at +-h, over all pixels and over the pixels whose discrete events (result and accepted-step
-    count of the ray, from prr_trace_rays_f64) are the same at -h, 0 and +h.  The adjoint freezes those
-    events, so it is the derivative of the second sum; the first also carries the pixels whose ray
-    switches between sky and shadow (the silhouette) inside +-h."""
-    import ctypes as C
-
-    from parrelray_b200 import abi, scenes
+    renders at +-h (weights held fixed), (1) over all pixels, (2) over the pixels whose discrete events
+    (result and accepted-step count of the ray, from prr_trace_rays_f64) are the same at -h, 0 and +h,
+    and (3) over the fit's sky weights (inverse.sky_weights with `margin`).  The adjoint freezes those
+    events, so it is the derivative of (2); (1) also carries the silhouette pixels, whose ray switches
+    between sky and shadow inside +-h or winds near the photon orbit."""
+    from parrelray_b200 import abi, inverse, scenes
 
     def frame(a, incl):
         return scenes.kerr_512_adjoint(spin=a, incl_deg=incl, precision=abi.PREC_FP64, size=size, **extra)
@@ -598,18 +597,16 @@ def adjoint_diagnosis(ctx, size: int, extra: dict, h: float = 1e-3) -> dict:
         return (st[:, 2].astype(np.int64) * 1000003 + st[:, 11].astype(np.int64)).reshape(d.height, d.width)
 
     def adjoint(d, w):
-        g = np.zeros(5)
-        ast = abi.Stats()
-        w = np.ascontiguousarray(w, dtype=np.float32)
-        abi.check(abi.load().prr_adjoint(ctx.h, C.byref(d), w.ctypes.data_as(abi._fp), -1, g.ctypes.data_as(abi._dp),
-                                         C.byref(ast)), ctx.h)
-        return g
+        return ctx.adjoint(d, w)[0]
 
     tgt = image(frame(0.7, 60.0))
     d0 = frame(0.3, 45.0)
-    w = 2.0 * (image(d0) - tgt)
+    img0 = image(d0)
+    w = 2.0 * (img0 - tgt)
+    sky = inverse.sky_weights(img0, tgt, margin)[:, :, None]
     s0 = signature(d0)
     g_all = adjoint(d0, w)
+    g_sky = adjoint(d0, w * sky)
     out = {}
     hd = math.degrees(h)
     for name, k, (dp, dm) in (("spin", 0, (frame(0.3 + h, 45.0), frame(0.3 - h, 45.0))),
@@ -618,66 +615,54 @@ def adjoint_diagnosis(ctx, size: int, extra: dict, h: float = 1e-3) -> dict:
         same = (signature(dp) == s0) & (signature(dm) == s0)
         fd_all = float(np.sum(w * (ip - im)) / (2 * h))
         fd_same = float(np.sum(w * same[:, :, None] * (ip - im)) / (2 * h))
+        fd_sky = float(np.sum(w * sky * (ip - im)) / (2 * h))
         g_same = adjoint(d0, w * same[:, :, None])
-        out[name] = {"adjoint_all_pixels": float(g_all[k]), "adjoint_same_events": float(g_same[k]),
-                     "central_difference_same_events": fd_same, "central_difference_all_pixels": fd_all,
+        out[name] = {"adjoint_all_pixels": float(g_all[k]), "central_difference_all_pixels": fd_all,
+                     "adjoint_same_events": float(g_same[k]), "central_difference_same_events": fd_same,
+                     "adjoint_sky_weights": float(g_sky[k]), "central_difference_sky_weights": fd_sky,
                      "pixels_with_event_changes": float(1.0 - same.mean())}
+    out["sky_weight_fraction"] = float(sky.mean())
     out["what"] = ("h = 1e-3 (spin; inclination in radians); the adjoint equals the central difference over "
-                   "pixels whose events do not change, and the silhouette pixels decide the sign of the whole "
-                   "loss's spin derivative")
+                   "pixels whose events do not change and over the sky weights; over all pixels the silhouette "
+                   "decides the sign of the spin derivative, which is why the fit weights the loss")
     return out
 
 
-def bench_adam_fit(ctx, iters: int, size: int, lr: float = 0.01, decay: float = 0.99, sphere: bool = False):
+def bench_adam_fit(ctx, iters: int, size: int, lr: float = 0.01, decay: float = 0.99, sphere: bool = False,
+                   margin: int = 2):
     """The inverse problem of the differentiable-render workload: target rendered at a = 0.7,
     inclination 60 deg (camera r = 20M, sphere phase 30 deg); Adam on (a, inclination) from (0.3,
     45 deg) with the step decaying as lr * decay^t, every gradient from prr_adjoint on the FP32
-    render (FP32 forward steps, FP64 adjoint and reduction).  Smooth sky (see smooth_sky)."""
-    import ctypes as C
-
-    from parrelray_b200 import abi, scenes
+    render (FP32 forward steps, FP64 adjoint and reduction), the loss restricted to the pixels that
+    show sky in both images at least `margin` pixels from the shadow (inverse.sky_weights).  Smooth
+    sky (see smooth_sky)."""
+    from parrelray_b200 import abi, inverse, scenes
 
     ctx.upload_texture(scenes.SKY_ID, smooth_sky())
     extra = {} if sphere else {"spheres": []}
-    diagnosis = adjoint_diagnosis(ctx, size, extra)
-    _, tgt, _ = ctx.render(scenes.kerr_512_adjoint(spin=0.7, incl_deg=60.0, precision=abi.PREC_FP32, size=size,
-                                                   **extra), want_float=True)
-    target = tgt[0].astype(np.float64)
-    q = np.array([0.3, math.radians(45.0)])
-    m = np.zeros(2)
-    v = np.zeros(2)
-    b1, b2, eps = 0.9, 0.999, 1e-8
-    losses, dev_ms, best = [], 0.0, (float("inf"), None)
-    g = np.zeros(5)
-    st = abi.Stats()
-    t0 = time.perf_counter()
-    for it in range(1, iters + 1):
-        d = scenes.kerr_512_adjoint(spin=float(q[0]), incl_deg=math.degrees(q[1]), precision=abi.PREC_FP32, size=size,
-                                    **extra)
-        _, cur, rs = ctx.render(d, want_float=True)
-        diff = cur[0].astype(np.float64) - target
-        losses.append(float(np.sum(diff * diff)))
-        if losses[-1] < best[0]:
-            best = (losses[-1], q.copy())
-        dl = np.ascontiguousarray(2.0 * diff, dtype=np.float32)
-        abi.check(abi.load().prr_adjoint(ctx.h, C.byref(d), dl.ctypes.data_as(abi._fp), 0 if sphere else -1,
-                                         g.ctypes.data_as(abi._dp), C.byref(st)), ctx.h)
-        dev_ms += rs.kernel_ms + st.kernel_ms + st.trace_ms
-        grad = np.array([g[0], g[2]])
-        m = b1 * m + (1 - b1) * grad
-        v = b2 * v + (1 - b2) * grad * grad
-        q = q - lr * decay ** (it - 1) * (m / (1 - b1 ** it)) / (np.sqrt(v / (1 - b2 ** it)) + eps)
-        q[0] = min(max(q[0], 0.0), 0.99)
-    wall = time.perf_counter() - t0
+    diagnosis = adjoint_diagnosis(ctx, size, extra, margin=margin)
+
+    def frame_at(q):
+        return scenes.kerr_512_adjoint(spin=float(q[0]), incl_deg=math.degrees(q[1]), precision=abi.PREC_FP32,
+                                       size=size, **extra)
+
+    _, tgt, _ = ctx.render(frame_at((0.7, math.radians(60.0))), want_float=True)
+    h = inverse.fit(ctx, frame_at, tgt[0], (0.3, math.radians(45.0)), (0, 2), iters, lr, decay, margin,
+                    0 if sphere else -1, lo=(0.0, 0.0), hi=(0.99, math.pi))
     ctx.upload_textures(scenes.standard_textures())
+    loss = h["loss"]
+    qf = h["q_final"]
     return {"workload": f"Adam on (a, i) from (0.3, 45 deg) towards (0.7, 60 deg), {size}x{size}, FP32 forward / "
-                        f"FP64 adjoint, smooth sky"
-                        + ("" if sphere else ", no sphere"),
-            "iterations": iters, "lr": lr, "lr_decay": decay, "loss_first": losses[0], "loss_last": losses[-1],
-            "loss_min": best[0], "a_best": float(best[1][0]), "incl_best_deg": math.degrees(best[1][1]),
-            "a_final": float(q[0]), "incl_final_deg": math.degrees(q[1]),
-            "device_ms_per_iteration": dev_ms / iters, "wall_s": wall,
-            "losses_every_20": [round(x, 4) for x in losses[::20]],
+                        f"FP64 adjoint, smooth sky" + ("" if sphere else ", no sphere"),
+            "loss": f"L2 over the pixels that show sky in both images, >= {margin} px from a shadow pixel of either",
+            "iterations": iters, "lr": lr, "lr_decay": decay,
+            "loss_first": loss[0], "loss_last": loss[-1], "loss_min": min(loss),
+            "weighted_loss_first": h["weighted_loss"][0], "weighted_loss_last": h["weighted_loss"][-1],
+            "weighted_fraction_first_last": [h["weighted_fraction"][0], h["weighted_fraction"][-1]],
+            "a_final": float(qf[0]), "incl_final_deg": math.degrees(qf[1]),
+            "error_final": {"spin": float(qf[0]) - 0.7, "inclination_deg": math.degrees(qf[1]) - 60.0},
+            "device_ms_per_iteration": float(np.mean(h["device_ms"])), "wall_s": h["wall_s"],
+            "losses_every_20": [round(x, 4) for x in loss[::20]],
             "gradient_at_start": diagnosis}
 
 
@@ -1008,8 +993,6 @@ def main():
                                                "persistent_table": table_ms, "persistent_contraction": ms}}
         if not args.no_adjoint:
             # discrete adjoint of the 512x512 differentiable-render workload: one gradient of an L2 image loss
-            import ctypes as C
-
             n = args.adjoint_size
             _, tgt, _ = ctx.render(scenes.kerr_512_adjoint(spin=0.7, precision=abi.PREC_FP32, size=n), want_float=True)
             res = {"unit": "ms", "workload": f"kerr a=0.3 i=45 r=20, {n}x{n}, 1 sphere, bilinear sky, tol 1e-6; "
@@ -1018,12 +1001,9 @@ def main():
             for prec, key in ((abi.PREC_FP32, "fp32_forward"), (abi.PREC_FP64, "fp64_forward")):
                 start = scenes.kerr_512_adjoint(spin=0.3, incl_deg=45.0, precision=prec, size=n)
                 _, cur, _ = ctx.render(start, want_float=True)
-                dl = np.ascontiguousarray(2.0 * (cur[0] - tgt[0]), dtype=np.float32)
-                g = np.zeros(5, dtype=np.float64)
-                ast = abi.Stats()
+                dl = 2.0 * (cur[0] - tgt[0])
                 for _ in range(2):  # the first call sizes the checkpoint buffer
-                    abi.check(abi.load().prr_adjoint(ctx.h, C.byref(start), dl.ctypes.data_as(abi._fp), 0,
-                                                     g.ctypes.data_as(abi._dp), C.byref(ast)), ctx.h)
+                    g, ast = ctx.adjoint(start, dl, 0)
                 res[key] = {"ms": ast.kernel_ms, "forward_render_ms": ast.trace_ms, "grad": g.tolist(),
                             "accepted_steps": ast.accepted}
             # the workload's form (FP32 forward steps, FP64 adjoint and reduction) is the headline number

@@ -314,12 +314,15 @@ prr_status prr_trace_rays_f64(prr_ctx *ctx, const prr_frame_desc *frame,
  * [radians]; 0 when sphere_index is -1).  The frame must use an orbit camera:
  * position (r sin i, 0, r cos i), yaw pi, pitch i - pi/2.  Step sizes and
  * discrete events (accept/reject, termination, which sphere is hit) are
- * frozen at the forward run; the forward run and the adjoint are FP64, the
- * reduction is FP64.  The RMS2X2 sky is piecewise constant (zero gradient);
- * use PRR_BG_BILINEAR for sky gradients.  The rays are visited longest first
- * (ordered by their forward step counts) so rays sharing a warp have similar
- * lengths.  stats->kernel_ms is the device time of that ordering plus the
- * adjoint kernel, stats->trace_ms the FP64 forward render time. */
+ * frozen at the forward run.  The forward run is in the frame's precision
+ * (an FP32 frame takes FP32 RKF45 steps and checkpoints, FP64 and SPLIT
+ * frames FP64 ones); the reverse sweep (recomputed stages and their
+ * vector-Jacobian products) and the reduction are FP64 in both.  The RMS2X2
+ * sky is piecewise constant (zero gradient); use PRR_BG_BILINEAR for sky
+ * gradients.  The rays are visited longest first (ordered by their forward
+ * step counts) so rays sharing a warp have similar lengths.
+ * stats->kernel_ms is the device time of that ordering plus the adjoint
+ * kernel, stats->trace_ms the forward render time. */
 prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, const float *dL_dimage, int sphere_index,
                        double grads[5], prr_stats *stats);
 

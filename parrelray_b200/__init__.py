@@ -172,6 +172,19 @@ class Context:
                                                 rgb.ctypes.data_as(abi._dp), C.byref(stats)))
         return state, rgb, stats
 
+    def adjoint(self, frame: FrameDesc, dl_dimage: np.ndarray, sphere_index: int = -1):
+        """prr_adjoint: d(loss)/d(spin, mass, inclination, camera r, sphere
+        phase) for dl_dimage = d(loss)/d(float image), shape (h, w, 3).
+        Returns (float64 array of 5, Stats)."""
+        dl = np.ascontiguousarray(dl_dimage, dtype=np.float32)
+        if dl.size != frame.width * frame.height * 3:
+            raise ValueError("dl_dimage must hold width*height*3 values")
+        grads = np.zeros(5, dtype=np.float64)
+        stats = Stats()
+        self._check(self.lib.prr_adjoint(self.h, C.byref(frame), dl.ctypes.data_as(abi._fp), int(sphere_index),
+                                         grads.ctypes.data_as(abi._dp), C.byref(stats)))
+        return grads, stats
+
 
 class Graph:
     """A batch of frames recorded into a CUDA graph (prr_graph_*): device

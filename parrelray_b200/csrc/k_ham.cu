@@ -74,135 +74,139 @@ __device__ __forceinline__ void warp_sum_add_h(unsigned long long *p, unsigned l
 __device__ __forceinline__ uint8_t q8h(float v) { return (uint8_t)roundf(255.0f * fminf(fmaxf(v, 0.0f), 1.0f)); }
 
 // Per-ray constants of the right-hand side.
-struct HamConst {
-    float M2, a, a2, a4, pt;  // 2M, a, a^2, 4 a^2, p_t
+template <class T> struct HamConst {
+    T M2, a, a2, a4, pt;  // 2M, a, a^2, 4 a^2, p_t
 };
 
 // dy/dlambda at (P = (x, y), Q = (p_x, p_y), W = (z, p_z)); outputs dP, dQ, dW
 // in the same pairing.  r is the Kerr-Schild radius, r^4 - (R^2 - a^2) r^2 -
 // a^2 z^2 = 0; f = 2 M r^3 / (r^4 + a^2 z^2); l = ((r x + a y)/q, (r y - a
 // x)/q, z/r) with q = r^2 + a^2 (l_t = 1).
-PRR_DEV void ham_rhs(float2 P, float2 Q, float2 W, const HamConst &c, float2 &dP, float2 &dQ, float2 &dW)
+template <class T>
+PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP, P2<T> &dQ, P2<T> &dW)
 {
-    const float X = P.x, Y = P.y, z = W.x, pz = W.y;
-    const float Z2 = mul_(z, z);
-    const float R2 = fma_(X, X, fma_(Y, Y, Z2));
-    const float b = add_(R2, -c.a2);
-    const float S2 = fma_(b, b, mul_(c.a4, Z2));
-    const float iS = rsq_(S2);
-    const float S = mul_(S2, iS);
-    const float r2 = mul_(0.5f, add_(b, S));
-    const float ir = rsq_(r2);
-    const float r = mul_(r2, ir);
-    const float q = add_(r2, c.a2), iq = rcp_(q);
-    const float Sig = fma_(r2, r2, mul_(c.a2, Z2)), iSig = rcp_(Sig);
-    const float2 iq_ = sp(iq);
+    using V = P2<T>;
+    const T X = P.x, Y = P.y, z = W.x, pz = W.y;
+    const T Z2 = mul_(z, z);
+    const T R2 = fma_(X, X, fma_(Y, Y, Z2));
+    const T b = add_(R2, -c.a2);
+    const T S2 = fma_(b, b, mul_(c.a4, Z2));
+    const T iS = rsq_(S2);
+    const T S = mul_(S2, iS);
+    const T r2 = mul_(T(0.5), add_(b, S));
+    const T ir = rsq_(r2);
+    const T r = mul_(r2, ir);
+    const T q = add_(r2, c.a2), iq = rcp_(q);
+    const T Sig = fma_(r2, r2, mul_(c.a2, Z2)), iSig = rcp_(Sig);
+    const V iq_ = sp(iq);
     // gradients of r and f
-    const float2 dr = mul_(P, sp(mul_(r, iS)));
-    const float drz = mul_(mul_(z, q), mul_(iS, ir));
-    const float r3 = mul_(r2, r);
-    const float f = mul_(mul_(c.M2, r3), iSig);
-    const float c1 = mul_(f, fma_(mul_(-4.0f, r3), iSig, mul_(3.0f, ir)));
-    const float2 df = mul_(sp(c1), dr);
-    const float dfz = fma_(c1, drz, mul_(mul_(-2.0f, f), mul_(c.a2, mul_(z, iSig))));
+    const V dr = mul_(P, sp(mul_(r, iS)));
+    const T drz = mul_(mul_(z, q), mul_(iS, ir));
+    const T r3 = mul_(r2, r);
+    const T f = mul_(mul_(c.M2, r3), iSig);
+    const T c1 = mul_(f, fma_(mul_(T(-4), r3), iSig, mul_(T(3), ir)));
+    const V df = mul_(sp(c1), dr);
+    const T dfz = fma_(c1, drz, mul_(mul_(T(-2), f), mul_(c.a2, mul_(z, iSig))));
     // l and Lam = l.p - p_t
-    const float2 l = mul_(fma_(sp(r), P, f2(mul_(c.a, Y), neg_(mul_(c.a, X)))), iq_);
-    const float lz = mul_(z, ir);
-    const float px = Q.x, py = Q.y;
-    const float Lam = fma_(l.x, px, fma_(l.y, py, fma_(lz, pz, neg_(c.pt))));
+    const V l = mul_(fma_(sp(r), P, f2(mul_(c.a, Y), neg_(mul_(c.a, X)))), iq_);
+    const T lz = mul_(z, ir);
+    const T px = Q.x, py = Q.y;
+    const T Lam = fma_(l.x, px, fma_(l.y, py, fma_(lz, pz, neg_(c.pt))));
     // gradient of l.p at fixed p
-    const float P0 = fma_(mul_(-2.0f, r), fma_(px, l.x, mul_(py, l.y)), fma_(px, X, mul_(py, Y)));
-    const float Pp = fma_(P0, iq, neg_(mul_(pz, mul_(lz, ir))));
-    const float2 dL = fma_(dr, sp(Pp), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
-    const float dLz = fma_(drz, Pp, mul_(pz, ir));
+    const T P0 = fma_(mul_(T(-2), r), fma_(px, l.x, mul_(py, l.y)), fma_(px, X, mul_(py, Y)));
+    const T Pp = fma_(P0, iq, neg_(mul_(pz, mul_(lz, ir))));
+    const V dL = fma_(dr, sp(Pp), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
+    const T dLz = fma_(drz, Pp, mul_(pz, ir));
     // Hamilton's equations
-    const float fL = mul_(f, Lam);
-    const float hL2 = mul_(mul_(0.5f, Lam), Lam);
+    const T fL = mul_(f, Lam);
+    const T hL2 = mul_(mul_(T(0.5), Lam), Lam);
     dQ = fma_(sp(hL2), df, mul_(sp(fL), dL));
     dP = fma_(sp(neg_(fL)), l, Q);
     dW = f2(fma_(neg_(fL), lz, pz), fma_(hL2, dfz, mul_(fL, dLz)));
 }
 
-// u = dx/dlambda (spatial) and u^t = -p_t + f Lam at (x, p), in FP32 with IEEE
+// u = dx/dlambda (spatial) and u^t = -p_t + f Lam at (x, p), with IEEE
 // square roots: used by the sphere test, the sky lookup and the outputs.
-PRR_DEV V4<float> ham_velocity(float x, float y, float z, float px, float py, float pz, const HamConst &c)
+template <class T> PRR_DEV V4<T> ham_velocity(T x, T y, T z, T px, T py, T pz, const HamConst<T> &c)
 {
-    const float R2 = x * x + y * y + z * z;
-    const float b = R2 - c.a2;
-    const float r2 = 0.5f * (b + sqrtf(b * b + c.a4 * z * z));
-    const float r = sqrtf(r2);
-    const float q = r2 + c.a2;
-    const float f = c.M2 * r2 * r / (r2 * r2 + c.a2 * z * z);
-    const float lx = (r * x + c.a * y) / q, ly = (r * y - c.a * x) / q, lz = z / r;
-    const float Lam = lx * px + ly * py + lz * pz - c.pt;
-    const float fL = f * Lam;
+    const T R2 = x * x + y * y + z * z;
+    const T b = R2 - c.a2;
+    const T r2 = T(0.5) * (b + sqrt(b * b + c.a4 * z * z));
+    const T r = sqrt(r2);
+    const T q = r2 + c.a2;
+    const T f = c.M2 * r2 * r / (r2 * r2 + c.a2 * z * z);
+    const T lx = (r * x + c.a * y) / q, ly = (r * y - c.a * x) / q, lz = z / r;
+    const T Lam = lx * px + ly * py + lz * pz - c.pt;
+    const T fL = f * Lam;
     return {px - fL * lx, py - fL * ly, pz - fL * lz, fL - c.pt};
 }
 
-struct HamRay {
-    float2 P, Q, W;     // (x, y), (p_x, p_y), (z, p_z)
-    float2 cP, cQ, cW;  // Kahan compensation
-    float h, trace_h, l;
+template <class T> struct HamRay {
+    P2<T> P, Q, W;     // (x, y), (p_x, p_y), (z, p_z)
+    P2<T> cP, cQ, cW;  // Kahan compensation (FP32 only)
+    T h, trace_h, l;
     int i, accepted, intersect;
 };
 
-struct HSlot {
+template <class T> struct HSlot {
     int frame, px, py, s, S;
     float acc0, acc1, acc2;
     bool busy, need;
     bool crit;      // split precision: the sample's initial data are near a photon orbit
     float flag_r;   // split precision: queue the ray for FP64 below this radius
-    HamRay R;
-    HamConst c;
-    Hot<float> q;
-    EmisRay<float> E;  // emission kernels only
+    HamRay<T> R;
+    HamConst<T> c;
+    Hot<T> q;
+    EmisRay<T> E;  // emission kernels only
 };
 
 // phys_init's null initial data, lowered: p_a = g_ab u^b.
-template <bool SPLIT, bool EMIS = false> __device__ __forceinline__ void ham_init(const FrameParams &fp, HSlot &sl, int s)
+template <class T, bool SPLIT, bool EMIS = false>
+__device__ __forceinline__ void ham_init(const FrameParams &fp, HSlot<T> &sl, int s)
 {
-    PhysRay<float> U;
-    phys_init<float>(fp, sl.px, sl.py, s, U);
-    if constexpr (SPLIT) sl.crit = near_critical<float>(fp, U);
-    const float M = fp.metric == PRR_METRIC_FLAT ? 0.0f : fp.M, a = fp.metric == PRR_METRIC_KERR ? fp.a : 0.0f;
-    float g[16];
-    metric_ks<float>(U.x.x, U.x.y, U.x.z, M, a, g);
-    const float u[4] = {U.u.x, U.u.y, U.u.z, U.u.w};
-    float p[4];
+    PhysRay<T> U;
+    phys_init<T>(fp, sl.px, sl.py, s, U);
+    if constexpr (SPLIT) sl.crit = near_critical<T>(fp, U);
+    const T M = fp.metric == PRR_METRIC_FLAT ? T(0) : (T)fp.M, a = fp.metric == PRR_METRIC_KERR ? (T)fp.a : T(0);
+    T g[16];
+    metric_ks<T>(U.x.x, U.x.y, U.x.z, M, a, g);
+    const T u[4] = {U.u.x, U.u.y, U.u.z, U.u.w};
+    T p[4];
 #pragma unroll
     for (int m = 0; m < 4; m++) p[m] = g[4 * m] * u[0] + g[4 * m + 1] * u[1] + g[4 * m + 2] * u[2] + g[4 * m + 3] * u[3];
-    HamRay &R = sl.R;
-    R.P = make_float2(U.x.x, U.x.y);
-    R.Q = make_float2(p[0], p[1]);
-    R.W = make_float2(U.x.z, p[2]);
-    R.cP = R.cQ = R.cW = make_float2(0.0f, 0.0f);
-    R.h = fp.h; R.trace_h = fp.h; R.l = 0.0f;
+    HamRay<T> &R = sl.R;
+    R.P = f2(U.x.x, U.x.y);
+    R.Q = f2(p[0], p[1]);
+    R.W = f2(U.x.z, p[2]);
+    R.cP = R.cQ = R.cW = sp(T(0));
+    R.h = (T)fp.h; R.trace_h = (T)fp.h; R.l = T(0);
     R.i = 0; R.accepted = 0; R.intersect = 0;
-    sl.c = {2.0f * M, a, a * a, 4.0f * a * a, p[3]};
-    if constexpr (EMIS) emis_init_p<float>(fp, U.x.x, U.x.y, U.x.z, p[3], sl.E);
+    sl.c = {T(2) * M, a, a * a, T(4) * a * a, p[3]};
+    if constexpr (EMIS) emis_init_p<T>(fp, U.x.x, U.x.y, U.x.z, p[3], sl.E);
 }
 
-struct HamStep {
-    float2 dP, dQ, dW;  // 4th-order increments
-    float err, hn;
+template <class T> struct HamStep {
+    P2<T> dP, dQ, dW;  // 4th-order increments
+    T err, hn;
 };
 
 // The six Fehlberg stages on the pairs, the 4th-order increments, the scaled
 // error norm and the next step (as pv::stages does for (x, u)).
-PRR_DEV HamStep ham_stages(const HamRay &R, const HamConst &c, const Hot<float> &q)
+template <class T> PRR_DEV HamStep<T> ham_stages(const HamRay<T> &R, const HamConst<T> &c, const Hot<T> &q)
 {
     using F = Fehlberg;
-    const float h = R.h;
-    const float2 H = sp(h);
-    const float2 P = R.P, Q = R.Q, W = R.W;
-#define PC(v) sp((float)(v))
+    using V = P2<T>;
+    const T h = R.h;
+    const V H = sp(h);
+    const V P = R.P, Q = R.Q, W = R.W;
+#define PC(v) sp((T)(v))
 #define RHS(kP, kQ, kW, zP, zQ, zW)                                                                                    \
     {                                                                                                                  \
-        float2 dP_, dQ_, dW_;                                                                                          \
-        ham_rhs(zP, zQ, zW, c, dP_, dQ_, dW_);                                                                         \
+        V dP_, dQ_, dW_;                                                                                               \
+        ham_rhs<T>(zP, zQ, zW, c, dP_, dQ_, dW_);                                                                      \
         kP = mul_(H, dP_); kQ = mul_(H, dQ_); kW = mul_(H, dW_);                                                        \
     }
-    float2 k1P, k1Q, k1W, k2P, k2Q, k2W, k3P, k3Q, k3W, k4P, k4Q, k4W, k5P, k5Q, k5W, k6P, k6Q, k6W;
+    V k1P, k1Q, k1W, k2P, k2Q, k2W, k3P, k3Q, k3W, k4P, k4Q, k4W, k5P, k5Q, k5W, k6P, k6Q, k6W;
     RHS(k1P, k1Q, k1W, P, Q, W)
 #define ST2(Y) fma_(PC(F::A21), k1##Y, Y)
     RHS(k2P, k2Q, k2W, ST2(P), ST2(Q), ST2(W))
@@ -222,75 +226,83 @@ PRR_DEV HamStep ham_stages(const HamRay &R, const HamConst &c, const Hot<float> 
     RHS(k6P, k6Q, k6W, ST6(P), ST6(Q), ST6(W))
 #undef ST6
 #undef RHS
-    HamStep o;
-    float2 err2 = sp(0.0f);
-    const float2 rtol = sp(q.rtol), atol = sp(q.atol);
+    HamStep<T> o;
+    V err2 = sp(T(0));
+    const V rtol = sp(q.rtol), atol = sp(q.atol);
 #define FIN(Y, OUT)                                                                                                    \
     {                                                                                                                  \
-        const float2 d = fma_(PC(F::K45), k5##Y, fma_(PC(F::K44), k4##Y, fma_(PC(F::K43), k3##Y, mul_(PC(F::K41), k1##Y)))); \
-        const float2 e = fma_(PC(F::E6), k6##Y, fma_(PC(F::E5), k5##Y, fma_(PC(F::E4), k4##Y,                          \
+        const V d = fma_(PC(F::K45), k5##Y, fma_(PC(F::K44), k4##Y, fma_(PC(F::K43), k3##Y, mul_(PC(F::K41), k1##Y)))); \
+        const V e = fma_(PC(F::E6), k6##Y, fma_(PC(F::E5), k5##Y, fma_(PC(F::E4), k4##Y,                          \
                                                                           fma_(PC(F::E3), k3##Y, mul_(PC(F::E1), k1##Y))))); \
-        const float2 sc = fma_(rtol, max_(abs_(Y), abs_(add_(Y, d))), atol);                                           \
+        const V sc = fma_(rtol, max_(abs_(Y), abs_(add_(Y, d))), atol);                                           \
         err2 = max_(err2, mul_(abs_(e), rcp_(sc)));                                                                    \
         OUT = d;                                                                                                       \
     }
     FIN(P, o.dP) FIN(Q, o.dQ) FIN(W, o.dW)
 #undef FIN
 #undef PC
-    const float err = fmaxf(err2.x, err2.y);
+    const T err = max_(err2.x, err2.y);
     o.err = err;
-    const float hn = mul_(mul_(0.9f, h), pow_(err, -0.2f));
+    const T hn = mul_(mul_(T(0.9), h), pow_(err, T(-0.2)));
     o.hn = min_(max_(hn, q.hmin), q.hmax);
     return o;
 }
 
-PRR_DEV void kahan2(float2 &s, float2 &c, float2 v)
+// state update: Kahan-compensated in FP32, a plain sum in FP64 (whose
+// roundoff over 10^4 steps stays far below the tolerances)
+template <class V> PRR_DEV void upd2(V &s, V &c, V v)
 {
-    kahan_add(s.x, c.x, v.x);
-    kahan_add(s.y, c.y, v.y);
+    if constexpr (sizeof(s.x) == 4) {
+        kahan_add(s.x, c.x, v.x);
+        kahan_add(s.y, c.y, v.y);
+    } else {
+        s.x += v.x;
+        s.y += v.y;
+    }
 }
 
 // phys_accept (phys_stepper.cuh) on the Hamiltonian state.
-template <bool EMIS>
-PRR_DEV int ham_accept(const FrameParams &fp, HSlot &sl, HamRay &R, const HamStep &st, int &result,
-                       V3<float> &colour, V4<float> &u_out)
+template <class T, bool EMIS>
+PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const HamStep<T> &st, int &result,
+                       V3<float> &colour, V4<T> &u_out)
 {
-    const Hot<float> &q = sl.q;
-    const float h = R.h, hn = st.hn;
+    using V = P2<T>;
+    const Hot<T> &q = sl.q;
+    const T h = R.h, hn = st.hn;
     if (R.intersect && R.i > 10000) R.intersect = 0;
     if (R.i > 8 * q.max_steps) { result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0}; return STEP_DONE; }
-    if (st.err > 1.0f && h != q.hmin && !R.intersect) { R.h = hn; return STEP_CONTINUE; }
+    if (st.err > T(1) && h != q.hmin && !R.intersect) { R.h = hn; return STEP_CONTINUE; }
 
     // candidate new state
-    float2 Pn = R.P, Qn = R.Q, Wn = R.W, cPn = R.cP, cQn = R.cQ, cWn = R.cW;
-    kahan2(Pn, cPn, st.dP);
-    kahan2(Qn, cQn, st.dQ);
-    kahan2(Wn, cWn, st.dW);
+    V Pn = R.P, Qn = R.Q, Wn = R.W, cPn = R.cP, cQn = R.cQ, cWn = R.cW;
+    upd2(Pn, cPn, st.dP);
+    upd2(Qn, cQn, st.dQ);
+    upd2(Wn, cWn, st.dW);
     if (isnan(Pn.x + Pn.y + Wn.x + Qn.x + Qn.y + Wn.y)) {
         result = PRR_RESULT_MATH_ERROR; colour = {0, 0, 0};
-        u_out = ham_velocity(R.P.x, R.P.y, R.W.x, R.Q.x, R.Q.y, R.W.y, sl.c);
+        u_out = ham_velocity<T>(R.P.x, R.P.y, R.W.x, R.Q.x, R.Q.y, R.W.y, sl.c);
         return STEP_DONE;
     }
-    const float xn = Pn.x, yn = Pn.y, zn = Wn.x;
+    const T xn = Pn.x, yn = Pn.y, zn = Wn.x;
 
     // sphere geometry, shared by User_UPDATE (window h) and User_ENDLOOP
     // (window = next step, or the previous one in intersection mode); the
     // velocity is formed only near a sphere
     bool hitU = false;
     int candH = -1, candN = -1, candT = -1;
-    float dH = 1e11f, dN = 1e11f, dT = 1e11f;
-    float vx = 0, vy = 0, vz = 0, v2 = 0;
+    T dH = T(1e11), dN = T(1e11), dT = T(1e11);
+    T vx = 0, vy = 0, vz = 0, v2 = 0;
     bool near = false;
-    for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<float>(fp.sph[s], xn, yn, zn);
+    for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn, yn, zn);
     if (near) {
-        const V4<float> un = ham_velocity(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
-        const float k = frsqrt<float>(un.x * un.x + un.y * un.y + un.z * un.z);
+        const V4<T> un = ham_velocity<T>(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
+        const T k = frsqrt<T>(un.x * un.x + un.y * un.y + un.z * un.z);
         vx = un.x * k; vy = un.y * k; vz = un.z * k;
         v2 = vx * vx + vy * vy + vz * vz;
         for (int s = 0; s < q.nspheres; s++) {
-            float d;
-            if (!sphere_d<float>(fp.sph[s], xn, yn, zn, vx, vy, vz, v2, d)) continue;
-            const float dd = d * d;
+            T d;
+            if (!sphere_d<T>(fp.sph[s], xn, yn, zn, vx, vy, vz, v2, d)) continue;
+            const T dd = d * d;
             if (!(dd > v2 * h)) { hitU = true; if (d <= dH) { dH = d; candH = s; } }
             if (!(dd > v2 * hn) && d <= dN) { dN = d; candN = s; }
             if (!(dd > v2 * R.trace_h) && d <= dT) { dT = d; candT = s; }
@@ -302,9 +314,9 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot &sl, HamRay &R, const HamSte
     }
     R.P = Pn; R.Q = Qn; R.W = Wn; R.cP = cPn; R.cQ = cQn; R.cW = cWn;
     R.accepted += 1;
-    if constexpr (EMIS) emis_step_p<float>(fp, q.M, q.a, xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c.pt, h, sl.E);
+    if constexpr (EMIS) emis_step_p<T>(fp, q.M, q.a, xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c.pt, h, sl.E);
     int candE;
-    float dE;
+    T dE;
     if (!hitU) {
         if (!R.intersect) R.h = hn;
         R.trace_h = R.h;
@@ -313,33 +325,43 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot &sl, HamRay &R, const HamSte
         candE = candT; dE = dT;
     }
     // User_ENDLOOP, on the squared radius
-    float r2 = xn * xn + yn * yn + zn * zn;
+    T r2 = xn * xn + yn * yn + zn * zn;
     if (q.metric == PRR_METRIC_KERR) {
-        const float b = r2 - q.a * q.a;
-        const float S2 = b * b + 4.0f * q.a * q.a * zn * zn;
-        r2 = 0.5f * (b + S2 * frsqrt<float>(S2));
+        const T b = r2 - q.a * q.a;
+        const T S2 = b * b + T(4) * q.a * q.a * zn * zn;
+        r2 = T(0.5) * (b + S2 * frsqrt<T>(S2));
     }
     const bool escaped = r2 >= q.rout * q.rout;
     if (escaped || (q.metric != PRR_METRIC_FLAT && r2 <= q.rstop * q.rstop)) {
         result = PRR_RESULT_SUCCESS;
-        u_out = ham_velocity(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
-        colour = escaped ? escape_colour<float>(fp, u_out) : V3<float>{0.0f, 0.0f, 0.0f};
+        u_out = ham_velocity<T>(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
+        colour = escaped ? escape_colour<T>(fp, u_out) : V3<float>{0.0f, 0.0f, 0.0f};
         return STEP_DONE;
     }
     if (candE >= 0) {
         result = PRR_RESULT_INTERSECTION;
-        colour = sphere_colour<float>(fp.sph[candE], xn, yn, zn, vx, vy, vz, dE);
-        u_out = {colour.x, colour.y, colour.z, 0.0f};
+        colour = sphere_colour<T>(fp.sph[candE], xn, yn, zn, vx, vy, vz, dE);
+        u_out = {(T)colour.x, (T)colour.y, (T)colour.z, T(0)};
         return STEP_DONE;
     }
-    if (sl.flag_r > 0.0f && r2 < sl.flag_r * sl.flag_r) return STEP_FLAG64;
+    if (sl.flag_r > 0.0f && r2 < (T)sl.flag_r * (T)sl.flag_r) return STEP_FLAG64;
     R.l += R.h;
     if (R.accepted >= q.max_steps) {
         result = PRR_RESULT_INFINITE_GEO; colour = {0, 0, 0};
-        u_out = ham_velocity(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
+        u_out = ham_velocity<T>(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
         return STEP_DONE;
     }
     return STEP_CONTINUE;
+}
+
+template <class O, class T>
+__device__ __forceinline__ void ham_write_state(O *o, float uvx, float uvy, int result, T x, T y, T z, const V4<T> &u,
+                                                int accepted)
+{
+    o[0] = (O)uvx; o[1] = (O)uvy; o[2] = (O)result;
+    o[3] = (O)x; o[4] = (O)y; o[5] = (O)z; o[6] = (O)0;
+    o[7] = (O)u.x; o[8] = (O)u.y; o[9] = (O)u.z; o[10] = (O)u.w;
+    o[11] = (O)accepted;
 }
 
 struct HCounts {
@@ -349,7 +371,7 @@ struct HCounts {
 // Split precision: a ray queued for the FP64 pass.  Its colour slot is zeroed
 // here and overwritten by k_fp64_requeue, which counts it as a ray.  Returns
 // true when the slot's pixel is complete.
-__device__ __forceinline__ bool ham_flag(const PersistentArgs &a, HSlot &sl, HCounts &c)
+__device__ __forceinline__ bool ham_flag(const PersistentArgs &a, HSlot<float> &sl, HCounts &c)
 {
     const FrameParams &fp = a.frames[sl.frame];
     c.att += (unsigned)sl.R.i;
@@ -362,7 +384,7 @@ __device__ __forceinline__ bool ham_flag(const PersistentArgs &a, HSlot &sl, HCo
     o[0] = o[1] = o[2] = 0.f;
     sl.s += 1;
     if (sl.s < sl.S) {
-        ham_init<true>(fp, sl, sl.s);
+        ham_init<float, true>(fp, sl, sl.s);
         return false;
     }
     return true;
@@ -371,27 +393,25 @@ __device__ __forceinline__ bool ham_flag(const PersistentArgs &a, HSlot &sl, HCo
 // A finished ray: counters, per-ray outputs, SSAA accumulation (split
 // precision: the per-sample colour), next sample or pixel output.  Returns
 // true when the slot's pixel is complete.
-template <bool SPLIT, bool EMIS>
-__device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, int result, V3<float> col,
-                                           const V4<float> &u, HCounts &c)
+template <class T, bool SPLIT, bool EMIS>
+__device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot<T> &sl, int result, V3<float> col,
+                                           const V4<T> &u, HCounts &c)
 {
     const FrameParams &fp = a.frames[sl.frame];
-    if constexpr (EMIS) col = emis_colour<float>(fp, sl.E, col);
+    if constexpr (EMIS) col = emis_colour<T>(fp, sl.E, col);
     c.att += (unsigned)sl.R.i;
     c.acc += (unsigned)sl.R.accepted;
     c.rays++;
-    const float x = sl.R.P.x, y = sl.R.P.y, z = sl.R.W.x;
-    if (!SPLIT && (a.ray_state || a.sample_rgb || a.ray_steps)) {  // per-ray outputs (single-frame runs)
+    const T x = sl.R.P.x, y = sl.R.P.y, z = sl.R.W.x;
+    if (!SPLIT && (a.ray_state || a.ray_state64 || a.sample_rgb || a.ray_steps)) {  // per-ray outputs (single-frame runs)
         const long long rid = ((long long)sl.py * fp.width + sl.px) * sl.S + sl.s;
         if (a.ray_steps) a.ray_steps[fp.ray_begin + rid] = sl.R.accepted;
-        if (a.ray_state) {
+        if (a.ray_state || a.ray_state64) {
             float uvx, uvy;
             ray_uv(fp, sl.px, sl.py, sl.s, uvx, uvy);
-            float *o = a.ray_state + 12 * rid;
-            o[0] = uvx; o[1] = uvy; o[2] = (float)result;
-            o[3] = x; o[4] = y; o[5] = z; o[6] = 0.0f;  // the coordinate time is not integrated
-            o[7] = u.x; o[8] = u.y; o[9] = u.z; o[10] = u.w;
-            o[11] = (float)sl.R.accepted;
+            // the coordinate time is not integrated: column 6 is 0
+            if (a.ray_state) ham_write_state(a.ray_state + 12 * rid, uvx, uvy, result, x, y, z, u, sl.R.accepted);
+            if (a.ray_state64) ham_write_state(a.ray_state64 + 12 * rid, uvx, uvy, result, x, y, z, u, sl.R.accepted);
         }
         if (a.sample_rgb) {
             float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
@@ -399,7 +419,7 @@ __device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, i
         }
     }
     if (result == PRR_RESULT_SUCCESS) {
-        if (metric_radius<float>(fp, x, y, z) >= sl.q.rout) c.esc++; else c.cap++;
+        if (metric_radius<T>(fp, x, y, z) >= sl.q.rout) c.esc++; else c.cap++;
     } else if (result == PRR_RESULT_INTERSECTION) c.hit++;
     else if (result == PRR_RESULT_INFINITE_GEO) c.inf++;
     else c.nan++;
@@ -409,7 +429,7 @@ __device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, i
         o[0] = col.x; o[1] = col.y; o[2] = col.z;
         sl.s += 1;
         if (sl.s < sl.S) {
-            ham_init<true>(fp, sl, sl.s);
+            ham_init<T, true>(fp, sl, sl.s);
             return false;
         }
         return true;
@@ -423,7 +443,7 @@ __device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, i
     }
     sl.s += 1;
     if (sl.s < sl.S) {
-        ham_init<false, EMIS>(fp, sl, sl.s);
+        ham_init<T, false, EMIS>(fp, sl, sl.s);
         return false;
     }
     float o0 = sl.acc0, o1 = sl.acc1, o2 = sl.acc2;
@@ -434,7 +454,8 @@ __device__ __forceinline__ bool ham_finish(const PersistentArgs &a, HSlot &sl, i
     return true;
 }
 
-template <bool SPLIT, bool EMIS> __device__ __forceinline__ void ham_start(const PersistentArgs &a, HSlot &sl, long long it)
+template <class T, bool SPLIT, bool EMIS>
+__device__ __forceinline__ void ham_start(const PersistentArgs &a, HSlot<T> &sl, long long it)
 {
     sl.frame = find_frame_h(a.frame_pix_begin, a.nframes, it);
     const FrameParams &fp = a.frames[sl.frame];
@@ -444,26 +465,32 @@ template <bool SPLIT, bool EMIS> __device__ __forceinline__ void ham_start(const
     sl.S = fp.samples;
     sl.s = 0;
     sl.acc0 = sl.acc1 = sl.acc2 = 0.f;
-    sl.q = make_hot<float>(fp);
-    sl.flag_r = SPLIT ? fp.fp64_rfac * kerr_r_plus<float>(sl.q.M, sl.q.a) : -1.0f;
-    ham_init<SPLIT, EMIS>(fp, sl, 0);
+    sl.q = make_hot<T>(fp);
+    sl.flag_r = SPLIT ? (float)(fp.fp64_rfac * kerr_r_plus<T>(sl.q.M, sl.q.a)) : -1.0f;
+    ham_init<T, SPLIT, EMIS>(fp, sl, 0);
     sl.busy = true;
 }
 
 }  // namespace
 
-// Resident CTAs per SM the small-CTA instantiation is built for.
+// Resident CTAs per SM the small-CTA (<= 64 threads) instantiations are
+// built for: FP32 8 (128 registers, no spills), FP64 PRR_HAM_SMALL_MINB_F64.
 #ifndef PRR_HAM_SMALL_MINB
 #define PRR_HAM_SMALL_MINB 8
 #endif
+#ifndef PRR_HAM_SMALL_MINB_F64
+#define PRR_HAM_SMALL_MINB_F64 6
+#endif
+template <class T> constexpr int ham_small_minb() { return sizeof(T) == 8 ? PRR_HAM_SMALL_MINB_F64 : PRR_HAM_SMALL_MINB; }
 
-template <int MAXT, int MINB, bool SPLIT, bool EMIS>
+template <class T, int MAXT, int MINB, bool SPLIT, bool EMIS>
 __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
 {
     static_assert(!(SPLIT && EMIS), "emission renders in FP32 or FP64, not split");
+    static_assert(!SPLIT || sizeof(T) == 4, "the split pass is FP32");
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    HSlot sl;
+    HSlot<T> sl;
     HCounts cnt;
     sl.busy = false; sl.need = true; sl.crit = false; sl.flag_r = -1.0f;
     sl.frame = 0; sl.px = sl.py = sl.s = 0; sl.S = 1;
@@ -485,7 +512,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
                 if (sl.need) {
                     const long long it = (long long)base + __popc(m & lt);
                     sl.need = false;
-                    if (it < a.total_pixels) ham_start<SPLIT, EMIS>(a, sl, it);
+                    if (it < a.total_pixels) ham_start<T, SPLIT, EMIS>(a, sl, it);
                     else sl.busy = false;
                 }
             }
@@ -505,24 +532,28 @@ __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
         }
         if (!sl.busy) continue;
         // split precision: a ray near a photon orbit goes to the FP64 pass before its first attempt
-        if (SPLIT && sl.R.i == 0 && sl.crit) {
-            if (ham_flag(a, sl, cnt)) { sl.busy = false; sl.need = true; }
-            continue;
+        if constexpr (SPLIT) {
+            if (sl.R.i == 0 && sl.crit) {
+                if (ham_flag(a, sl, cnt)) { sl.busy = false; sl.need = true; }
+                continue;
+            }
         }
         // the loop bound of trace_RKF (l < 1000, solver.cuh:158) and the attempt counter
-        if (!(sl.R.l < 1000.0f)) {
-            const V4<float> u = ham_velocity(sl.R.P.x, sl.R.P.y, sl.R.W.x, sl.R.Q.x, sl.R.Q.y, sl.R.W.y, sl.c);
-            if (ham_finish<SPLIT, EMIS>(a, sl, PRR_RESULT_INFINITE_GEO, {0.f, 0.f, 0.f}, u, cnt)) { sl.busy = false; sl.need = true; }
+        if (!(sl.R.l < T(1000))) {
+            const V4<T> u = ham_velocity<T>(sl.R.P.x, sl.R.P.y, sl.R.W.x, sl.R.Q.x, sl.R.Q.y, sl.R.W.y, sl.c);
+            if (ham_finish<T, SPLIT, EMIS>(a, sl, PRR_RESULT_INFINITE_GEO, {0.f, 0.f, 0.f}, u, cnt)) { sl.busy = false; sl.need = true; }
             continue;
         }
         sl.R.i += 1;
-        const HamStep st = ham_stages(sl.R, sl.c, sl.q);
+        const HamStep<T> st = ham_stages<T>(sl.R, sl.c, sl.q);
         int result = 0;
         V3<float> col;
-        V4<float> u;
-        const int r = ham_accept<EMIS>(a.frames[sl.frame], sl, sl.R, st, result, col, u);
+        V4<T> u;
+        const int r = ham_accept<T, EMIS>(a.frames[sl.frame], sl, sl.R, st, result, col, u);
         if (r == STEP_CONTINUE) continue;
-        const bool done = (SPLIT && r == STEP_FLAG64) ? ham_flag(a, sl, cnt) : ham_finish<SPLIT, EMIS>(a, sl, result, col, u, cnt);
+        bool done;
+        if constexpr (SPLIT) done = r == STEP_FLAG64 ? ham_flag(a, sl, cnt) : ham_finish<T, SPLIT, EMIS>(a, sl, result, col, u, cnt);
+        else done = ham_finish<T, SPLIT, EMIS>(a, sl, result, col, u, cnt);
         if (done) { sl.busy = false; sl.need = true; }
     }
     warp_sum_add_h(&a.counters[C_ATTEMPTS], cnt.att);
@@ -536,39 +567,46 @@ __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
     if (SPLIT) warp_sum_add_h(&a.counters[C_FP64], cnt.f64);
 }
 
-template <bool SPLIT, bool EMIS> static cudaError_t ham_launch(const PersistentArgs &a, int block, int grid, cudaStream_t st)
+template <class T, bool SPLIT, bool EMIS> static cudaError_t ham_launch(const PersistentArgs &a, int block, int grid, cudaStream_t st)
 {
-    if (block <= 64) k_ham<64, PRR_HAM_SMALL_MINB, SPLIT, EMIS><<<grid, block, 0, st>>>(a);
-    else k_ham<256, 1, SPLIT, EMIS><<<grid, block, 0, st>>>(a);
+    if (block <= 64) k_ham<T, 64, ham_small_minb<T>(), SPLIT, EMIS><<<grid, block, 0, st>>>(a);
+    else k_ham<T, 256, 1, SPLIT, EMIS><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-template <bool SPLIT, bool EMIS> static int ham_occ(int block)
+template <class T, bool SPLIT, bool EMIS> static int ham_occ(int block)
 {
     int n = 0;
-    cudaError_t e = block <= 64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<64, PRR_HAM_SMALL_MINB, SPLIT, EMIS>, block, 0)
-                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<256, 1, SPLIT, EMIS>, block, 0);
+    cudaError_t e = block <= 64
+                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<T, 64, ham_small_minb<T>(), SPLIT, EMIS>, block, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ham<T, 256, 1, SPLIT, EMIS>, block, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
 }
 
-cudaError_t launch_ham(const PersistentArgs &a, bool split, int block, int blocks_per_sm, int nsm, cudaStream_t st)
+cudaError_t launch_ham(const PersistentArgs &a, int precision, bool split, int block, int blocks_per_sm, int nsm,
+                       cudaStream_t st)
 {
     if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
-    if (split && (!a.sample_rgb || !a.fp64_queue)) return cudaErrorInvalidValue;
+    if (split && (precision != PRR_PREC_FP32 || !a.sample_rgb || !a.fp64_queue)) return cudaErrorInvalidValue;
     if (split && a.emission) return cudaErrorInvalidValue;
     int grid = nsm * blocks_per_sm;
     if (grid < 1) grid = 1;
-    if (split) return ham_launch<true, false>(a, block, grid, st);
-    if (a.emission) return ham_launch<false, true>(a, block, grid, st);
-    return ham_launch<false, false>(a, block, grid, st);
+    if (precision == PRR_PREC_FP64) {
+        if (a.emission) return ham_launch<double, false, true>(a, block, grid, st);
+        return ham_launch<double, false, false>(a, block, grid, st);
+    }
+    if (split) return ham_launch<float, true, false>(a, block, grid, st);
+    if (a.emission) return ham_launch<float, false, true>(a, block, grid, st);
+    return ham_launch<float, false, false>(a, block, grid, st);
 }
 
-int ham_occupancy(int block, bool split, bool emission)
+int ham_occupancy(int precision, int block, bool split, bool emission)
 {
-    if (split) return ham_occ<true, false>(block);
-    if (emission) return ham_occ<false, true>(block);
-    return ham_occ<false, false>(block);
+    if (precision == PRR_PREC_FP64) return emission ? ham_occ<double, false, true>(block) : ham_occ<double, false, false>(block);
+    if (split) return ham_occ<float, true, false>(block);
+    if (emission) return ham_occ<float, false, true>(block);
+    return ham_occ<float, false, false>(block);
 }
 
 }  // namespace prr

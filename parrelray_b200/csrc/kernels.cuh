@@ -60,22 +60,24 @@ struct PersistentArgs {
     int emission;                // 1 = some frame has plasma emission (the kernels with emission.cuh)
     int hamiltonian;             // 1 = FP32 one-slot renders integrate (x, p) in Hamiltonian form (k_ham.cu)
 };
-// Dispatches to the kernel of the precision: FP32 with one pixel slot per
-// thread (emission included) and the FP32 pass of SPLIT, with a.hamiltonian
-// -> k_ham (k_ham.cu); other FP32 renders with the register contraction ->
-// k_pair (k_pair.cu, rays_per_thread slots per thread); FP64 and the
-// Christoffel-table variant -> k_persistent.
+// Dispatches to the kernel of the precision: with a.hamiltonian, FP64, FP32
+// with one pixel slot per thread (emission included) and the FP32 pass of
+// SPLIT -> k_ham (k_ham.cu); other FP32 renders with the register
+// contraction -> k_pair (k_pair.cu, rays_per_thread slots per thread); FP64
+// without a.hamiltonian and the Christoffel-table variant -> k_persistent.
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st);
 
 // k_persistent.cu: resident CTAs per SM of the kernel launch_persistent picks.
 int persistent_occupancy(int precision, int geod_table, int block, int rays_per_thread = 1, int emission = 0,
                          int hamiltonian = 0);
 
-// k_ham.cu: the FP32 renderer in Hamiltonian form (one pixel slot per thread);
-// `split`: the FP32 pass of a split-precision render (needs sample_rgb and
-// fp64_queue); a.emission: the instantiation with plasma emission.
-cudaError_t launch_ham(const PersistentArgs &a, bool split, int block, int blocks_per_sm, int nsm, cudaStream_t st);
-int ham_occupancy(int block, bool split = false, bool emission = false);
+// k_ham.cu: the renderer in Hamiltonian form (one pixel slot per thread), in
+// `precision` PRR_PREC_FP32 or PRR_PREC_FP64; `split`: the FP32 pass of a
+// split-precision render (needs sample_rgb and fp64_queue); a.emission: the
+// instantiation with plasma emission.
+cudaError_t launch_ham(const PersistentArgs &a, int precision, bool split, int block, int blocks_per_sm, int nsm,
+                       cudaStream_t st);
+int ham_occupancy(int precision, int block, bool split = false, bool emission = false);
 
 // k_pair.cu: the FP32 renderer with `rpt` pixel slots per thread; `split`:
 // the FP32 pass of a split-precision render (rpt 1; needs sample_rgb and

@@ -116,6 +116,35 @@ template <class V> PRR_DEV Vec4<V> geod(const Vec4<V> &p, const Vec4<V> &u, V Ma
 PRR_DEV float2 f2(float a, float b) { return make_float2(a, b); }
 PRR_DEV float2 sp(float a) { return make_float2(a, a); }
 
+// FP64 lane values and pairs, so code written on (pair, scalar) values
+// builds in both precisions (k_ham.cu); FP64 has no paired instructions, so
+// a double2 operation is two scalar ones.
+PRR_DEV double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
+PRR_DEV double add_(double a, double b) { return __dadd_rn(a, b); }
+PRR_DEV double mul_(double a, double b) { return __dmul_rn(a, b); }
+PRR_DEV double rsq_(double a) { return frsqrt<double>(a); }
+PRR_DEV double rcp_(double a) { return frcp<double>(a); }
+PRR_DEV double abs_(double a) { return fabs(a); }
+PRR_DEV double max_(double a, double b) { return fmax(a, b); }
+PRR_DEV double min_(double a, double b) { return fmin(a, b); }
+PRR_DEV double pow_(double b, double e) { return fpow<double>(b, e); }
+PRR_DEV double neg_(double a) { return -a; }
+PRR_DEV double2 f2(double a, double b) { return make_double2(a, b); }
+PRR_DEV double2 sp(double a) { return make_double2(a, a); }
+PRR_DEV double2 fma_(double2 a, double2 b, double2 c) { return make_double2(__fma_rn(a.x, b.x, c.x), __fma_rn(a.y, b.y, c.y)); }
+PRR_DEV double2 add_(double2 a, double2 b) { return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y)); }
+PRR_DEV double2 mul_(double2 a, double2 b) { return make_double2(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)); }
+PRR_DEV double2 abs_(double2 a) { return make_double2(fabs(a.x), fabs(a.y)); }
+PRR_DEV double2 max_(double2 a, double2 b) { return make_double2(fmax(a.x, b.x), fmax(a.y, b.y)); }
+PRR_DEV double2 rcp_(double2 a) { return make_double2(frcp<double>(a.x), frcp<double>(a.y)); }
+PRR_DEV double2 neg_(double2 a) { return make_double2(-a.x, -a.y); }
+
+// the pair type of a lane type
+template <class T> struct PairOf;
+template <> struct PairOf<float> { using type = float2; };
+template <> struct PairOf<double> { using type = double2; };
+template <class T> using P2 = typename PairOf<T>::type;
+
 // geod<float> with the x and y components of one ray paired: P = (X, Y) and
 // U = (u^x, u^y) in, (du^x, du^y) in gxy and du^z, du^t in gz, gt out.  The
 // operations are geod's, one for one and in its order; where geod applies

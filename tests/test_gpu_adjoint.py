@@ -131,3 +131,26 @@ def test_fp32_forward_adjoint_tracks_the_fp64_one(gpu, small_textures):
     assert np.linalg.norm(g32 - g64) <= 0.02 * np.linalg.norm(g64), (g32, g64)
     big = np.abs(g64) > 0.1 * np.abs(g64).max()
     assert np.all(np.abs(g32[big] - g64[big]) <= 0.05 * np.abs(g64[big])), (g32, g64)
+
+
+def test_sky_weighted_adam_fit_recovers_spin_and_inclination(gpu, small_textures):
+    """The differentiable-render workload's inverse problem at 128x128 (FP32 forward, FP64 adjoint,
+    no sphere): Adam from (a, i) = (0.3, 45 deg) on the L2 loss over the pixels that show sky in both
+    images at least 2 px from the shadow (inverse.sky_weights) reaches the target (0.7, 60 deg)."""
+    from parrelray_b200 import inverse
+
+    tex = dict(small_textures)
+    tex[scenes.SKY_ID] = smooth_sky()
+    gpu.upload_textures(tex)
+
+    def frame_at(q):
+        return scenes.kerr_512_adjoint(spin=float(q[0]), incl_deg=math.degrees(q[1]), precision=abi.PREC_FP32,
+                                       size=128, spheres=[])
+
+    _, tgt, _ = gpu.render(frame_at((0.7, math.radians(60.0))), want_float=True)
+    h = inverse.fit(gpu, frame_at, tgt[0], (0.3, math.radians(45.0)), (0, 2), iters=150, lr=0.01, decay=0.99,
+                    margin=2, lo=(0.0, 0.0), hi=(0.99, math.pi))
+    a, incl = h["q_final"][0], math.degrees(h["q_final"][1])
+    info = (a, incl, [round(x, 2) for x in h["loss"][::15]])
+    assert abs(a - 0.7) < 0.02 and abs(incl - 60.0) < 0.3, info
+    assert h["loss"][-1] < 0.01 * h["loss"][0], info
