@@ -981,16 +981,24 @@ def main():
             ctx.set_option(abi.OPT_GEOD_TABLE, 1)
             table_ms = timed_device()                      # persistent scheduler + Christoffel table
             ctx.set_option(abi.OPT_GEOD_TABLE, -1)
+            ctx.set_option(abi.OPT_HAMILTONIAN, abi.HAM_FP64)
+            contraction_ms = timed_device()                # persistent scheduler + contraction, (x, u) state
+            ctx.set_option(abi.OPT_HAMILTONIAN, abi.HAM_FP32 | abi.HAM_FP64)
             extra["plain"] = {"value": rays / (plain_ms * 1e-3) / 1e6, "ms_per_step": plain_ms,
                               "speedup": plain_ms / ms,
-                              "speedup_scheduler_only": plain_contraction_ms / ms,
+                              "speedup_scheduler_only": plain_contraction_ms / contraction_ms,
                               "speedup_scheduler_only_table": plain_ms / table_ms,
                               "speedup_geodesic_form_only": plain_ms / plain_contraction_ms,
+                              "speedup_hamiltonian_form": contraction_ms / ms,
                               "what": "one ray per thread, 64-row layers, AoS rays in HBM, textbook stages, "
-                                      "Christoffel-table geodesic; speedup = both changes, scheduler_only = the "
-                                      "persistent compaction scheduler with the geodesic form held fixed",
+                                      "Christoffel-table geodesic; speedup = all changes; scheduler_only = the "
+                                      "persistent compaction scheduler with the geodesic form held fixed (contraction, "
+                                      "or table); geodesic_form_only = contraction against table on the plain "
+                                      "schedule; hamiltonian_form = the (x, p) state against the (x, u) contraction "
+                                      "on the persistent schedule",
                               "breakdown_ms": {"plain_table": plain_ms, "plain_contraction": plain_contraction_ms,
-                                               "persistent_table": table_ms, "persistent_contraction": ms}}
+                                               "persistent_table": table_ms, "persistent_contraction": contraction_ms,
+                                               "persistent_hamiltonian": ms}}
         if not args.no_adjoint:
             # discrete adjoint of the 512x512 differentiable-render workload: one gradient of an L2 image loss
             n = args.adjoint_size

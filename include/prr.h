@@ -322,7 +322,10 @@ prr_status prr_trace_rays_f64(prr_ctx *ctx, const prr_frame_desc *frame,
  * gradients.  The rays are visited longest first (ordered by their forward
  * step counts) so rays sharing a warp have similar lengths.
  * stats->kernel_ms is the device time of that ordering plus the adjoint
- * kernel, stats->trace_ms the forward render time. */
+ * kernel, stats->trace_ms the forward render time, stats->accepted the
+ * adjoint's forward steps and stats->n_math_error the rays it dropped (their
+ * checkpoints did not fit max_steps, or a recomputed segment disagreed with
+ * the forward steps; neither happens on valid frames). */
 prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, const float *dL_dimage, int sphere_index,
                        double grads[5], prr_stats *stats);
 
@@ -431,12 +434,17 @@ prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, prr_launch_co
                                      everywhere (A/B runs) */
 #define PRR_OPT_WATCHDOG_CYCLES 2 /* >0: persistent kernels stop after this many SM clock cycles and the
                                      call returns PRR_ERR_TIMEOUT; 0: off (default) */
-#define PRR_OPT_HAMILTONIAN 3     /* FP32 PHYSICAL renders with one pixel per thread and no emission:
-                                     1 (default) integrate (x, p) in Hamiltonian form (p_t conserved, six
-                                     state components); 0: integrate (x, u) with the geodesic contraction.
-                                     Both use the same tableau, error test, caps, hooks and colours; in the
-                                     Hamiltonian form the coordinate time is not integrated, so r.w of
-                                     prr_trace_rays is 0 there */
+#define PRR_OPT_HAMILTONIAN 3     /* which PHYSICAL renders integrate (x, p) in Hamiltonian form (p_t
+                                     conserved, six state components) instead of (x, u) with the geodesic
+                                     contraction: a bit mask of PRR_HAM_FP32 (FP32 renders with one pixel
+                                     per thread, emission frames and the FP32 pass of SPLIT included) and
+                                     PRR_HAM_FP64 (FP64 renders); default both (3), 0 for neither.  Both
+                                     forms use the same tableau, error test (over their own state), caps,
+                                     hooks and colours; in the Hamiltonian form the coordinate time is not
+                                     integrated, so r.w of prr_trace_rays(_f64) is 0 there.  The FP64 pass
+                                     of SPLIT and the adjoint's own stepping use the (x, u) form */
+#define PRR_HAM_FP32 1
+#define PRR_HAM_FP64 2
 prr_status prr_set_option(prr_ctx *ctx, int option, long long value);
 
 /* Measures FP32 and FP64 FMA throughput (TFLOP/s) of the context's device

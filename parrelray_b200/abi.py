@@ -32,6 +32,7 @@ PREC_FP32, PREC_FP64, PREC_SPLIT = 0, 1, 2
 SCHED_PLAIN, SCHED_PERSISTENT = 0, 1
 BG_RMS2X2, BG_BILINEAR = 0, 1
 OPT_GEOD_TABLE, OPT_WATCHDOG_CYCLES, OPT_HAMILTONIAN = 1, 2, 3
+HAM_FP32, HAM_FP64 = 1, 2  # PRR_OPT_HAMILTONIAN mask bits
 EMISSION_NONE, EMISSION_DISK, EMISSION_GRID = 0, 1, 2
 CMAP_AFMHOT, CMAP_GREY = 0, 1
 

@@ -299,7 +299,13 @@ prr_status prr_set_option(prr_ctx *ctx, int option, long long value)
     if (!ctx) return PRR_ERR_INVALID;
     switch (option) {
     case PRR_OPT_GEOD_TABLE: ctx->geod_table = value < 0 ? -1 : (value ? 1 : 0); return PRR_OK;
-    case PRR_OPT_HAMILTONIAN: ctx->hamiltonian = value ? 1 : 0; return PRR_OK;
+    case PRR_OPT_HAMILTONIAN:
+        if (value < 0 || value > (PRR_HAM_FP32 | PRR_HAM_FP64)) {
+            ctx->err = "PRR_OPT_HAMILTONIAN takes a mask of PRR_HAM_FP32 and PRR_HAM_FP64 (0..3)";
+            return PRR_ERR_INVALID;
+        }
+        ctx->hamiltonian = (int)value;
+        return PRR_OK;
     case PRR_OPT_WATCHDOG_CYCLES: ctx->watchdog_cycles = value > 0 ? value : 0; return PRR_OK;
     default: fail(ctx, "prr_set_option: unknown option"); return PRR_ERR_INVALID;
     }

@@ -216,6 +216,19 @@ template <class TF> __device__ __forceinline__ void state8(const PhysRay<TF> &R,
     y[4] = (double)R.u.x; y[5] = (double)R.u.y; y[6] = (double)R.u.z; y[7] = (double)R.u.w;
 }
 
+// One RKF45 attempt of the adjoint's own forward steps.  The forward pass and
+// both recompute passes go through this one out-of-line copy, so a recomputed
+// segment repeats the forward steps bit for bit: inlined copies of the same
+// source may contract multiply-adds differently, and a recomputed step
+// sequence that drifts from the forward one would pull lambda back through
+// steps that were never taken.
+template <class TF>
+__device__ __noinline__ int adj_attempt(const FrameParams &fp, const Hot<TF> &q, PhysRay<TF> &R, int &result,
+                                        V3<float> &col, int &hit)
+{
+    return phys_attempt<TF, 0>(fp, q, R, result, col, (TF)-1, &hit);
+}
+
 template <class TF> __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoint(AdjointArgs A)
 {
     const FrameParams &fp = *A.frame;
@@ -254,7 +267,7 @@ template <class TF> __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoi
         bool ok = true;
         while (true) {
             int before = R.accepted;
-            int st = phys_attempt<TF, 0>(fp, qf, R, result, col, (TF)-1, &hit);
+            int st = adj_attempt<TF>(fp, qf, R, result, col, hit);
             if (st == STEP_CONTINUE && R.accepted > before && R.accepted % ADJ_K == 0) {
                 int slot = R.accepted / ADJ_K;
                 if (slot >= A.max_ckpt) { ok = false; break; }
@@ -282,7 +295,7 @@ template <class TF> __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoi
         }
         if (!any) continue;
         // lambda_N = gc . dc/dy_N ; direct phase term
-        double lam[8] = {0, 0, 0, 0, 0, 0, 0, 0}, th[2] = {0, 0};
+        double lam[8] = {0, 0, 0, 0, 0, 0, 0, 0}, th[2] = {0, 0}, phase_c = 0.0;
         {
             DC st[8];
             double yN[8];
@@ -311,24 +324,29 @@ template <class TF> __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoi
             const DC *cc3 = &cd.x;
             for (int c = 0; c < 3; c++) {
                 for (int j = 0; j < 8; j++) lam[j] += gc[c] * cc3[c].d[j];
-                gacc[P_PHASE] += gc[c] * cc3[c].d[8 + P_PHASE];
+                phase_c += gc[c] * cc3[c].d[8 + P_PHASE];
             }
         }
-        // reverse sweep, segment by segment, each in two recompute passes
+        // reverse sweep, segment by segment, each in two recompute passes.  A
+        // recomputation that does not reach the steps the forward pass took
+        // (it cannot, as both run the same code, but it is checked rather than
+        // trusted) drops the ray: its states would be missing.
         int r2 = 0, h2 = -1;
         V3<float> c2;
-        for (int seg = (N - 1) / ADJ_K; seg >= 0 && N > 0; seg--) {
+        bool consistent = true;
+        for (int seg = (N - 1) / ADJ_K; seg >= 0 && N > 0 && consistent; seg--) {
             const int lo = seg * ADJ_K, hi = min(N, lo + ADJ_K);
             const int nsub = (hi - lo + ADJ_SUB - 1) / ADJ_SUB;
             // pass 1: the segment's sub-checkpoints
             PhysRay<TF> Rs = ck[seg];
             sub[0] = Rs;
             while (Rs.accepted < lo + (nsub - 1) * ADJ_SUB) {
-                int st = phys_attempt<TF, 0>(fp, qf, Rs, r2, c2, (TF)-1, &h2);
+                int st = adj_attempt<TF>(fp, qf, Rs, r2, c2, h2);
                 const int j = (Rs.accepted - lo) / ADJ_SUB;
                 if ((Rs.accepted - lo) % ADJ_SUB == 0 && j < nsub) sub[j] = Rs;
                 if (st != STEP_CONTINUE) break;
             }
+            if (Rs.accepted < lo + (nsub - 1) * ADJ_SUB) { consistent = false; break; }
             // pass 2: each sub-segment, last first: keep its states, then pull lambda back
             for (int j = nsub - 1; j >= 0; j--) {
                 Rs = sub[j];
@@ -337,7 +355,7 @@ template <class TF> __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoi
                     const int before = Rs.accepted;
                     TF yb[8] = {Rs.x.x, Rs.x.y, Rs.x.z, Rs.x.w, Rs.u.x, Rs.u.y, Rs.u.z, Rs.u.w};
                     const TF hb = Rs.h;
-                    int st = phys_attempt<TF, 0>(fp, qf, Rs, r2, c2, (TF)-1, &h2);
+                    int st = adj_attempt<TF>(fp, qf, Rs, r2, c2, h2);
                     if (Rs.accepted > before) {
                         const int slot = before - slo;
                         for (int c = 0; c < 8; c++) ystore[slot][c] = yb[c];
@@ -345,6 +363,7 @@ template <class TF> __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoi
                     }
                     if (st != STEP_CONTINUE) break;
                 }
+                if (Rs.accepted != shi) { consistent = false; break; }
                 for (int n = shi - 1; n >= slo; n--) {
                     double y[8];
                     for (int c = 0; c < 8; c++) y[c] = (double)ystore[n - slo][c];
@@ -352,6 +371,8 @@ template <class TF> __global__ void __launch_bounds__(128, PRR_ADJ_MINB) k_adjoi
                 }
             }
         }
+        if (!consistent) { n_bad++; continue; }
+        gacc[P_PHASE] += phase_c;
         gacc[P_SPIN] += th[0];
         gacc[P_MASS] += th[1];
         for (int c = 0; c < 8; c++)

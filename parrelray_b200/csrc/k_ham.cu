@@ -99,30 +99,32 @@ PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP,
     const T q = add_(r2, c.a2), iq = rcp_(q);
     const T Sig = fma_(r2, r2, mul_(c.a2, Z2)), iSig = rcp_(Sig);
     const V iq_ = sp(iq);
-    // gradients of r and f
+    // gradients of r and of f/2 (the 1/2 of 1/2 Lam^2 grad f folded in)
     const V dr = mul_(P, sp(mul_(r, iS)));
     const T drz = mul_(mul_(z, q), mul_(iS, ir));
     const T r3 = mul_(r2, r);
-    const T f = mul_(mul_(c.M2, r3), iSig);
-    const T c1 = mul_(f, fma_(mul_(T(-4), r3), iSig, mul_(T(3), ir)));
-    const V df = mul_(sp(c1), dr);
-    const T dfz = fma_(c1, drz, mul_(mul_(T(-2), f), mul_(c.a2, mul_(z, iSig))));
+    const T t = mul_(r3, iSig);
+    const T f = mul_(c.M2, t);
+    const T c1h = mul_(f, fma_(T(-2), t, mul_(T(1.5), ir)));
+    const V dfh = mul_(sp(c1h), dr);
+    const T dfzh = fma_(c1h, drz, mul_(mul_(f, iSig), mul_(neg_(c.a2), z)));
     // l and Lam = l.p - p_t
     const V l = mul_(fma_(sp(r), P, f2(mul_(c.a, Y), neg_(mul_(c.a, X)))), iq_);
     const T lz = mul_(z, ir);
     const T px = Q.x, py = Q.y;
-    const T Lam = fma_(l.x, px, fma_(l.y, py, fma_(lz, pz, neg_(c.pt))));
+    const T lpxy = fma_(px, l.x, mul_(py, l.y));
+    const T Lam = fma_(lz, pz, add_(lpxy, neg_(c.pt)));
     // gradient of l.p at fixed p
-    const T P0 = fma_(mul_(T(-2), r), fma_(px, l.x, mul_(py, l.y)), fma_(px, X, mul_(py, Y)));
+    const T P0 = fma_(mul_(T(-2), r), lpxy, fma_(px, X, mul_(py, Y)));
     const T Pp = fma_(P0, iq, neg_(mul_(pz, mul_(lz, ir))));
     const V dL = fma_(dr, sp(Pp), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
     const T dLz = fma_(drz, Pp, mul_(pz, ir));
     // Hamilton's equations
     const T fL = mul_(f, Lam);
-    const T hL2 = mul_(mul_(T(0.5), Lam), Lam);
-    dQ = fma_(sp(hL2), df, mul_(sp(fL), dL));
+    const T L2 = mul_(Lam, Lam);
+    dQ = fma_(sp(L2), dfh, mul_(sp(fL), dL));
     dP = fma_(sp(neg_(fL)), l, Q);
-    dW = f2(fma_(neg_(fL), lz, pz), fma_(hL2, dfz, mul_(fL, dLz)));
+    dW = f2(fma_(neg_(fL), lz, pz), fma_(L2, dfzh, mul_(fL, dLz)));
 }
 
 // u = dx/dlambda (spatial) and u^t = -p_t + f Lam at (x, p), with IEEE
@@ -293,7 +295,9 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const 
     T dH = T(1e11), dN = T(1e11), dT = T(1e11);
     T vx = 0, vy = 0, vz = 0, v2 = 0;
     bool near = false;
-    for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn, yn, zn);
+    const T R2 = xn * xn + yn * yn + zn * zn;
+    if (R2 >= (T)fp.sph_lo2 && R2 <= (T)fp.sph_hi2)
+        for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn, yn, zn);
     if (near) {
         const V4<T> un = ham_velocity<T>(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
         const T k = frsqrt<T>(un.x * un.x + un.y * un.y + un.z * un.z);
@@ -325,7 +329,7 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const 
         candE = candT; dE = dT;
     }
     // User_ENDLOOP, on the squared radius
-    T r2 = xn * xn + yn * yn + zn * zn;
+    T r2 = R2;
     if (q.metric == PRR_METRIC_KERR) {
         const T b = r2 - q.a * q.a;
         const T S2 = b * b + T(4) * q.a * q.a * zn * zn;
@@ -474,12 +478,15 @@ __device__ __forceinline__ void ham_start(const PersistentArgs &a, HSlot<T> &sl,
 }  // namespace
 
 // Resident CTAs per SM the small-CTA (<= 64 threads) instantiations are
-// built for: FP32 8 (128 registers, no spills), FP64 PRR_HAM_SMALL_MINB_F64.
+// built for: FP32 8 (128 registers, no spills); FP64 8 as well (128
+// registers, 458 bytes of spills that stay in L1): the FP64 form is latency
+// bound, and on the 1080p frame 8 CTAs measured 871 ms, 6 (168 registers)
+// 922 ms, 4 (192 registers, no spills) 1100 ms.
 #ifndef PRR_HAM_SMALL_MINB
 #define PRR_HAM_SMALL_MINB 8
 #endif
 #ifndef PRR_HAM_SMALL_MINB_F64
-#define PRR_HAM_SMALL_MINB_F64 6
+#define PRR_HAM_SMALL_MINB_F64 8
 #endif
 template <class T> constexpr int ham_small_minb() { return sizeof(T) == 8 ? PRR_HAM_SMALL_MINB_F64 : PRR_HAM_SMALL_MINB; }
 

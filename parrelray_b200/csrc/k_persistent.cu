@@ -267,19 +267,20 @@ cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block,
 {
     if (block < 32 || block > 256 || block % 32) return cudaErrorInvalidValue;
     if (precision == PRR_PREC_FP64) {
-        if (a.hamiltonian) return launch_ham(a, PRR_PREC_FP64, false, block, blocks_per_sm, nsm, st);
+        if (a.hamiltonian & PRR_HAM_FP64) return launch_ham(a, PRR_PREC_FP64, false, block, blocks_per_sm, nsm, st);
         if (a.emission) return launch_one<double, 0, true>(a, block, blocks_per_sm, nsm, st);
         return launch_one<double, 0, false>(a, block, blocks_per_sm, nsm, st);
     }
     if (precision == PRR_PREC_SPLIT) {
-        if (a.hamiltonian) return launch_ham(a, PRR_PREC_FP32, true, block, blocks_per_sm, nsm, st);
+        if (a.hamiltonian & PRR_HAM_FP32) return launch_ham(a, PRR_PREC_FP32, true, block, blocks_per_sm, nsm, st);
         return launch_pair(a, 1, true, block, blocks_per_sm, nsm, st);
     }
     if (a.geod_table) {
         if (a.emission) return cudaErrorInvalidValue;  // emission runs with the register contraction
         return launch_one<float, 1, false>(a, block, blocks_per_sm, nsm, st);
     }
-    if (a.hamiltonian && (a.rays_per_thread != 2 || a.emission)) return launch_ham(a, PRR_PREC_FP32, false, block, blocks_per_sm, nsm, st);
+    if ((a.hamiltonian & PRR_HAM_FP32) && (a.rays_per_thread != 2 || a.emission))
+        return launch_ham(a, PRR_PREC_FP32, false, block, blocks_per_sm, nsm, st);
     return launch_pair(a, a.rays_per_thread == 2 ? 2 : 1, false, block, blocks_per_sm, nsm, st);
 }
 
@@ -287,11 +288,13 @@ int persistent_occupancy(int precision, int geod_table, int block, int rays_per_
 {
     int n = 0;
     cudaError_t e;
-    if (precision == PRR_PREC_FP64 && hamiltonian) return ham_occupancy(PRR_PREC_FP64, block, false, emission != 0);
+    if (precision == PRR_PREC_FP64 && (hamiltonian & PRR_HAM_FP64)) return ham_occupancy(PRR_PREC_FP64, block, false, emission != 0);
     if (precision == PRR_PREC_FP64) e = emission ? occupancy_one<double, 0, true>(&n, block) : occupancy_one<double, 0, false>(&n, block);
-    else if (precision == PRR_PREC_SPLIT) return hamiltonian ? ham_occupancy(PRR_PREC_FP32, block, true) : pair_occupancy(1, true, block);
+    else if (precision == PRR_PREC_SPLIT)
+        return (hamiltonian & PRR_HAM_FP32) ? ham_occupancy(PRR_PREC_FP32, block, true) : pair_occupancy(1, true, block);
     else if (geod_table) e = occupancy_one<float, 1, false>(&n, block);
-    else if (hamiltonian && (rays_per_thread != 2 || emission)) return ham_occupancy(PRR_PREC_FP32, block, false, emission != 0);
+    else if ((hamiltonian & PRR_HAM_FP32) && (rays_per_thread != 2 || emission))
+        return ham_occupancy(PRR_PREC_FP32, block, false, emission != 0);
     else return pair_occupancy(rays_per_thread == 2 ? 2 : 1, false, block, emission != 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;

@@ -58,13 +58,14 @@ struct PersistentArgs {
     int rays_per_thread;         // FP32: pixel slots in flight per thread (1 or 2; 0 = 1)
     int *ray_steps;              // optional: accepted steps per ray (not k_pair; single frame)
     int emission;                // 1 = some frame has plasma emission (the kernels with emission.cuh)
-    int hamiltonian;             // 1 = FP32 one-slot renders integrate (x, p) in Hamiltonian form (k_ham.cu)
+    int hamiltonian;             // PRR_HAM_FP32 | PRR_HAM_FP64 mask: renders that integrate (x, p) in Hamiltonian form (k_ham.cu)
 };
-// Dispatches to the kernel of the precision: with a.hamiltonian, FP64, FP32
-// with one pixel slot per thread (emission included) and the FP32 pass of
-// SPLIT -> k_ham (k_ham.cu); other FP32 renders with the register
-// contraction -> k_pair (k_pair.cu, rays_per_thread slots per thread); FP64
-// without a.hamiltonian and the Christoffel-table variant -> k_persistent.
+// Dispatches to the kernel of the precision: FP32 with one pixel slot per
+// thread (emission included) and the FP32 pass of SPLIT with PRR_HAM_FP32 in
+// a.hamiltonian, and FP64 with PRR_HAM_FP64 -> k_ham (k_ham.cu); other FP32
+// renders with the register contraction -> k_pair (k_pair.cu,
+// rays_per_thread slots per thread); other FP64 renders and the
+// Christoffel-table variant -> k_persistent.
 cudaError_t launch_persistent(const PersistentArgs &a, int precision, int block, int blocks_per_sm, int nsm, cudaStream_t st);
 
 // k_persistent.cu: resident CTAs per SM of the kernel launch_persistent picks.

@@ -171,7 +171,7 @@ extern "C" prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, co
     a.rgb8 = d_rgb8;
     a.counters = (unsigned long long *)base;
     a.emission = plan.any_emission;
-    a.hamiltonian = 1;
+    a.hamiltonian = PRR_HAM_FP32 | PRR_HAM_FP64;  // a context's default
     // the launch shape prr_autotune picks for the 1080p Kerr workload: CTAs of
     // 64 threads at their occupancy limit, one pixel per thread, a warp refill
     // every 64 attempts

@@ -310,7 +310,9 @@ PRR_DEV int phys_accept(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, c
     T dH = (T)1e11, dN = (T)1e11, dT = (T)1e11;
     T vx = 0, vy = 0, vz = 0, v2 = 0;
     bool near = false;
-    for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn.x, xn.y, xn.z);
+    const T R2 = xn.x * xn.x + xn.y * xn.y + xn.z * xn.z;
+    if (R2 >= (T)fp.sph_lo2 && R2 <= (T)fp.sph_hi2)
+        for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn.x, xn.y, xn.z);
     if (near) {
         T k = frsqrt<T>(un.x * un.x + un.y * un.y + un.z * un.z);
         vx = un.x * k; vy = un.y * k; vz = un.z * k;
@@ -341,7 +343,7 @@ PRR_DEV int phys_accept(const FrameParams &fp, const Hot<T> &q, PhysRay<T> &R, c
         candE = candT; dE = dT;
     }
     // User_ENDLOOP, on the squared radius (one square root for Kerr, none otherwise)
-    T r2 = xn.x * xn.x + xn.y * xn.y + xn.z * xn.z;
+    T r2 = R2;
     if (q.metric == PRR_METRIC_KERR) {
         T b = r2 - q.a * q.a;
         T S2 = b * b + (T)4 * q.a * q.a * xn.z * xn.z;

@@ -29,19 +29,26 @@ template <class T> struct V3 { T x, y, z; };
 template <class T> struct V4 { T x, y, z, w; };
 
 // Reciprocal, reciprocal square root and power for the PHYSICAL-mode hot
-// loop.  FP32 uses the SFU approximations (rcp.approx / rsqrt.approx /
-// lg2+ex2: a few ulp, far below the 1e-6 integration tolerance) instead of
-// the IEEE-rounded multi-instruction sequences.  FP64 uses the correctly
+// loop.  FP32 issues the SFU approximations directly (PTX rcp.approx.ftz,
+// rsqrt.approx.ftz, lg2.approx.ftz and ex2.approx.ftz: relative errors of
+// about 2^-23, far below the 1e-6 integration tolerance), with subnormal
+// inputs and results flushed to zero, so no range or subnormal fix-up
+// instructions surround them; the arguments on this path (squared radii,
+// norms, error ratios) are normal numbers or 0.  FP64 uses the correctly
 // rounded reciprocal (no general division) and CUDA's double rsqrt (within
 // an ulp) in place of a square root followed by a division.
+PRR_DEV float sfu_rcp(float v) { float r; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v)); return r; }
+PRR_DEV float sfu_rsqrt(float v) { float r; asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v)); return r; }
+PRR_DEV float sfu_lg2(float v) { float r; asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v)); return r; }
+PRR_DEV float sfu_ex2(float v) { float r; asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v)); return r; }
 template <class T> PRR_DEV T frcp(T v) { return (T)1 / v; }
-template <> PRR_DEV float frcp<float>(float v) { return __fdividef(1.0f, v); }
+template <> PRR_DEV float frcp<float>(float v) { return sfu_rcp(v); }
 template <> PRR_DEV double frcp<double>(double v) { return __drcp_rn(v); }
 template <class T> PRR_DEV T frsqrt(T v) { return (T)1 / sqrt(v); }
-template <> PRR_DEV float frsqrt<float>(float v) { return rsqrtf(v); }
+template <> PRR_DEV float frsqrt<float>(float v) { return sfu_rsqrt(v); }
 template <> PRR_DEV double frsqrt<double>(double v) { return rsqrt(v); }
 template <class T> PRR_DEV T fpow(T b, T e) { return pow(b, e); }
-template <> PRR_DEV float fpow<float>(float b, float e) { return exp2f(e * __log2f(b)); }
+template <> PRR_DEV float fpow<float>(float b, float e) { return sfu_ex2(e * sfu_lg2(b)); }
 
 template <class T> PRR_HD V4<T> v4add(const V4<T> &a, const V4<T> &b) { return {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
 // f4 scaled by t; the reference's operator*(float, f4) multiplies each
@@ -131,6 +138,9 @@ struct FrameParams {
     DevTex bg;      // bg.p == nullptr: black sky
     float fp64_delta, fp64_rfac;
     int nspheres;
+    // every sphere is far (sphere_far) from a point p with |p|^2 outside
+    // [sph_lo2, sph_hi2] (Euclidean |p|; empty when there are no spheres)
+    float sph_lo2, sph_hi2;
     int camera;           // prr_camera
     unsigned ssaa_seed;   // RANDOM / JITTERED offsets
     float cfwd[3], cright[3], cup[3];  // Camera::computeVectors basis (PINHOLE, PANORAMA)

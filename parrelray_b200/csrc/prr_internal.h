@@ -54,7 +54,7 @@ struct prr_ctx {
     int schedule = PRR_SCHED_PERSISTENT;
     prr_launch_config cfg{};
     int geod_table = -1;  // -1: per schedule (PERSISTENT contraction, PLAIN table); 0: contraction; 1: table
-    int hamiltonian = 1;  // FP32 one-slot renders in Hamiltonian form (PRR_OPT_HAMILTONIAN)
+    int hamiltonian = PRR_HAM_FP32 | PRR_HAM_FP64;  // renders in Hamiltonian form (PRR_OPT_HAMILTONIAN)
     long long watchdog_cycles = 0;
     std::vector<MetricPlugin> plugins;
     int *ray_steps_out = nullptr;  // set by prr_adjoint around its forward render: per-ray accepted steps

@@ -199,6 +199,27 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
             float far2 = (float)((reach * reach + (double)S.radius * S.radius) * 1.01 + 1e-3);
             p.sph[s] = {S.center[0], S.center[1], S.center[2], S.radius, dev_tex(ctx, S.texture_id), far2};
         }
+        // the shell that holds every sphere's far radius: |p - c| >= | |p| - |c| |, so a point
+        // with |p| > |c| + sqrt(far2) or |p| < |c| - sqrt(far2) is far from that sphere (the bounds
+        // widened by 1e-4 relative and absolute against rounding)
+        {
+            double lo = INFINITY, hi = -1.0;
+            for (int s = 0; s < d.nspheres; s++) {
+                const DevSphere &S = p.sph[s];
+                const double c = std::sqrt((double)S.cx * S.cx + (double)S.cy * S.cy + (double)S.cz * S.cz);
+                const double fr = std::sqrt((double)S.far2);
+                hi = std::max(hi, c + fr);
+                lo = std::min(lo, c - fr);
+            }
+            if (d.nspheres == 0) {
+                p.sph_lo2 = 1.0f; p.sph_hi2 = 0.0f;
+            } else {
+                hi = hi * (1.0 + 1e-4) + 1e-4;
+                lo = lo * (1.0 - 1e-4) - 1e-4;
+                p.sph_hi2 = (float)(hi * hi);
+                p.sph_lo2 = lo > 0.0 ? (float)(lo * lo) : -1.0f;
+            }
+        }
         p.width = d.width; p.height = d.height; p.samples = d.samples; p.ssaa = d.ssaa;
         p.vfov = d.vfov; p.cam[0] = d.cam_pos[0]; p.cam[1] = d.cam_pos[1]; p.cam[2] = d.cam_pos[2];
         p.alpha = d.cam_alpha; p.beta = d.cam_beta;
@@ -602,7 +623,7 @@ extern "C" prr_status prr_adjoint(prr_ctx *ctx, const prr_frame_desc *frame, con
         memset(stats, 0, sizeof(*stats));
         stats->rays = nrays;
         stats->accepted = (int64_t)c[C_ACCEPTED];
-        stats->n_math_error = (int64_t)c[C_MATH_ERROR];  // rays whose checkpoints did not fit
+        stats->n_math_error = (int64_t)c[C_MATH_ERROR];  // rays dropped: checkpoints did not fit, or a recomputation disagreed
         stats->kernel_ms = adj_ms;
         stats->trace_ms = forward_ms;
         stats->kernel_launches = ctx->last_launches + 2;  // + the ray-order iota and the adjoint (the radix sort's own kernels not counted)

@@ -1,3 +1,4 @@
+import contextlib
 import os
 import sys
 from pathlib import Path
@@ -61,6 +62,19 @@ def gpu(built):
     ctx = Context(0)
     yield ctx
     ctx.close()
+
+
+@contextlib.contextmanager
+def hamiltonian_forms(ctx, mask: int):
+    """Sets PRR_OPT_HAMILTONIAN on a (session-wide) context for a block and
+    restores the default (both precisions in Hamiltonian form) after it."""
+    from parrelray_b200 import abi
+
+    ctx.set_option(abi.OPT_HAMILTONIAN, mask)
+    try:
+        yield ctx
+    finally:
+        ctx.set_option(abi.OPT_HAMILTONIAN, abi.HAM_FP32 | abi.HAM_FP64)
 
 
 def pixel_rule(a8: np.ndarray, b8: np.ndarray) -> float:

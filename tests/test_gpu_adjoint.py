@@ -154,3 +154,25 @@ def test_sky_weighted_adam_fit_recovers_spin_and_inclination(gpu, small_textures
     info = (a, incl, [round(x, 2) for x in h["loss"][::15]])
     assert abs(a - 0.7) < 0.02 and abs(incl - 60.0) < 0.3, info
     assert h["loss"][-1] < 0.01 * h["loss"][0], info
+
+
+def test_adjoint_does_not_depend_on_earlier_calls(gpu, small_textures):
+    """The adjoint's recomputed segments repeat its forward steps exactly (one out-of-line step
+    function), so no ray is dropped as inconsistent, and an FP32-forward gradient is the same
+    whether the previous call was an FP64-forward adjoint (whose checkpoints and stack are laid out
+    differently) or nothing: nothing is read that the call did not write."""
+    tex = dict(small_textures)
+    tex[scenes.SKY_ID] = smooth_sky()
+    gpu.upload_textures(tex)
+    kw = dict(size=64, spin=0.3, incl_deg=45.0, spheres=[])
+    _, tgt, _ = gpu.render(scenes.kerr_512_adjoint(spin=0.7, incl_deg=60.0, size=64, spheres=[]), want_float=True)
+    d32 = scenes.kerr_512_adjoint(precision=abi.PREC_FP32, **kw)
+    _, cur, _ = gpu.render(d32, want_float=True)
+    dl = 2.0 * (cur[0] - tgt[0])
+    g1, s1 = gpu.adjoint(d32, dl)
+    g64, s64 = gpu.adjoint(scenes.kerr_512_adjoint(precision=abi.PREC_FP64, **kw), dl)
+    g2, s2 = gpu.adjoint(d32, dl)
+    for s in (s1, s64, s2):
+        assert s.n_math_error == 0 and s.accepted > 0
+    assert np.allclose(g1, g2, rtol=1e-9, atol=1e-9), (g1, g2)
+    assert np.all(np.isfinite(g64)) and np.linalg.norm(g1 - g64) <= 0.05 * np.linalg.norm(g64), (g1, g64)

@@ -11,7 +11,7 @@
 import numpy as np
 import pytest
 
-from conftest import pixel_rule, quantize
+from conftest import hamiltonian_forms, pixel_rule, quantize
 from parrelray_b200 import abi, scenes
 
 pytestmark = pytest.mark.gpu
@@ -39,23 +39,40 @@ def escape_dirs(st):
     return u / np.linalg.norm(u, axis=1, keepdims=True)
 
 
-def test_fp64_gpu_matches_fp64_oracle(gpu, small_textures, kerr_oracle_fp64):
+@pytest.mark.parametrize("form", ["contraction", "hamiltonian"])
+def test_fp64_gpu_matches_fp64_oracle(gpu, small_textures, kerr_oracle_fp64, form):
     """Outcome, escape direction (the observable the background lookup uses)
     and hit colour.  The final POSITION is not compared: the last step
-    overshoots r = rout by up to one step, so it depends on the step sequence."""
+    overshoots r = rout by up to one step, so it depends on the step sequence.
+    The oracle integrates (x, u); the FP64 renderer in the same form takes the
+    same steps, so the two agree to 1e-6 rad.  In Hamiltonian form the error
+    test runs over (x, p), so the step sequence differs and the two agree to
+    the integration's truncation error (1e-5 rad at tolerance 1e-6)."""
     d, st, rgb, _ = kerr_oracle_fp64
     gpu.upload_textures(small_textures)
-    gs, grgb, stats = gpu.trace_rays_f64(d)
+    mask = abi.HAM_FP32 | (abi.HAM_FP64 if form == "hamiltonian" else 0)
+    with hamiltonian_forms(gpu, mask):
+        gs, grgb, stats = gpu.trace_rays_f64(d)
     same = gs[:, 2] == st[:, 2]
     assert same.mean() >= 0.999
     esc = same & (st[:, 2] == abi.RESULT_SUCCESS) & (np.linalg.norm(st[:, 3:6], axis=1) >= d.rout)
     assert esc.sum() > 0.5 * len(st)
+    if form == "hamiltonian":
+        # different step sequences: rays within +-2% of the critical curve amplify the truncation
+        # error without bound, so they are compared by outcome and colour only
+        from oracles import kerr_criticality
+
+        esc &= kerr_criticality(st, d.mass, d.spin) >= 2 * 0.02
     # |a x b| resolves small angles (arccos of the dot product bottoms out at 1.5e-8)
     ang = np.linalg.norm(np.cross(escape_dirs(gs[esc]), escape_dirs(st[esc])), axis=1)
-    # a background texel spans 3e-3 rad; 1e-6 is the FP64 agreement bar
-    assert np.mean(ang < 1e-6) >= 0.99, np.percentile(ang, [50, 99, 99.9])
+    # a background texel spans 3e-3 rad
+    bar = 1e-6 if form == "contraction" else 1e-5
+    assert np.mean(ang < bar) >= 0.99, np.percentile(ang, [50, 99, 99.9])
     assert np.mean(ang < 1e-4) >= 0.999, np.percentile(ang, [50, 99, 99.9])
     assert np.mean(np.abs(grgb[same] - rgb[same]).max(axis=1) <= 1 / 255) >= 0.995
+    if form == "hamiltonian":
+        assert np.all(gs[:, 6] == 0.0)  # the coordinate time is not integrated in this form
+        return
     # same step count -> the whole state agrees.  Both sides form the initial
     # direction in FP32 as the reference does (Camera::rayDir_Spherical), and
     # CUDA's cosf/sinf may differ from glibc's by one ulp, so FP64 trajectories
@@ -141,7 +158,8 @@ def test_camera_models_and_stochastic_ssaa(gpu, oracle, small_textures, camera, 
     d = kerr_frame(W=40, H=24, S=S, precision=abi.PREC_FP64, fxaa=False)
     d.camera, d.ssaa, d.ssaa_seed = camera, ssaa, 1234
     gpu.upload_textures(small_textures)
-    gs, _, _ = gpu.trace_rays_f64(d)
+    with hamiltonian_forms(gpu, abi.HAM_FP32):  # FP64 in the oracle's (x, u) form: the same steps
+        gs, _, _ = gpu.trace_rays_f64(d)
     st, _ = oracle.trace(d, small_textures, precision=1)
     assert np.array_equal(gs[:, :2].astype(np.float32), st[:, :2].astype(np.float32))
     same = gs[:, 2] == st[:, 2]
@@ -165,11 +183,8 @@ def test_hamiltonian_and_contraction_forms_agree(gpu, small_textures, kerr_oracl
     d = kerr_frame()
     gpu.upload_textures(small_textures)
     a, _, sa = gpu.render(d)
-    gpu.set_option(abi.OPT_HAMILTONIAN, 0)
-    try:
+    with hamiltonian_forms(gpu, 0):
         b, _, sb = gpu.render(d)
-    finally:
-        gpu.set_option(abi.OPT_HAMILTONIAN, 1)
     assert pixel_rule(a[0], b[0]) >= 0.999
     for img in (a[0], b[0]):
         assert pixel_rule(img, quantize(ref_img)) >= 0.999 - 1.0 / (d.width * d.height)
