@@ -74,12 +74,12 @@ F_ATTEMPT = 6 * FLOPS_GEOD_KERR + FLOPS_STAGES
 # the 960x540 copy of the headline frame (one launch, 64-thread CTAs at 8 per SM, refill every 64
 # attempts): FFMA x 2 FLOP, paired FFMA2 x 4 (two FMAs per thread instruction), FMUL/FADD x 1, paired
 # FMUL2/FADD2 x 2, summed and divided by the launch's attempt counter.  k_ham (the Hamiltonian form)
-# executes 1,055 FLOP per attempt; k_pair (the (x, u) contraction, the form F_ATTEMPT counts) 1,532.
-NCU_FLOP_PER_ATTEMPT = {"k_ham": 1055.0, "k_pair": 1532.0}
+# executes 967 FLOP per attempt; k_pair (the (x, u) contraction, the form F_ATTEMPT counts) 1,459.
+NCU_FLOP_PER_ATTEMPT = {"k_ham": 967.0, "k_pair": 1459.0}
 NCU_FLOP_RULE = ("FP32 FLOP executed, from ncu sass_thread_inst_executed_op_{ffma,fmul,fadd}{,2}: FFMA 2, FFMA2 4, "
                  "FMUL/FADD 1, FMUL2/FADD2 2, per attempt")
 # DRAM bytes of one launch of the tracing kernel (ncu, 960x540 copy of the headline frame)
-TRAFFIC_PER_LAUNCH = 8.76544e6
+TRAFFIC_PER_LAUNCH = 9.249792e6
 
 
 def reserve_stdout():
@@ -828,6 +828,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--plain-stride", type=int, default=1,
                     help="trajectory: render every n-th frame with the plain schedule (1: all 240)")
+    ap.add_argument("--form", default="hamiltonian", choices=["hamiltonian", "contraction"],
+                    help="profiling variant: the geodesic form of the timed frame (default: the product's)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
+                    help="profiling variant: the arithmetic of the timed frame (default: the workload's FP32)")
     ap.add_argument("--launch", default=None,
                     help="block,blocks_per_sm,compaction_interval,rays_per_thread for the persistent renderer "
                          "(default: prr_autotune on the frame, outside the timed region)")
@@ -859,6 +863,16 @@ def main():
     tex = scenes.standard_textures()
     ctx.upload_textures(tex)
     frames = orbit_frames(ws, args.width, args.height)
+    variant = {}
+    if args.precision == "fp64":  # profiling variants, named in the output's config
+        for f in frames:
+            f.precision = abi.PREC_FP64
+        variant["precision"] = "fp64"
+    ham_mask = abi.HAM_FP32 | abi.HAM_FP64
+    if args.form == "contraction":
+        ham_mask = 0
+        ctx.set_option(abi.OPT_HAMILTONIAN, ham_mask)
+        variant["form"] = "contraction"
     frame = frames[rank]  # this rank's share when every rank draws one frame (weak scaling)
     npx = frame.width * frame.height
     t_tune = time.perf_counter()
@@ -953,7 +967,7 @@ def main():
                     "kernel": pair_kernel_name(ctx.launch_config()), "kernel_ms": st.trace_ms,
                     "flop_per_attempt": F_ATTEMPT, "attempts": st.attempts,
                     "frac_basis": "algorithmic: attempts x F_attempt (the work of one RKF45 attempt of the (x, u) "
-                                  "system in the Kerr-Schild contraction form, FMA = 2; ncu counts 1,532 executed "
+                                  "system in the Kerr-Schild contraction form, FMA = 2; ncu counts 1,459 executed "
                                   "for it) / kernel time",
                     "ncu_counted": {"achieved": counted, "frac": counted / fp32_peak,
                                     "flop_per_attempt": ncu_flop, "rule": NCU_FLOP_RULE,
@@ -983,7 +997,7 @@ def main():
             ctx.set_option(abi.OPT_GEOD_TABLE, -1)
             ctx.set_option(abi.OPT_HAMILTONIAN, abi.HAM_FP64)
             contraction_ms = timed_device()                # persistent scheduler + contraction, (x, u) state
-            ctx.set_option(abi.OPT_HAMILTONIAN, abi.HAM_FP32 | abi.HAM_FP64)
+            ctx.set_option(abi.OPT_HAMILTONIAN, ham_mask)
             extra["plain"] = {"value": rays / (plain_ms * 1e-3) / 1e6, "ms_per_step": plain_ms,
                               "speedup": plain_ms / ms,
                               "speedup_scheduler_only": plain_contraction_ms / contraction_ms,
@@ -1073,7 +1087,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural textures)",
-            "config": workload_config(args.width, args.height),
+            "config": dict(workload_config(args.width, args.height), **({"variant": variant} if variant else {})),
             "launch": {"schedule": "persistent" + (", frames pulled from a shared counter" if ws > 1 else ""),
                        "shape": {k: getattr(ctx.launch_config(), k) for k, _ in LaunchConfig._fields_},
                        "source": tuned_on, "autotune_s": round(t_tune, 2)},

@@ -451,6 +451,12 @@ prr_status prr_set_option(prr_ctx *ctx, int option, long long value);
  * with a dependent-chain FMA kernel; either pointer may be NULL. */
 prr_status prr_measure_peak(prr_ctx *ctx, double *fp32_tflops, double *fp64_tflops);
 
+/* Evaluates on the device the reciprocal and reciprocal square root that the
+ * PHYSICAL-mode kernels use, for checking their error: for each of the n
+ * inputs x[i] (1 <= n <= 2^20), out[4i .. 4i+3] = FP64 1/x, FP64 1/sqrt(x),
+ * FP32 1/(float)x, FP32 1/sqrt((float)x) (the FP32 values widened). */
+prr_status prr_check_recip(prr_ctx *ctx, const double *x, int n, double *out);
+
 /* ---- input decks (replaces main/io.h:21-58 readParams, the getters of
  *      main/Parameters.cpp:20-44, checkFrame prr.cpp:139-153, createScene
  *      prr.cpp:159-198, Spacetime::setupScene/updateScene

@@ -110,6 +110,14 @@ class Context:
         self._check(self.lib.prr_measure_peak(self.h, C.byref(f32), C.byref(f64)))
         return f32.value, f64.value
 
+    def check_recip(self, x: np.ndarray) -> np.ndarray:
+        """prr_check_recip: (n, 4) float64 of the device's FP64 1/x, 1/sqrt(x) and FP32 1/x,
+        1/sqrt(x) as the PHYSICAL kernels compute them."""
+        xs = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        out = np.empty((xs.size, 4), dtype=np.float64)
+        self._check(self.lib.prr_check_recip(self.h, xs.ctypes.data_as(abi._dp), xs.size, out.ctypes.data_as(abi._dp)))
+        return out
+
     def render(self, frames, want_float: bool = False, out8: np.ndarray | None = None):
         """Renders one or more frames; returns (list of uint8 (h, w, 3)
         images, list of float32 images or None, Stats).  `out8` may supply

@@ -116,6 +116,7 @@ SIGNATURES = {
     "prr_autotune": (C.c_int, [_P, C.POINTER(FrameDesc), C.POINTER(LaunchConfig)]),
     "prr_set_option": (C.c_int, [_P, C.c_int, C.c_longlong]),
     "prr_measure_peak": (C.c_int, [_P, _dp, _dp]),
+    "prr_check_recip": (C.c_int, [_P, _dp, C.c_int, _dp]),
     "prr_make_texture": (C.c_int, [C.c_int, C.c_uint32, C.c_int, C.c_int, _u8p]),
     "prr_frame_desc_defaults": (None, [C.POINTER(FrameDesc)]),
     "prr_sizeof": (C.c_size_t, [C.c_int]),

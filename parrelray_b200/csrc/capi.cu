@@ -401,4 +401,21 @@ prr_status prr_measure_peak(prr_ctx *ctx, double *fp32_tflops, double *fp64_tflo
     return PRR_OK;
 }
 
+prr_status prr_check_recip(prr_ctx *ctx, const double *x, int n, double *out)
+{
+    if (!ctx) return PRR_ERR_INVALID;
+    if (!x || !out || n < 1 || n > (1 << 20)) {
+        ctx->err = "prr_check_recip: needs 1..2^20 inputs and an output of 4 doubles per input";
+        return PRR_ERR_INVALID;
+    }
+    PRR_CK(ctx, cudaSetDevice(ctx->device));
+    if (ctx->scratch.ensure((size_t)n * 5 * sizeof(double)) != PRR_OK) return PRR_ERR_NOMEM;
+    double *d_x = (double *)ctx->scratch.p, *d_out = d_x + n;
+    PRR_CK(ctx, cudaMemcpyAsync(d_x, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    PRR_CK(ctx, launch_check_recip(d_x, n, d_out, ctx->stream));
+    PRR_CK(ctx, cudaMemcpyAsync(out, d_out, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PRR_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return PRR_OK;
+}
+
 }  // extern "C"

@@ -34,4 +34,25 @@ cudaError_t launch_dfma_peak(double *sink, int blocks, int threads, int iters, c
     return cudaGetLastError();
 }
 
+// The reciprocal and reciprocal square root of the PHYSICAL path
+// (prr_device.cuh frcp/frsqrt) on x[i]: out[4i .. 4i+3] = FP64 1/x, FP64
+// 1/sqrt(x), FP32 1/(float)x, FP32 1/sqrt((float)x), for tests of their
+// error against the correctly rounded values.
+__global__ void k_check_recip(const double *x, int n, double *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = x[i];
+    out[4 * i] = frcp<double>(v);
+    out[4 * i + 1] = frsqrt<double>(v);
+    out[4 * i + 2] = (double)frcp<float>((float)v);
+    out[4 * i + 3] = (double)frsqrt<float>((float)v);
+}
+
+cudaError_t launch_check_recip(const double *x, int n, double *out, cudaStream_t st)
+{
+    k_check_recip<<<(n + 255) / 256, 256, 0, st>>>(x, n, out);
+    return cudaGetLastError();
+}
+
 }  // namespace prr

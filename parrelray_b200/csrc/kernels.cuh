@@ -120,5 +120,7 @@ constexpr int ADJ_CHECKPOINT_INTERVAL = 64;
 // fma_peak.cu
 cudaError_t launch_fma_peak(float *sink, int blocks, int threads, int iters, cudaStream_t st);
 cudaError_t launch_dfma_peak(double *sink, int blocks, int threads, int iters, cudaStream_t st);
+// fma_peak.cu: frcp/frsqrt (FP64 and FP32) on n inputs, 4 outputs each
+cudaError_t launch_check_recip(const double *x, int n, double *out, cudaStream_t st);
 
 }  // namespace prr

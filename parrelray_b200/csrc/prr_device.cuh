@@ -34,19 +34,42 @@ template <class T> struct V4 { T x, y, z, w; };
 // about 2^-23, far below the 1e-6 integration tolerance), with subnormal
 // inputs and results flushed to zero, so no range or subnormal fix-up
 // instructions surround them; the arguments on this path (squared radii,
-// norms, error ratios) are normal numbers or 0.  FP64 uses the correctly
-// rounded reciprocal (no general division) and CUDA's double rsqrt (within
-// an ulp) in place of a square root followed by a division.
+// norms, error ratios) are normal numbers or 0.  FP64 starts from the SFU's
+// double-precision seeds (PTX rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64, good
+// to about 2^-22) and refines them with two Newton-Raphson steps on DFMA
+// (x <- x + x (1 - v x) for 1/v; y <- y + y (1/2 - (v/2) y^2) for 1/sqrt(v);
+// each step doubles the correct bits, Markstein's formulation of the
+// iterations with a fused multiply-add), to within an ulp or two of the
+// correctly rounded values, for normal positive arguments.
 PRR_DEV float sfu_rcp(float v) { float r; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v)); return r; }
 PRR_DEV float sfu_rsqrt(float v) { float r; asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v)); return r; }
 PRR_DEV float sfu_lg2(float v) { float r; asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v)); return r; }
 PRR_DEV float sfu_ex2(float v) { float r; asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v)); return r; }
+PRR_DEV double nr_rcp(double v)
+{
+    double x;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(v));
+    double e = __fma_rn(-v, x, 1.0);
+    x = __fma_rn(x, e, x);
+    e = __fma_rn(-v, x, 1.0);
+    return __fma_rn(x, e, x);
+}
+PRR_DEV double nr_rsqrt(double v)
+{
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(v));
+    const double hv = 0.5 * v;
+    double r = __fma_rn(-hv * y, y, 0.5);
+    y = __fma_rn(y, r, y);
+    r = __fma_rn(-hv * y, y, 0.5);
+    return __fma_rn(y, r, y);
+}
 template <class T> PRR_DEV T frcp(T v) { return (T)1 / v; }
 template <> PRR_DEV float frcp<float>(float v) { return sfu_rcp(v); }
-template <> PRR_DEV double frcp<double>(double v) { return __drcp_rn(v); }
+template <> PRR_DEV double frcp<double>(double v) { return nr_rcp(v); }
 template <class T> PRR_DEV T frsqrt(T v) { return (T)1 / sqrt(v); }
 template <> PRR_DEV float frsqrt<float>(float v) { return sfu_rsqrt(v); }
-template <> PRR_DEV double frsqrt<double>(double v) { return rsqrt(v); }
+template <> PRR_DEV double frsqrt<double>(double v) { return nr_rsqrt(v); }
 template <class T> PRR_DEV T fpow(T b, T e) { return pow(b, e); }
 template <> PRR_DEV float fpow<float>(float b, float e) { return sfu_ex2(e * sfu_lg2(b)); }
 

@@ -192,3 +192,20 @@ def test_hamiltonian_and_contraction_forms_agree(gpu, small_textures, kerr_oracl
     assert sa.rays == sb.rays == d.nrays and sa.n_math_error == 0
     st, _, _ = gpu.trace_rays(d)
     assert np.all(st[:, 6] == 0.0)  # the coordinate time is not integrated in this form
+
+
+def test_device_reciprocals_against_correct_rounding(gpu):
+    """The reciprocal and reciprocal square root of the PHYSICAL kernels (SFU seeds; in FP64 two
+    Newton-Raphson steps on top) against the correctly rounded values, over the range the path
+    feeds them (squared radii, Sigma, norms, error scales: 1e-12 .. 1e12)."""
+    rng = np.random.default_rng(5)
+    x = np.concatenate([10.0 ** rng.uniform(-12, 12, 200000), [1.0, 2.0, 3.0, 0.5, 1e-6, 1e6, 25.0, 100.0]])
+    out = gpu.check_recip(x)
+    rel = lambda got, ref: np.abs(got / ref - 1.0)
+    # FP64: within 2 ulp (2^-52 relative)
+    assert rel(out[:, 0], 1.0 / x).max() <= 2.0 ** -51, rel(out[:, 0], 1.0 / x).max()
+    assert rel(out[:, 1], 1.0 / np.sqrt(x)).max() <= 2.0 ** -51, rel(out[:, 1], 1.0 / np.sqrt(x)).max()
+    # FP32 SFU approximations: a few ulp of FP32 (2^-21 relative)
+    x32 = x.astype(np.float32).astype(np.float64)
+    assert rel(out[:, 2], 1.0 / x32).max() <= 2.0 ** -21
+    assert rel(out[:, 3], 1.0 / np.sqrt(x32)).max() <= 2.0 ** -21
