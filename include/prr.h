@@ -441,8 +441,8 @@ prr_status prr_autotune(prr_ctx *ctx, const prr_frame_desc *frame, prr_launch_co
                                      PRR_HAM_FP64 (FP64 renders); default both (3), 0 for neither.  Both
                                      forms use the same tableau, error test (over their own state), caps,
                                      hooks and colours; in the Hamiltonian form the coordinate time is not
-                                     integrated, so r.w of prr_trace_rays(_f64) is 0 there.  The FP64 pass
-                                     of SPLIT and the adjoint's own stepping use the (x, u) form */
+                                     integrated, so r.w of prr_trace_rays(_f64) is 0 there.  PRR_HAM_FP64
+                                     also covers the FP64 pass of SPLIT; the adjoint always steps (x, u) */
 #define PRR_HAM_FP32 1
 #define PRR_HAM_FP64 2
 prr_status prr_set_option(prr_ctx *ctx, int option, long long value);

@@ -250,13 +250,17 @@ template <class T> PRR_DEV HamStep<T> ham_stages(const HamRay<T> &R, const HamCo
     return o;
 }
 
-// state update: Kahan-compensated in FP32, a plain sum in FP64 (whose
-// roundoff over 10^4 steps stays far below the tolerances)
+// state update: Kahan-compensated in FP32 (both components of a pair at once
+// on the paired adds: y = v - c, t = s + y, c = (t - s) - y, s = t, each
+// lane rounded as its scalar add), a plain sum in FP64 (whose roundoff over
+// 10^4 steps stays far below the tolerances)
 template <class V> PRR_DEV void upd2(V &s, V &c, V v)
 {
     if constexpr (sizeof(s.x) == 4) {
-        kahan_add(s.x, c.x, v.x);
-        kahan_add(s.y, c.y, v.y);
+        const V y = add_(v, neg_(c));
+        const V t = add_(s, y);
+        c = add_(add_(t, neg_(s)), neg_(y));
+        s = t;
     } else {
         s.x += v.x;
         s.y += v.y;
@@ -280,7 +284,8 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const 
     upd2(Pn, cPn, st.dP);
     upd2(Qn, cQn, st.dQ);
     upd2(Wn, cWn, st.dW);
-    if (isnan(Pn.x + Pn.y + Wn.x + Qn.x + Qn.y + Wn.y)) {
+    const V nan_probe = add_(add_(Pn, Qn), Wn);  // NaN in any component propagates
+    if (isnan(nan_probe.x + nan_probe.y)) {
         result = PRR_RESULT_MATH_ERROR; colour = {0, 0, 0};
         u_out = ham_velocity<T>(R.P.x, R.P.y, R.W.x, R.Q.x, R.Q.y, R.W.y, sl.c);
         return STEP_DONE;
@@ -572,6 +577,95 @@ __global__ void __launch_bounds__(MAXT, MINB) k_ham(PersistentArgs a)
     warp_sum_add_h(&a.counters[C_INFINITE], cnt.inf);
     warp_sum_add_h(&a.counters[C_MATH_ERROR], cnt.nan);
     if (SPLIT) warp_sum_add_h(&a.counters[C_FP64], cnt.f64);
+}
+
+// FP64 re-integration, in Hamiltonian form, of the rays a split-precision
+// FP32 pass queued (k_fp64_requeue's job for the (x, u) form): each queued
+// ray is integrated again from the camera in FP64 and its per-sample colour
+// overwritten; it is counted as a ray here.  64-thread CTAs built for the
+// FP64 renderer's occupancy.
+template <int MAXT, int MINB> __global__ void __launch_bounds__(MAXT, MINB) k_ham_requeue(PersistentArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    bool busy = false, need = true;
+    HSlot<double> sl;
+    sl.busy = false; sl.need = false; sl.crit = false; sl.flag_r = -1.0f;
+    sl.frame = 0; sl.px = sl.py = sl.s = 0; sl.S = 1;
+    sl.acc0 = sl.acc1 = sl.acc2 = 0.f;
+    long long rid = 0;
+    HCounts cnt;
+    long long nq = (long long)*(volatile unsigned long long *)&a.counters[C_FP64_QUEUED];
+    if (nq > a.fp64_capacity) nq = a.fp64_capacity;
+    while (true) {
+        const unsigned needmask = __ballot_sync(FULL, need);
+        if (needmask) {
+            const int leader = __ffs(needmask) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(&a.counters[C_WORK_FP64], (unsigned long long)__popc(needmask));
+            base = __shfl_sync(FULL, base, leader);
+            if (need) {
+                const long long it = (long long)base + __popc(needmask & ((1u << lane) - 1));
+                need = false;
+                busy = false;
+                if (it < nq) {
+                    const unsigned long long e = a.fp64_queue[it];
+                    sl.frame = (int)(e >> 40);
+                    rid = (long long)(e & ((1ull << 40) - 1));
+                    const FrameParams &fp = a.frames[sl.frame];
+                    const long long pix = rid / fp.samples;
+                    sl.s = (int)(rid - pix * fp.samples);
+                    sl.px = (int)(pix % fp.width);
+                    sl.py = (int)(pix / fp.width);
+                    sl.S = fp.samples;
+                    sl.q = make_hot<double>(fp);
+                    ham_init<double, false, false>(fp, sl, sl.s);
+                    busy = true;
+                }
+            }
+        }
+        if (__ballot_sync(FULL, busy) == 0) break;
+        if (!busy) continue;
+        const FrameParams &fp = a.frames[sl.frame];
+        int result = 0;
+        V3<float> col = {0.f, 0.f, 0.f};
+        if (sl.R.l < 1000.0) {  // the loop bound of trace_RKF (solver.cuh:158)
+            sl.R.i += 1;
+            const HamStep<double> st = ham_stages<double>(sl.R, sl.c, sl.q);
+            V4<double> u;
+            if (ham_accept<double, false>(fp, sl, sl.R, st, result, col, u) == STEP_CONTINUE) continue;
+        } else {
+            result = PRR_RESULT_INFINITE_GEO;
+        }
+        cnt.att += (unsigned)sl.R.i;
+        cnt.acc += (unsigned)sl.R.accepted;
+        cnt.rays++;
+        if (result == PRR_RESULT_SUCCESS) {
+            if (metric_radius<double>(fp, sl.R.P.x, sl.R.P.y, sl.R.W.x) >= sl.q.rout) cnt.esc++; else cnt.cap++;
+        } else if (result == PRR_RESULT_INTERSECTION) cnt.hit++;
+        else if (result == PRR_RESULT_INFINITE_GEO) cnt.inf++;
+        else cnt.nan++;
+        float *o = a.sample_rgb + 3 * (fp.ray_begin + rid);
+        o[0] = col.x; o[1] = col.y; o[2] = col.z;
+        busy = false;
+        need = true;
+    }
+    warp_sum_add_h(&a.counters[C_ATTEMPTS], cnt.att);
+    warp_sum_add_h(&a.counters[C_ACCEPTED], cnt.acc);
+    warp_sum_add_h(&a.counters[C_RAYS], cnt.rays);
+    warp_sum_add_h(&a.counters[C_ESCAPED], cnt.esc);
+    warp_sum_add_h(&a.counters[C_CAPTURED], cnt.cap);
+    warp_sum_add_h(&a.counters[C_INTERSECTION], cnt.hit);
+    warp_sum_add_h(&a.counters[C_INFINITE], cnt.inf);
+    warp_sum_add_h(&a.counters[C_MATH_ERROR], cnt.nan);
+}
+
+cudaError_t launch_ham_requeue(const PersistentArgs &a, int nsm, cudaStream_t st)
+{
+    int bpsm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_ham_requeue<64, ham_small_minb<double>()>, 64, 0);
+    if (e != cudaSuccess) return e;
+    k_ham_requeue<64, ham_small_minb<double>()><<<nsm * (bpsm > 0 ? bpsm : 1), 64, 0, st>>>(a);
+    return cudaGetLastError();
 }
 
 template <class T, bool SPLIT, bool EMIS> static cudaError_t ham_launch(const PersistentArgs &a, int block, int grid, cudaStream_t st)

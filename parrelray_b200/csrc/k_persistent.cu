@@ -302,6 +302,7 @@ int persistent_occupancy(int precision, int geod_table, int block, int rays_per_
 
 cudaError_t launch_fp64_requeue(const PersistentArgs &a, int block, int nsm, cudaStream_t st)
 {
+    if (a.hamiltonian & PRR_HAM_FP64) return launch_ham_requeue(a, nsm, st);
     int bpsm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_fp64_requeue, 128, 0);
     if (e != cudaSuccess) return e;

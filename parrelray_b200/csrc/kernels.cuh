@@ -79,6 +79,9 @@ int persistent_occupancy(int precision, int geod_table, int block, int rays_per_
 cudaError_t launch_ham(const PersistentArgs &a, int precision, bool split, int block, int blocks_per_sm, int nsm,
                        cudaStream_t st);
 int ham_occupancy(int precision, int block, bool split = false, bool emission = false);
+// k_ham.cu: the FP64 pass of a split-precision render in Hamiltonian form
+// (launch_fp64_requeue calls it when a.hamiltonian has PRR_HAM_FP64).
+cudaError_t launch_ham_requeue(const PersistentArgs &a, int nsm, cudaStream_t st);
 
 // k_pair.cu: the FP32 renderer with `rpt` pixel slots per thread; `split`:
 // the FP32 pass of a split-precision render (rpt 1; needs sample_rgb and
