@@ -138,14 +138,25 @@ def build_metric_plugin(header: Path, name: str | None = None, verbose: bool = F
         shutil.copytree(COMPAT / sub, stage / sub)
     (stage / "metrics").mkdir(parents=True)
     shutil.copy(header, stage / "metrics" / header.name)
-    tu = stage / f"plugin_{name}.cu"
-    tu.write_text(f'#include "metrics/{header.name}"\n#include "prr_plugin.cuh"\n')
+    # two translation units: the REFERENCE renderer and the colouring with -fmad=false (the reference's
+    # FP32 operation order), the PHYSICAL renderer with contraction on; the header's rayToRGB kernel is
+    # renamed in the second, which does not launch it
+    tu_ref = stage / f"plugin_{name}_reference.cu"
+    tu_ref.write_text(f'#define PRR_PLUGIN_PART 1\n#include "metrics/{header.name}"\n#include "prr_plugin.cuh"\n')
+    tu_phys = stage / f"plugin_{name}_physical.cu"
+    tu_phys.write_text(f'#define PRR_PLUGIN_PART 2\n#define rayToRGB prr_plugin_header_rayToRGB_unused\n'
+                       f'#include "metrics/{header.name}"\n#undef rayToRGB\n#include "prr_plugin.cuh"\n')
     out.parent.mkdir(parents=True, exist_ok=True)
+    common = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-w",
+              f'-DPRR_PLUGIN_NAME="{name}"', *(["-DSPHERICAL"] if spherical else []),
+              "-I", str(stage), "-I", str(COMPAT), "-I", str(CSRC), "-I", str(INCLUDE)]
     try:
-        _run([nvcc(), "-fmad=false", *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-              "--expt-relaxed-constexpr", "-w", f'-DPRR_PLUGIN_NAME="{name}"', *(["-DSPHERICAL"] if spherical else []),
-              "-I", str(stage), "-I", str(COMPAT),
-              "-I", str(CSRC), "-I", str(INCLUDE), str(tu), "-o", str(out)], verbose)
+        _run([nvcc(), "-fmad=false", *common, "-c", str(tu_ref), "-o", str(stage / "reference.o")], verbose)
+        _run([nvcc(), *common, "-c", str(tu_phys), "-o", str(stage / "physical.o")], verbose)
+        # the header's functions are defined in both units (their host-side stubs would collide): every
+        # symbol of the second but its entry point becomes local to it
+        _run(["objcopy", "--keep-global-symbol=prr_plugin_trace_physical", str(stage / "physical.o")], verbose)
+        _run([nvcc(), *ARCH, "-shared", str(stage / "reference.o"), str(stage / "physical.o"), "-o", str(out)], verbose)
     finally:
         shutil.rmtree(stage, ignore_errors=True)
     return out

@@ -27,7 +27,15 @@
 // the same hooks on the persistent, warp-compacted scheduler with the
 // PHYSICAL stepper (hook_stepper.cuh).
 // SSAA combine, FXAA and quantisation then run in the library as for the
-// built-in metrics.  Built with -fmad=false, as the built-in REFERENCE path.
+// built-in metrics.
+//
+// PRR_PLUGIN_PART selects what a translation unit holds: 1 the REFERENCE
+// renderer, the colouring (the header's rayToRGB) and the library's metadata
+// entry points, built with -fmad=false as the built-in REFERENCE path, so the
+// header's FP32 arithmetic is the reference's operation for operation; 2 the
+// PHYSICAL renderer, built with contraction on (its bar is the FP64 oracle,
+// not the reference's rounding), which colours through part 1's
+// prr_plugin_colour; 0 (or undefined) both, in one translation unit.
 #include <algorithm>
 
 #include "hook_stepper.cuh"
@@ -37,6 +45,11 @@
 #ifndef PRR_PLUGIN_NAME
 #define PRR_PLUGIN_NAME "plugin"
 #endif
+#ifndef PRR_PLUGIN_PART
+#define PRR_PLUGIN_PART 0
+#endif
+#define PRR_PLUGIN_HAS_REFERENCE (PRR_PLUGIN_PART == 0 || PRR_PLUGIN_PART == 1)
+#define PRR_PLUGIN_HAS_PHYSICAL (PRR_PLUGIN_PART == 0 || PRR_PLUGIN_PART == 2)
 
 namespace prr_plugin {
 
@@ -165,6 +178,7 @@ __device__ __forceinline__ void warp_add(unsigned long long *p, unsigned long lo
     if ((threadIdx.x & 31) == (__ffs(mask) - 1)) atomicAdd(p, v);
 }
 
+#if PRR_PLUGIN_HAS_REFERENCE
 __global__ void __launch_bounds__(128) k_plugin_trace(const FrameParams *__restrict__ fps, int frame, long long nrays,
                                                       Ray *__restrict__ rays, float *__restrict__ state,
                                                       unsigned long long *__restrict__ counters)
@@ -198,6 +212,9 @@ __global__ void __launch_bounds__(128) k_plugin_trace(const FrameParams *__restr
     }
 }
 
+#endif  // PRR_PLUGIN_HAS_REFERENCE
+
+#if PRR_PLUGIN_HAS_PHYSICAL
 // PHYSICAL mode through the header's hooks (hook_stepper.cuh) on the
 // persistent scheduler: CTAs stay resident and each lane integrates one ray
 // at a time, one RKF45 attempt per loop iteration; every `interval` attempts
@@ -279,6 +296,9 @@ __global__ void __launch_bounds__(128) k_plugin_phys(const FrameParams *__restri
     }
 }
 
+#endif  // PRR_PLUGIN_HAS_PHYSICAL
+
+#if PRR_PLUGIN_HAS_REFERENCE
 // Per-sample colour (Ray::u after rayToRGB) and outcome counters.
 __global__ void k_plugin_collect(const Ray *__restrict__ rays, long long nrays, float rout, float *__restrict__ rgb,
                                  unsigned long long *__restrict__ counters)
@@ -303,24 +323,25 @@ __global__ void k_plugin_collect(const Ray *__restrict__ rays, long long nrays, 
     }
 }
 
+#endif  // PRR_PLUGIN_HAS_REFERENCE
+
 }  // namespace prr_plugin
 
 // ---- the plug-in library's C entry points (loaded by prr_load_metric_plugin) ----
 
+// rayToRGB as renderframe launches it (prr.cpp:317-319) over d_rays, then the
+// per-sample colours d_rgb and outcome counters; asynchronous on `stream`.
+extern "C" int prr_plugin_colour(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays,
+                                 float *d_rgb, unsigned long long *d_counters, void *stream);
+
+#if PRR_PLUGIN_HAS_REFERENCE
 extern "C" int prr_plugin_abi_version(void) { return PRR_ABI_VERSION; }
 extern "C" size_t prr_plugin_frame_params_size(void) { return sizeof(prr::FrameParams); }
 extern "C" size_t prr_plugin_ray_bytes(void) { return sizeof(Ray); }
 extern "C" const char *prr_plugin_name(void) { return PRR_PLUGIN_NAME; }
 
-// Traces frame `frame` of the device frame table d_fps (h_fp: the same block
-// on the host) into d_rays (nrays Ray records), and writes the per-sample
-// colours d_rgb (3 floats/ray) and, when non-null, the per-ray states d_state
-// (12 floats/ray) and counters.  Asynchronous on `stream`; returns a
-// cudaError_t.
 namespace prr_plugin {
 
-// rayToRGB as renderframe launches it (prr.cpp:317-319), then the colours
-// and outcome counters.
 inline cudaError_t colour_rays(const FrameParams &fp, const FrameParams *dfp, int frame, long long nrays, Ray *rays,
                                float *d_rgb, unsigned long long *d_counters, cudaStream_t st)
 {
@@ -337,6 +358,18 @@ inline cudaError_t colour_rays(const FrameParams &fp, const FrameParams *dfp, in
 
 }  // namespace prr_plugin
 
+extern "C" int prr_plugin_colour(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays,
+                                 float *d_rgb, unsigned long long *d_counters, void *stream)
+{
+    return (int)prr_plugin::colour_rays(*(const prr::FrameParams *)h_fp, (const prr::FrameParams *)d_fps, frame,
+                                        nrays, (Ray *)d_rays, d_rgb, d_counters, (cudaStream_t)stream);
+}
+
+// Traces frame `frame` of the device frame table d_fps (h_fp: the same block
+// on the host) into d_rays (nrays Ray records), and writes the per-sample
+// colours d_rgb (3 floats/ray) and, when non-null, the per-ray states d_state
+// (12 floats/ray) and counters.  Asynchronous on `stream`; returns a
+// cudaError_t.
 extern "C" int prr_plugin_trace(const void *h_fp, const void *d_fps, int frame, long long nrays, void *d_rays,
                                 float *d_state, float *d_rgb, unsigned long long *d_counters, void *stream)
 {
@@ -352,7 +385,9 @@ extern "C" int prr_plugin_trace(const void *h_fp, const void *d_fps, int frame, 
     if (e != cudaSuccess) return (int)e;
     return (int)colour_rays(fp, dfp, frame, nrays, rays, d_rgb, d_counters, st);
 }
+#endif  // PRR_PLUGIN_HAS_REFERENCE
 
+#if PRR_PLUGIN_HAS_PHYSICAL
 // PHYSICAL mode (FP32) on the persistent scheduler, same arguments and
 // outputs as prr_plugin_trace; d_counters is required (its work counter is
 // reset here).  Launches k_plugin_phys with resident CTAs of 128 threads on
@@ -364,7 +399,6 @@ extern "C" int prr_plugin_trace_physical(const void *h_fp, const void *d_fps, in
     if (nrays <= 0) return (int)cudaSuccess;
     if (!d_counters) return (int)cudaErrorInvalidValue;
     cudaStream_t st = (cudaStream_t)stream;
-    const FrameParams &fp = *(const FrameParams *)h_fp;
     const FrameParams *dfp = (const FrameParams *)d_fps;
     Ray *rays = (Ray *)d_rays;
     int dev = 0, nsm = 0, bpsm = 0;
@@ -376,5 +410,6 @@ extern "C" int prr_plugin_trace_physical(const void *h_fp, const void *d_fps, in
     const long long grid = std::min<long long>((long long)nsm * (bpsm > 0 ? bpsm : 1), (nrays + 127) / 128);
     k_plugin_phys<<<(unsigned)grid, 128, 0, st>>>(dfp, frame, nrays, rays, d_state, d_counters, 16);
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-    return (int)colour_rays(fp, dfp, frame, nrays, rays, d_rgb, d_counters, st);
+    return prr_plugin_colour(h_fp, d_fps, frame, nrays, d_rays, d_rgb, d_counters, stream);
 }
+#endif  // PRR_PLUGIN_HAS_PHYSICAL
