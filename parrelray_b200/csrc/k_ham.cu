@@ -75,7 +75,7 @@ __device__ __forceinline__ uint8_t q8h(float v) { return (uint8_t)roundf(255.0f 
 
 // Per-ray constants of the right-hand side.
 template <class T> struct HamConst {
-    T M2, a, a2, a4, pt;  // 2M, a, a^2, 4 a^2, p_t
+    T M2, a, a2, nha2, pt;  // 2M, a, a^2, -a^2/2, p_t
 };
 
 // dy/dlambda at (P = (x, y), Q = (p_x, p_y), W = (z, p_z)); outputs dP, dQ, dW
@@ -87,38 +87,42 @@ PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP,
 {
     using V = P2<T>;
     const T X = P.x, Y = P.y, z = W.x, pz = W.y;
+    // with hb = (R^2 - a^2)/2 and Sh = S/2, S = sqrt((R^2 - a^2)^2 + 4 a^2 z^2):
+    // r^2 = hb + Sh, grad r = (x, y, z q / r^2) r / S
     const T Z2 = mul_(z, z);
     const T R2 = fma_(X, X, fma_(Y, Y, Z2));
-    const T b = add_(R2, -c.a2);
-    const T S2 = fma_(b, b, mul_(c.a4, Z2));
-    const T iS = rsq_(S2);
-    const T S = mul_(S2, iS);
-    const T r2 = mul_(T(0.5), add_(b, S));
+    const T hb = fma_(T(0.5), R2, c.nha2);
+    const T a2Z2 = mul_(c.a2, Z2);
+    const T S2h = fma_(hb, hb, a2Z2);
+    const T iSh = rsq_(S2h);
+    const T r2 = add_(hb, mul_(S2h, iSh));
     const T ir = rsq_(r2);
     const T r = mul_(r2, ir);
     const T q = add_(r2, c.a2), iq = rcp_(q);
-    const T Sig = fma_(r2, r2, mul_(c.a2, Z2)), iSig = rcp_(Sig);
+    const T Sig = fma_(r2, r2, a2Z2), iSig = rcp_(Sig);
     const V iq_ = sp(iq);
-    // gradients of r and of f/2 (the 1/2 of 1/2 Lam^2 grad f folded in)
-    const V dr = mul_(P, sp(mul_(r, iS)));
-    const T drz = mul_(mul_(z, q), mul_(iS, ir));
+    // twice the gradient of r, and the gradient of f/2 (the 1/2 of 1/2 Lam^2 grad f folded in):
+    // grad f = c1 grad r with c1 = f (3/r - 4 r^3/Sigma); c1/4 = f (3/(4r) - r^3/Sigma)
+    const V dr2 = mul_(P, sp(mul_(r, iSh)));
+    const T drz2 = mul_(mul_(z, q), mul_(iSh, ir));
     const T r3 = mul_(r2, r);
     const T t = mul_(r3, iSig);
     const T f = mul_(c.M2, t);
-    const T c1h = mul_(f, fma_(T(-2), t, mul_(T(1.5), ir)));
-    const V dfh = mul_(sp(c1h), dr);
-    const T dfzh = fma_(c1h, drz, mul_(mul_(f, iSig), mul_(neg_(c.a2), z)));
+    const T c1q = mul_(f, fma_(T(0.75), ir, neg_(t)));
+    const V dfh = mul_(sp(c1q), dr2);
+    const T dfzh = fma_(c1q, drz2, mul_(mul_(f, iSig), mul_(neg_(c.a2), z)));
     // l and Lam = l.p - p_t
     const V l = mul_(fma_(sp(r), P, f2(mul_(c.a, Y), neg_(mul_(c.a, X)))), iq_);
     const T lz = mul_(z, ir);
     const T px = Q.x, py = Q.y;
     const T lpxy = fma_(px, l.x, mul_(py, l.y));
     const T Lam = fma_(lz, pz, add_(lpxy, neg_(c.pt)));
-    // gradient of l.p at fixed p
-    const T P0 = fma_(mul_(T(-2), r), lpxy, fma_(px, X, mul_(py, Y)));
-    const T Pp = fma_(P0, iq, neg_(mul_(pz, mul_(lz, ir))));
-    const V dL = fma_(dr, sp(Pp), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
-    const T dLz = fma_(drz, Pp, mul_(pz, ir));
+    // gradient of l.p at fixed p: grad r times Pp = ((x p_x + y p_y) - 2 r l.p_xy)/q - p_z l_z / r, taken
+    // as (2 grad r) (Pp / 2)
+    const T P0h = fma_(neg_(r), lpxy, mul_(T(0.5), fma_(px, X, mul_(py, Y))));
+    const T Pph = fma_(P0h, iq, neg_(mul_(mul_(T(0.5), pz), mul_(lz, ir))));
+    const V dL = fma_(dr2, sp(Pph), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
+    const T dLz = fma_(drz2, Pph, mul_(pz, ir));
     // Hamilton's equations
     const T fL = mul_(f, Lam);
     const T L2 = mul_(Lam, Lam);
@@ -132,8 +136,8 @@ PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP,
 template <class T> PRR_DEV V4<T> ham_velocity(T x, T y, T z, T px, T py, T pz, const HamConst<T> &c)
 {
     const T R2 = x * x + y * y + z * z;
-    const T b = R2 - c.a2;
-    const T r2 = T(0.5) * (b + sqrt(b * b + c.a4 * z * z));
+    const T hb = T(0.5) * R2 + c.nha2;
+    const T r2 = hb + sqrt(hb * hb + c.a2 * z * z);
     const T r = sqrt(r2);
     const T q = r2 + c.a2;
     const T f = c.M2 * r2 * r / (r2 * r2 + c.a2 * z * z);
@@ -183,7 +187,7 @@ __device__ __forceinline__ void ham_init(const FrameParams &fp, HSlot<T> &sl, in
     R.cP = R.cQ = R.cW = sp(T(0));
     R.h = (T)fp.h; R.trace_h = (T)fp.h; R.l = T(0);
     R.i = 0; R.accepted = 0; R.intersect = 0;
-    sl.c = {T(2) * M, a, a * a, T(4) * a * a, p[3]};
+    sl.c = {T(2) * M, a, a * a, T(-0.5) * a * a, p[3]};
     if constexpr (EMIS) emis_init_p<T>(fp, U.x.x, U.x.y, U.x.z, p[3], sl.E);
 }
 
