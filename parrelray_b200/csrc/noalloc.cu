@@ -178,7 +178,7 @@ extern "C" prr_status prr_render_noalloc(const prr_frame_desc *frames, int n, co
     const int block = 64;
     a.compaction_interval = 64;
     a.rays_per_thread = 1;
-    const int bpsm = persistent_occupancy(plan.precision, 0, block, 1, plan.any_emission, 1);
+    const int bpsm = persistent_occupancy(plan.precision, 0, block, 1, plan.any_emission, a.hamiltonian);
     if (e == cudaSuccess) e = launch_persistent(a, plan.precision, block, bpsm > 0 ? bpsm : 1, nsm, st);
     for (int f = 0; f < n && e == cudaSuccess; f++) {
         const FrameParams &p = plan.fp[f];

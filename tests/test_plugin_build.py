@@ -62,6 +62,9 @@ def test_user_header_builds_unchanged(built, tmp_path):
     assert lib.prr_plugin_name() == b"testflat"
     assert lib.prr_plugin_ray_bytes() == 48  # the reference's Ray layout (main/base.h:172-176)
     assert lib.prr_plugin_abi_version() == abi.load().prr_abi_version()  # plug-ins embed the frame layout
+    # the REFERENCE unit (-fmad=false) and the PHYSICAL unit (contraction on) both export their entry points
+    for sym in ("prr_plugin_trace", "prr_plugin_trace_physical", "prr_plugin_colour"):
+        assert hasattr(lib, sym), sym
     assert h.read_text() == USER_HEADER  # the header itself is not touched
     assert not (build.BUILD / "plugins" / "testflat").exists()  # staging copy removed
 
