@@ -36,15 +36,19 @@ template <class T> struct EmisRay {
 
 // f and l_x, l_y, l_z of the Kerr-Schild metric at (x, y, z), and the
 // Kerr-Schild r; flat (M = 0): f = 0.
-template <class T> PRR_DEV void ks_fl(T x, T y, T z, T M, T a, T &r, T &f, T l[3])
+template <class T> PRR_DEV void ks_fl_at(T x, T y, T z, T M, T a, T r, T &f, T l[3])
 {
-    r = ks_radius<T>(x, y, z, a);
     f = 0; l[0] = l[1] = l[2] = 0;
     if (M != (T)0) {
         const T r2 = r * r, q = r2 + a * a;
         f = ediv<T>((T)2 * M * r2 * r, r2 * r2 + a * a * z * z);
         l[0] = ediv<T>(r * x + a * y, q); l[1] = ediv<T>(r * y - a * x, q); l[2] = ediv<T>(z, r);
     }
+}
+template <class T> PRR_DEV void ks_fl(T x, T y, T z, T M, T a, T &r, T &f, T l[3])
+{
+    r = ks_radius<T>(x, y, z, a);
+    ks_fl_at<T>(x, y, z, M, a, r, f, l);
 }
 
 // nu_cam of a static observer at the camera: -k_t / sqrt(-g_tt).  The camera
@@ -97,9 +101,10 @@ PRR_DEV void emis_step(const FrameParams &fp, T M, T a, const V4<T> &x, const V4
 {
     const EmisParams &e = fp.em;
     if (e.kind == PRR_EMISSION_NONE) return;  // a frame without plasma in a batch with some
-    T r, f, l[3];
-    ks_fl<T>(x.x, x.y, x.z, M, a, r, f, l);
-    if (!(r >= (T)e.r_in && r <= (T)e.r_out)) return;
+    const T r = ks_radius<T>(x.x, x.y, x.z, a);
+    if (!(r >= (T)e.r_in && r <= (T)e.r_out)) return;  // outside the emitting shell: f and l are not needed
+    T f, l[3];
+    ks_fl_at<T>(x.x, x.y, x.z, M, a, r, f, l);
     T n, theta = 1, v[3];
     bool flow = false;
     if (e.kind == PRR_EMISSION_DISK) {
@@ -140,9 +145,10 @@ PRR_DEV void emis_step_p(const FrameParams &fp, T M, T a, T x, T y, T z, T px, T
 {
     const EmisParams &e = fp.em;
     if (e.kind == PRR_EMISSION_NONE) return;
-    T r, f, l[3];
-    ks_fl<T>(x, y, z, M, a, r, f, l);
-    if (!(r >= (T)e.r_in && r <= (T)e.r_out)) return;
+    const T r = ks_radius<T>(x, y, z, a);
+    if (!(r >= (T)e.r_in && r <= (T)e.r_out)) return;  // outside the emitting shell: f and l are not needed
+    T f, l[3];
+    ks_fl_at<T>(x, y, z, M, a, r, f, l);
     T n, theta = 1, v[3];
     bool flow = false;
     if (e.kind == PRR_EMISSION_DISK) {
