@@ -95,7 +95,7 @@ PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP,
     const T a2Z2 = mul_(c.a2, Z2);
     const T S2h = fma_(hb, hb, a2Z2);
     const T iSh = rsq_(S2h);
-    const T r2 = add_(hb, mul_(S2h, iSh));
+    const T r2 = fma_(S2h, iSh, hb);
     const T ir = rsq_(r2);
     const T r = mul_(r2, ir);
     const T q = add_(r2, c.a2), iq = rcp_(q);
@@ -120,9 +120,10 @@ PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP,
     // gradient of l.p at fixed p: grad r times Pp = ((x p_x + y p_y) - 2 r l.p_xy)/q - p_z l_z / r, taken
     // as (2 grad r) (Pp / 2)
     const T P0h = fma_(neg_(r), lpxy, mul_(T(0.5), fma_(px, X, mul_(py, Y))));
-    const T Pph = fma_(P0h, iq, neg_(mul_(mul_(T(0.5), pz), mul_(lz, ir))));
+    const T pzir = mul_(pz, ir);
+    const T Pph = fma_(P0h, iq, neg_(mul_(mul_(T(0.5), lz), pzir)));
     const V dL = fma_(dr2, sp(Pph), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
-    const T dLz = fma_(drz2, Pph, mul_(pz, ir));
+    const T dLz = fma_(drz2, Pph, pzir);
     // Hamilton's equations
     const T fL = mul_(f, Lam);
     const T L2 = mul_(Lam, Lam);
@@ -335,10 +336,10 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const 
     }
     // User_ENDLOOP, on the squared radius
     T r2 = R2;
-    if (q.metric == PRR_METRIC_KERR) {
-        const T b = r2 - q.a * q.a;
-        const T S2 = b * b + T(4) * q.a * q.a * zn * zn;
-        r2 = T(0.5) * (b + S2 * frsqrt<T>(S2));
+    if (q.metric == PRR_METRIC_KERR) {  // r^2 = hb + sqrt(hb^2 + a^2 z^2), hb = (R^2 - a^2)/2
+        const T hb = fma_(T(0.5), R2, sl.c.nha2);
+        const T S2h = fma_(hb, hb, mul_(sl.c.a2, mul_(zn, zn)));
+        r2 = fma_(S2h, frsqrt<T>(S2h), hb);
     }
     const bool escaped = r2 >= q.rout * q.rout;
     if (escaped || (q.metric != PRR_METRIC_FLAT && r2 <= q.rstop * q.rstop)) {
