@@ -120,10 +120,9 @@ PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP,
     // gradient of l.p at fixed p: grad r times Pp = ((x p_x + y p_y) - 2 r l.p_xy)/q - p_z l_z / r, taken
     // as (2 grad r) (Pp / 2)
     const T P0h = fma_(neg_(r), lpxy, mul_(T(0.5), fma_(px, X, mul_(py, Y))));
-    const T pzir = mul_(pz, ir);
-    const T Pph = fma_(P0h, iq, neg_(mul_(mul_(T(0.5), lz), pzir)));
+    const T Pph = fma_(P0h, iq, neg_(mul_(mul_(T(0.5), pz), mul_(lz, ir))));
     const V dL = fma_(dr2, sp(Pph), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
-    const T dLz = fma_(drz2, Pph, pzir);
+    const T dLz = fma_(drz2, Pph, mul_(pz, ir));
     // Hamilton's equations
     const T fL = mul_(f, Lam);
     const T L2 = mul_(Lam, Lam);
