@@ -36,6 +36,9 @@ Reported (one JSON line on rank 0):
   reference_cuda  the reference's own CUDA build (its sources, nvcc, sm_100a)
                   on this GPU: trace_RKF at eps 1e-6 on a band of rows, and
                   its whole frame pipeline at the deck's eps 1e-3
+From `plain` on, the sections run at N = 1 only: at N > 1 the line carries
+the headline, e2e, roofline and stats, so that no rank waits in the final
+barrier while rank 0 runs single-GPU studies.
 `--impl reference` runs the CPU arm alone: the FP64 host restatement on a
 fixed seeded sample of the frame's rays each step (see run_reference_arm).
 """
@@ -977,7 +980,7 @@ def main():
                     "fp64_peak_tflops": fp64_peak}
         extra["roofline"] = roofline
         extra["stats"] = {k: v for k, v in st.as_dict().items()}
-        if not args.no_plain:
+        if not args.no_plain and ws == 1:
             def timed_device(n=1):
                 ctx.render(frame)  # warm-up of this configuration
                 ev0.record(stream)
@@ -1013,7 +1016,7 @@ def main():
                               "breakdown_ms": {"plain_table": plain_ms, "plain_contraction": plain_contraction_ms,
                                                "persistent_table": table_ms, "persistent_contraction": contraction_ms,
                                                "persistent_hamiltonian": ms}}
-        if not args.no_adjoint:
+        if not args.no_adjoint and ws == 1:
             # discrete adjoint of the 512x512 differentiable-render workload: one gradient of an L2 image loss
             n = args.adjoint_size
             _, tgt, _ = ctx.render(scenes.kerr_512_adjoint(spin=0.7, precision=abi.PREC_FP32, size=n), want_float=True)
@@ -1043,7 +1046,7 @@ def main():
         ctx.upload_textures(tex)
         if not args.no_plugin and ws == 1:
             extra["plugin_kerr_header"] = bench_plugin_kerr(ctx, torch, stream, frame)
-        if not args.no_accuracy:
+        if not args.no_accuracy and ws == 1:
             extra["accuracy"] = bench_accuracy(ctx, frame, fp64_peak)
         if not args.no_cpu and ws == 1:
             # the cpu_baseline leg: the CPU restatement and the reference's host build, on this host's cores
