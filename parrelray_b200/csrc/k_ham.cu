@@ -10,7 +10,7 @@
 // and p_t = -E is a constant of the motion (the metric does not depend on
 // t), so the state is (x, y, z, p_x, p_y, p_z): six components instead of the
 // eight of (x, u), no coordinate time, and no directional derivatives or
-// raised contraction in the right-hand side (about 74 FP32 operations and 4
+// raised contraction in the right-hand side (about 65 FP32 operations and 4
 // SFU operations per evaluation, against about 110 for the contraction
 // geod_ks evaluates for du/dlambda).  The velocity u = dx/dlambda, which the
 // sphere test, the sky lookup and the per-ray outputs need, is formed from
@@ -101,16 +101,16 @@ PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP,
     const T q = add_(r2, c.a2), iq = rcp_(q);
     const T Sig = fma_(r2, r2, a2Z2), iSig = rcp_(Sig);
     const V iq_ = sp(iq);
-    // twice the gradient of r, and the gradient of f/2 (the 1/2 of 1/2 Lam^2 grad f folded in):
-    // grad f = c1 grad r with c1 = f (3/r - 4 r^3/Sigma); c1/4 = f (3/(4r) - r^3/Sigma)
+    // twice the gradient of r, and grad f / (2 f) (the 1/2 of 1/2 Lam^2 grad f folded in, and f taken out
+    // into f Lam below): grad f = c1 grad r with c1 = f (3/r - 4 r^3/Sigma); c1/(4 f) = 3/(4r) - r^3/Sigma
     const V dr2 = mul_(P, sp(mul_(r, iSh)));
     const T drz2 = mul_(mul_(z, q), mul_(iSh, ir));
     const T r3 = mul_(r2, r);
     const T t = mul_(r3, iSig);
     const T f = mul_(c.M2, t);
-    const T c1q = mul_(f, fma_(T(0.75), ir, neg_(t)));
-    const V dfh = mul_(sp(c1q), dr2);
-    const T dfzh = fma_(c1q, drz2, mul_(mul_(f, iSig), mul_(neg_(c.a2), z)));
+    const T c1h = fma_(T(0.75), ir, neg_(t));
+    const V dgh = mul_(sp(c1h), dr2);
+    const T dgzh = fma_(c1h, drz2, mul_(iSig, mul_(neg_(c.a2), z)));
     // l and Lam = l.p - p_t
     const V l = mul_(fma_(sp(r), P, f2(mul_(c.a, Y), neg_(mul_(c.a, X)))), iq_);
     const T lz = mul_(z, ir);
@@ -123,12 +123,12 @@ PRR_DEV void ham_rhs(P2<T> P, P2<T> Q, P2<T> W, const HamConst<T> &c, P2<T> &dP,
     const T Pph = fma_(P0h, iq, neg_(mul_(mul_(T(0.5), pz), mul_(lz, ir))));
     const V dL = fma_(dr2, sp(Pph), mul_(f2(fma_(r, px, neg_(mul_(c.a, py))), fma_(c.a, px, mul_(r, py))), iq_));
     const T dLz = fma_(drz2, Pph, mul_(pz, ir));
-    // Hamilton's equations
+    // Hamilton's equations, dp = 1/2 Lam^2 grad f + f Lam grad Lam = f Lam (Lam grad f / (2 f) + grad Lam)
     const T fL = mul_(f, Lam);
-    const T L2 = mul_(Lam, Lam);
-    dQ = fma_(sp(L2), dfh, mul_(sp(fL), dL));
-    dP = fma_(sp(neg_(fL)), l, Q);
-    dW = f2(fma_(neg_(fL), lz, pz), fma_(L2, dfzh, mul_(fL, dLz)));
+    const V sfL = sp(fL);
+    dQ = mul_(sfL, fma_(sp(Lam), dgh, dL));
+    dP = fma_(neg_(sfL), l, Q);
+    dW = f2(fma_(neg_(fL), lz, pz), mul_(fL, fma_(Lam, dgzh, dLz)));
 }
 
 // u = dx/dlambda (spatial) and u^t = -p_t + f Lam at (x, p), with IEEE
