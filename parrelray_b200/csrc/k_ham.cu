@@ -151,6 +151,7 @@ template <class T> struct HamRay {
     P2<T> P, Q, W;     // (x, y), (p_x, p_y), (z, p_z)
     P2<T> cP, cQ, cW;  // Kahan compensation (FP32 only)
     T h, trace_h, l;
+    T safe;  // FP32: distance to the nearest sphere's far radius at the last test, less the path since
     int i, accepted, intersect;
 };
 
@@ -187,6 +188,7 @@ __device__ __forceinline__ void ham_init(const FrameParams &fp, HSlot<T> &sl, in
     R.cP = R.cQ = R.cW = sp(T(0));
     R.h = (T)fp.h; R.trace_h = (T)fp.h; R.l = T(0);
     R.i = 0; R.accepted = 0; R.intersect = 0;
+    R.safe = T(-1);
     sl.c = {T(2) * M, a, a * a, T(-0.5) * a * a, p[3]};
     if constexpr (EMIS) emis_init_p<T>(fp, U.x.x, U.x.y, U.x.z, p[3], sl.E);
 }
@@ -301,8 +303,30 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const 
     T vx = 0, vy = 0, vz = 0, v2 = 0;
     bool near = false;
     const T R2 = xn * xn + yn * yn + zn * zn;
-    if (R2 >= (T)fp.sph_lo2 && R2 <= (T)fp.sph_hi2)
-        for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn, yn, zn);
+    T safe = T(0);
+    if constexpr (sizeof(T) == 4) {
+        // The far tests run only when the path since the last test may have come within a sphere's far
+        // radius: R.safe is the distance from the last tested point to the nearest far radius, less 1e-3,
+        // and every accepted step takes its increment's L1 length (>= its Euclidean length) off it (the
+        // compensated sums stay within rounding of the increments' sum). A point the margin covers is far
+        // from every sphere, so skipping its tests changes nothing. One lane's test refreshes the margins
+        // of the warp's other active lanes, which then run out together (a warp pays for the test once).
+        safe = R.safe - (abs_(st.dP.x) + abs_(st.dP.y) + abs_(st.dW.x));
+        if (__any_sync(__activemask(), !(safe > T(0)))) {
+            T m = T(1e30);
+            for (int s = 0; s < q.nspheres; s++) {
+                const DevSphere &S = fp.sph[s];
+                const T dx = xn - (T)S.cx, dy = yn - (T)S.cy, dz = zn - (T)S.cz;
+                const T d2 = fmax(dx * dx + dy * dy + dz * dz, T(1e-30));
+                near |= !(d2 > (T)S.far2);
+                m = fmin(m, d2 * frsqrt<T>(d2) - (T)S.far);
+            }
+            safe = m - T(1e-3);
+        }
+    } else {  // FP64: the square roots of a re-test cost more than the shell test saves on close cameras
+        if (R2 >= (T)fp.sph_lo2 && R2 <= (T)fp.sph_hi2)
+            for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn, yn, zn);
+    }
     if (near) {
         const V4<T> un = ham_velocity<T>(xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c);
         const T k = frsqrt<T>(un.x * un.x + un.y * un.y + un.z * un.z);
@@ -322,6 +346,7 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const 
         return STEP_CONTINUE;
     }
     R.P = Pn; R.Q = Qn; R.W = Wn; R.cP = cPn; R.cQ = cQn; R.cW = cWn;
+    R.safe = safe;
     R.accepted += 1;
     if constexpr (EMIS) emis_step_p<T>(fp, q.M, q.a, xn, yn, zn, Qn.x, Qn.y, Wn.y, sl.c.pt, h, sl.E);
     int candE;

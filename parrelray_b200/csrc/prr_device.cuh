@@ -126,6 +126,7 @@ struct DevSphere {
     float cx, cy, cz, r;
     DevTex tex;  // tex.p == nullptr: untextured (grey 0.5)
     float far2;  // squared distance beyond which no hit test can pass (PHYSICAL-mode early out)
+    float far;   // sqrt(far2)
 };
 
 // Everything a kernel needs about one frame, prepared on the host from a

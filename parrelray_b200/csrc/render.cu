@@ -197,7 +197,8 @@ prr_status build_plan(prr_ctx *ctx, const prr_frame_desc *frames, int n, RenderP
             // a hit with any window h <= hmax needs |p - c|^2 <= ((sqrt(hmax) + R)/2)^2 + R^2
             double reach = 0.5 * (std::sqrt((double)d.hmax) + S.radius);
             float far2 = (float)((reach * reach + (double)S.radius * S.radius) * 1.01 + 1e-3);
-            p.sph[s] = {S.center[0], S.center[1], S.center[2], S.radius, dev_tex(ctx, S.texture_id), far2};
+            p.sph[s] = {S.center[0], S.center[1], S.center[2], S.radius, dev_tex(ctx, S.texture_id), far2,
+                        (float)std::sqrt((double)far2)};
         }
         // the shell that holds every sphere's far radius: |p - c| >= | |p| - |c| |, so a point
         // with |p| > |c| + sqrt(far2) or |p| < |c| - sqrt(far2) is far from that sphere (the bounds
