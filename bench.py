@@ -77,12 +77,12 @@ F_ATTEMPT = 6 * FLOPS_GEOD_KERR + FLOPS_STAGES
 # the 960x540 copy of the headline frame (one launch, 64-thread CTAs at 8 per SM, refill every 64
 # attempts): FFMA x 2 FLOP, paired FFMA2 x 4 (two FMAs per thread instruction), FMUL/FADD x 1, paired
 # FMUL2/FADD2 x 2, summed and divided by the launch's attempt counter.  k_ham (the Hamiltonian form)
-# executes 940 FLOP per attempt; k_pair (the (x, u) contraction, the form F_ATTEMPT counts) 1,459.
-NCU_FLOP_PER_ATTEMPT = {"k_ham": 940.0, "k_pair": 1459.0}
+# executes 938 FLOP per attempt; k_pair (the (x, u) contraction, the form F_ATTEMPT counts) 1,459.
+NCU_FLOP_PER_ATTEMPT = {"k_ham": 938.0, "k_pair": 1459.0}
 NCU_FLOP_RULE = ("FP32 FLOP executed, from ncu sass_thread_inst_executed_op_{ffma,fmul,fadd}{,2}: FFMA 2, FFMA2 4, "
                  "FMUL/FADD 1, FMUL2/FADD2 2, per attempt")
 # DRAM bytes of one launch of the tracing kernel (ncu, 960x540 copy of the headline frame)
-TRAFFIC_PER_LAUNCH = 8.748032e6
+TRAFFIC_PER_LAUNCH = 8.724224e6
 
 
 def reserve_stdout():
