@@ -209,3 +209,33 @@ def test_device_reciprocals_against_correct_rounding(gpu):
     x32 = x.astype(np.float32).astype(np.float64)
     assert rel(out[:, 2], 1.0 / x32).max() <= 2.0 ** -21
     assert rel(out[:, 3], 1.0 / np.sqrt(x32)).max() <= 2.0 ** -21
+
+
+def eight_sphere_frame(precision=abi.PREC_FP32, W=96, H=54):
+    """Eight spheres (the most a frame holds) on orbits of 5 to 13.4 M around a Kerr a = 0.9 hole, with the
+    camera at 13 M among them: rays start close to spheres, graze their far radii and hit them (5 % of the
+    rays end on a sphere), which is where the FP32 renderer's per-ray sphere margins decide when to test."""
+    sph = []
+    for k in range(8):
+        x, y, _ = scenes.orbit_point(5.0 + 1.2 * k, 45.0 * k + 20.0)
+        sph.append((x, y, 0.5 * (k % 3 - 1), 0.9 + 0.2 * (k % 4), scenes.SPHERE_ID0 + k % 3))
+    return scenes.make_frame(W, H, r=13.0, incl_deg=75.0, fov_deg=80.0, metric=abi.METRIC_KERR, mass=1.0, spin=0.9,
+                             samples=1, fxaa=False, spheres=sph, precision=precision, tol=1e-6)
+
+
+def test_fp32_eight_spheres_camera_among_them_vs_fp64_oracle(gpu, oracle, small_textures):
+    """Per-ray outcomes and per-sample colours of the FP32 product on a sphere-heavy frame against the FP64
+    host oracle: the same result for >= 99.5 % of the rays, the colour within 1/255 for >= 99.5 %, and as
+    many rays ending on a sphere as the oracle's, to 1 % (at least 2 rays)."""
+    st_ref, rgb_ref = oracle.trace(eight_sphere_frame(abi.PREC_FP64), small_textures, precision=1)
+    d = eight_sphere_frame()
+    gpu.upload_textures(small_textures)
+    st, rgb, _ = gpu.trace_rays(d)
+    res_ref, res = st_ref[:, 2].astype(int), st[:, 2].astype(int)
+    hits_ref = int(np.sum(res_ref == abi.RESULT_INTERSECTION))
+    assert hits_ref > 0.03 * d.nrays, hits_ref  # the frame does exercise the sphere tests
+    assert abs(int(np.sum(res == abi.RESULT_INTERSECTION)) - hits_ref) <= max(2, hits_ref // 100)
+    assert np.mean(res == res_ref) >= 0.995, np.mean(res == res_ref)
+    dcol = np.abs(quantize(rgb).astype(np.int32) - quantize(rgb_ref).astype(np.int32)).max(axis=-1)
+    assert np.mean(dcol <= 1) >= 0.995, np.mean(dcol <= 1)
+    assert not np.any(res == abi.RESULT_MATH_ERROR)
