@@ -323,7 +323,8 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const 
             }
             safe = m - T(1e-3);
         }
-    } else {  // FP64: the square roots of a re-test cost more than the shell test saves on close cameras
+    } else {  // FP64 keeps the shell test: with the margin, close cameras re-test often, each re-test pays
+              // FP64 square roots, and the kernel spills more
         if (R2 >= (T)fp.sph_lo2 && R2 <= (T)fp.sph_hi2)
             for (int s = 0; s < q.nspheres; s++) near |= !sphere_far<T>(fp.sph[s], xn, yn, zn);
     }
