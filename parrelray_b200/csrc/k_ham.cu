@@ -308,10 +308,12 @@ PRR_DEV int ham_accept(const FrameParams &fp, HSlot<T> &sl, HamRay<T> &R, const 
         // The far tests run only when the path since the last test may have come within a sphere's far
         // radius: R.safe is the distance from the last tested point to the nearest far radius, less 1e-3,
         // and every accepted step takes its increment's L1 length (>= its Euclidean length) off it (the
-        // compensated sums stay within rounding of the increments' sum). A point the margin covers is far
-        // from every sphere, so skipping its tests changes nothing. One lane's test refreshes the margins
-        // of the warp's other active lanes, which then run out together (a warp pays for the test once).
-        safe = R.safe - (abs_(st.dP.x) + abs_(st.dP.y) + abs_(st.dW.x));
+        // compensated sums stay within rounding of the increments' sum). The length is summed rounding up
+        // and subtracted rounding down, so the margin never drifts above the true distance, however many
+        // small steps round against it. A point the margin covers is far from every sphere, so skipping
+        // its tests changes nothing. One lane's test refreshes the margins of the warp's other active
+        // lanes, which then run out together (a warp pays for the test once).
+        safe = __fsub_rd(R.safe, __fadd_ru(__fadd_ru(fabsf(st.dP.x), fabsf(st.dP.y)), fabsf(st.dW.x)));
         if (__any_sync(__activemask(), !(safe > T(0)))) {
             T m = T(1e30);
             for (int s = 0; s < q.nspheres; s++) {
